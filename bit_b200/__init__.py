@@ -1,0 +1,353 @@
+"""bit_b200 -- B200-native treecode behind the C ABI of include/bit_b200.h.
+
+Host-side mirror of the reference's treecode interface (ongbw/bit, src/tree3d.h):
+
+    ctx  = bit_b200.Context()
+    tree = ctx.treemake(x, y, z, maxmemb)          # treemake      src/tree3d.cpp:1345
+    tree.treemoments(q, nterms, w=None)            # treemoments   src/tree3d.cpp:2631
+    pot  = tree.treepotential(acc, del_)           # treepotential src/tree3d.cpp:4679
+    pot  = tree.shielded_treepot(kappa, acc)       # shielded_treepot src/tree3d.cpp:3448
+    fx, fy, fz = tree.treeforce(acc, del_)         # treeforce     src/tree3d.cpp:851
+    tree.treeempty()                               # treeempty     src/tree3d.cpp:990
+
+Every call goes through libbit_b200.so; there is no CPU fallback.  If the library is
+missing, importing works but the first call raises ``BitError``.
+"""
+import ctypes as C
+import os
+import weakref
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libbit_b200.so")
+
+COULOMB, SCREENED, SCREENED_REG = 0, 1, 2
+FP64, MIXED = 0, 1
+REFERENCE, CONSISTENT = 0, 1
+# intG of the reference's screened self term (src/tree3d.cpp:3585)
+REF_INTG = -0.0000483811229725
+NTERMS_MAX = 10
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
+          4: "capacity exceeded", 5: "degenerate input", 6: "GMRES breakdown",
+          7: "not converged", 8: "no CUDA device", 9: "HBM budget exceeded",
+          10: "invalid call order"}
+
+
+class BitError(RuntimeError):
+    def __init__(self, status, msg=""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+
+
+class CtxOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("stream", C.c_void_p), ("hbm_budget", C.c_size_t)]
+
+
+class EvalParams(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("mode", C.c_int), ("precision", C.c_int),
+                ("del_", C.c_double), ("mac_del", C.c_double), ("kappa", C.c_double),
+                ("acc", C.c_double), ("intg", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("t_build", C.c_double), ("t_moments", C.c_double), ("t_lists", C.c_double),
+                ("t_far", C.c_double), ("t_near", C.c_double), ("t_total", C.c_double),
+                ("far_pairs", C.c_longlong), ("near_pairs", C.c_longlong),
+                ("far_entries", C.c_longlong), ("near_entries", C.c_longlong),
+                ("batches", C.c_longlong), ("numtree", C.c_int), ("nleaves", C.c_int),
+                ("depth", C.c_int), ("nterms", C.c_int), ("far_launches", C.c_int),
+                ("near_launches", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GmresOpts(C.Structure):
+    _fields_ = [("restart", C.c_int), ("maxit", C.c_int), ("tol", C.c_double),
+                ("precision", C.c_int), ("inner_tol", C.c_double),
+                ("max_refinements", C.c_int)]
+
+
+class GmresInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refinements", C.c_int), ("matvecs_fp64", C.c_int),
+                ("matvecs_fp32", C.c_int), ("relres", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+
+# (name, restype, argtypes) of every entry point in include/bit_b200.h
+SIGNATURES = [
+    ("bit_status_string", C.c_char_p, [C.c_int]),
+    ("bit_abi_version", C.c_int, []),
+    ("bit_kernel_launches", C.c_longlong, []),
+    ("bit_ctx_create", C.c_int, [C.POINTER(_vp), C.POINTER(CtxOpts)]),
+    ("bit_ctx_destroy", C.c_int, [_vp]),
+    ("bit_ctx_last_error", C.c_char_p, [_vp]),
+    ("bit_ctx_synchronize", C.c_int, [_vp]),
+    ("bit_ctx_stream", C.c_int, [_vp, C.POINTER(_vp)]),
+    ("bit_ctx_memory", C.c_int, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    ("bit_tree_build", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, C.c_int, C.POINTER(_vp)]),
+    ("bit_tree_build_device", C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_int, C.POINTER(_vp)]),
+    ("bit_tree_destroy", C.c_int, [_vp]),
+    ("bit_tree_info", C.c_int, [_vp, _ip, _ip, _ip]),
+    ("bit_tree_set_charges", C.c_int, [_vp, _dp, _dp]),
+    ("bit_tree_set_charges_device", C.c_int, [_vp, _vp, _vp]),
+    ("bit_tree_moments", C.c_int, [_vp, C.c_int]),
+    ("bit_tree_export", C.c_int, [_vp, _ip, _ip, _dp, _ip]),
+    ("bit_tree_export_moments", C.c_int, [_vp, _dp]),
+    ("bit_eval_particles", C.c_int, [_vp, C.POINTER(EvalParams), _dp]),
+    ("bit_eval_particles_device", C.c_int, [_vp, C.POINTER(EvalParams), _vp]),
+    ("bit_eval_points", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _dp, _dp, _dp, _dp]),
+    ("bit_eval_force", C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp]),
+    ("bit_treecode_potential", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int,
+                                         C.c_int, C.POINTER(EvalParams), _dp]),
+    ("bit_tree_stats", C.c_int, [_vp, C.POINTER(Stats)]),
+    ("bit_tree_target_lists", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _ip, _ip, C.c_int,
+                                        _ip]),
+    ("bit_bie_solve", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, C.c_double, _dp, _dp, _dp,
+                                C.POINTER(GmresOpts), C.POINTER(GmresInfo)]),
+    ("bit_gmres_dense", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip]),
+]
+
+_lib = None
+
+
+def lib():
+    """The loaded libbit_b200.so (raises BitError if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BitError(2, f"{LIB_PATH} not built (run python -m bit_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def kernel_launches():
+    """Kernels launched by libbit_b200 in this process so far."""
+    return lib().bit_kernel_launches()
+
+
+def params(kernel=COULOMB, mode=CONSISTENT, precision=FP64, del_=0.0, mac_del=0.0, kappa=0.0,
+           acc=0.5, intg=REF_INTG):
+    return EvalParams(kernel, mode, precision, del_, mac_del, kappa, acc, intg)
+
+
+class Context:
+    """One CUDA stream on one device (bit_ctx_create)."""
+
+    def __init__(self, device=0, stream=None, hbm_budget=0):
+        self.h = _vp()
+        self._trees = weakref.WeakSet()
+        opts = CtxOpts(device, stream, hbm_budget)
+        st = lib().bit_ctx_create(C.byref(self.h), C.byref(opts))
+        if st:
+            raise BitError(st, "bit_ctx_create")
+
+    def check(self, st, what):
+        if st:
+            msg = lib().bit_ctx_last_error(self.h)
+            raise BitError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self.h:
+            for t in list(self._trees):
+                t.treeempty()
+            lib().bit_ctx_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        s = _vp()
+        lib().bit_ctx_stream(self.h, C.byref(s))
+        return s.value
+
+    def memory(self):
+        a, b = C.c_size_t(), C.c_size_t()
+        lib().bit_ctx_memory(self.h, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def synchronize(self):
+        self.check(lib().bit_ctx_synchronize(self.h), "synchronize")
+
+    def treemake(self, x, y, z, maxmemb):
+        return Tree(self, x, y, z, maxmemb)
+
+    def treemake_device(self, n, xptr, yptr, zptr, maxmemb):
+        return Tree(self, None, None, None, maxmemb, device=(n, xptr, yptr, zptr))
+
+    def treecode_potential(self, x, y, z, q, nterms, maxmemb, prm, w=None):
+        x, y, z, q = map(_f64, (x, y, z, q))
+        w = None if w is None else _f64(w)
+        out = np.zeros(len(x))
+        st = lib().bit_treecode_potential(self.h, len(x), _d(x), _d(y), _d(z), _d(q),
+                                          None if w is None else _d(w), nterms, maxmemb,
+                                          C.byref(prm), _d(out))
+        self.check(st, "bit_treecode_potential")
+        return out
+
+    def gmres_dense(self, A, b, x0=None):
+        """solver::gmres (src/solver.h:157) on the device."""
+        A, b = _f64(A), _f64(b)
+        x = np.ones(len(b)) if x0 is None else _f64(x0).copy()
+        it = C.c_int()
+        st = lib().bit_gmres_dense(self.h, len(b), _d(A), _d(b), _d(x), C.byref(it))
+        if st not in (0, 6):
+            self.check(st, "bit_gmres_dense")
+        return x, it.value, st
+
+
+class Tree:
+    def __init__(self, ctx, x, y, z, maxmemb, device=None):
+        self.ctx = ctx
+        self.h = _vp()
+        if device is None:
+            self.x, self.y, self.z = map(_f64, (x, y, z))
+            self.n = len(self.x)
+            st = lib().bit_tree_build(ctx.h, self.n, _d(self.x), _d(self.y), _d(self.z),
+                                      maxmemb, C.byref(self.h))
+        else:
+            self.n, xp, yp, zp = device
+            st = lib().bit_tree_build_device(ctx.h, self.n, xp, yp, zp, maxmemb,
+                                             C.byref(self.h))
+        ctx.check(st, "bit_tree_build")
+        ctx._trees.add(self)
+        self.maxmemb = maxmemb
+        self.nterms = 0
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        lib().bit_tree_info(self.h, C.byref(a), C.byref(b), C.byref(c))
+        self.numtree, self.nleaves, self.depth = a.value, b.value, c.value
+
+    def treeempty(self):
+        if self.h:
+            if self.ctx.h:
+                lib().bit_tree_destroy(self.h)
+            self.h = _vp()
+
+    close = treeempty
+
+    def __del__(self):
+        try:
+            self.treeempty()
+        except Exception:
+            pass
+
+    def set_charges(self, q, w=None):
+        q = _f64(q)
+        w = None if w is None else _f64(w)
+        self.ctx.check(lib().bit_tree_set_charges(self.h, _d(q), None if w is None else _d(w)),
+                       "bit_tree_set_charges")
+
+    def set_charges_device(self, qptr, wptr=None):
+        self.ctx.check(lib().bit_tree_set_charges_device(self.h, qptr, wptr),
+                       "bit_tree_set_charges_device")
+
+    def moments(self, nterms):
+        self.ctx.check(lib().bit_tree_moments(self.h, nterms), "bit_tree_moments")
+        self.nterms = nterms
+
+    def treemoments(self, q, nterms, w=None):
+        self.set_charges(q, w)
+        self.moments(nterms)
+
+    def export(self):
+        nt = self.numtree
+        nm = np.zeros(nt, np.int32)
+        ch = np.zeros(nt * 8, np.int32)
+        f = np.zeros(nt * 13)
+        self.ctx.check(lib().bit_tree_export(self.h, nm.ctypes.data_as(_ip), ch.ctypes.data_as(_ip),
+                                             _d(f), None), "bit_tree_export")
+        mem = np.zeros(int(nm.sum()), np.int32)
+        self.ctx.check(lib().bit_tree_export(self.h, None, None, None, mem.ctypes.data_as(_ip)),
+                       "bit_tree_export")
+        return nm, ch.reshape(nt, 8), f.reshape(nt, 13), mem
+
+    def export_moments(self):
+        T = self.nterms * (self.nterms + 1) * (self.nterms + 2) // 6
+        m = np.zeros(self.numtree * T)
+        self.ctx.check(lib().bit_tree_export_moments(self.h, _d(m)), "bit_tree_export_moments")
+        return m.reshape(self.numtree, T)
+
+    def evaluate(self, prm, points=None):
+        if points is not None:
+            pts = _f64(points)
+            tx, ty, tz = [np.ascontiguousarray(pts[:, a]) for a in range(3)]
+            out = np.zeros(len(pts))
+            self.ctx.check(lib().bit_eval_points(self.h, C.byref(prm), len(pts), _d(tx), _d(ty),
+                                                 _d(tz), _d(out)), "bit_eval_points")
+            return out
+        out = np.zeros(self.n)
+        self.ctx.check(lib().bit_eval_particles(self.h, C.byref(prm), _d(out)),
+                       "bit_eval_particles")
+        return out
+
+    def evaluate_device(self, prm, outptr):
+        self.ctx.check(lib().bit_eval_particles_device(self.h, C.byref(prm), outptr),
+                       "bit_eval_particles_device")
+
+    def treepotential(self, acc, del_, mode=CONSISTENT, precision=FP64, points=None):
+        return self.evaluate(params(COULOMB, mode, precision, del_=del_, acc=acc), points)
+
+    def shielded_treepot(self, kappa, acc, mode=CONSISTENT, precision=FP64, mac_del=0.0,
+                         intg=REF_INTG, points=None):
+        return self.evaluate(params(SCREENED, mode, precision, mac_del=mac_del, kappa=kappa,
+                                    acc=acc, intg=intg), points)
+
+    def treeforce(self, acc, del_, precision=FP64):
+        fx, fy, fz = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self.ctx.check(lib().bit_eval_force(self.h, del_, acc, precision, _d(fx), _d(fy), _d(fz)),
+                       "bit_eval_force")
+        return fx, fy, fz
+
+    def stats(self):
+        s = Stats()
+        self.ctx.check(lib().bit_tree_stats(self.h, C.byref(s)), "bit_tree_stats")
+        return s.as_dict()
+
+    def target_lists(self, prm, p, cap=8192):
+        node = np.zeros(cap, np.int32)
+        kind = np.zeros(cap, np.int32)
+        n = C.c_int()
+        self.ctx.check(lib().bit_tree_target_lists(self.h, C.byref(prm), p,
+                                                   node.ctypes.data_as(_ip),
+                                                   kind.ctypes.data_as(_ip), cap, C.byref(n)),
+                       "bit_tree_target_lists")
+        return node[:n.value].copy(), kind[:n.value].copy()
+
+    def bie_solve(self, prm, nterms, diag, w, f, restart=50, tol=1e-8, maxit=1000,
+                  precision=FP64, inner_tol=0.0, max_refinements=0):
+        """GMRES(m) on (diag*I + K) s = f with the treecode as the matvec."""
+        w, f = _f64(w), _f64(f)
+        s = np.zeros(self.n)
+        opts = GmresOpts(restart, maxit, tol, precision, inner_tol, max_refinements)
+        info = GmresInfo()
+        st = lib().bit_bie_solve(self.h, C.byref(prm), nterms, diag, _d(w), _d(f), _d(s),
+                                 C.byref(opts), C.byref(info))
+        if st not in (0, 7):
+            self.ctx.check(st, "bit_bie_solve")
+        return s, info.as_dict(), st

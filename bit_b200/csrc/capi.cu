@@ -1,0 +1,616 @@
+// The extern "C" boundary (include/bit_b200.h): argument checking, status codes, device
+// memory accounting, and the order of kernel phases for each entry point.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+
+namespace bit {
+
+void* dev_alloc(Ctx* c, size_t bytes) {
+  if (c->budget && c->in_use + bytes > c->budget)
+    fail(BIT_ERR_BUDGET, "allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget");
+  void* p = nullptr;
+  BIT_CUDA(cudaMalloc(&p, bytes));
+  c->in_use += bytes;
+  c->peak = std::max(c->peak, c->in_use);
+  c->allocs.push_back({p, bytes});
+  return p;
+}
+
+void dev_free(Ctx* c, void* p) {
+  if (!p) return;
+  for (size_t i = 0; i < c->allocs.size(); i++)
+    if (c->allocs[i].first == p) {
+      c->in_use -= c->allocs[i].second;
+      c->allocs[i] = c->allocs.back();
+      c->allocs.pop_back();
+      break;
+    }
+  cudaFree(p);
+}
+
+namespace {
+
+__global__ void k_scatter_out(int n, const int* perm, const double* sorted, double* out) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) out[perm[e]] = sorted[e];
+}
+
+template <class F>
+bit_status guard(Ctx* c, F&& f) {
+  try {
+    f();
+    if (c) c->last_error.clear();
+    return BIT_OK;
+  } catch (const Error& e) {
+    if (c) c->last_error = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (c) c->last_error = "host allocation failed";
+    return BIT_ERR_OUT_OF_MEMORY;
+  } catch (...) {
+    if (c) c->last_error = "unexpected internal error";
+    return BIT_ERR_CUDA;
+  }
+}
+
+void check_params(const bit_eval_params* p) {
+  if (!p) fail(BIT_ERR_INVALID_ARGUMENT, "params is NULL");
+  if (p->kernel < BIT_KERNEL_COULOMB || p->kernel > BIT_KERNEL_SCREENED_REG)
+    fail(BIT_ERR_INVALID_ARGUMENT, "unknown kernel");
+  if (p->mode != BIT_MODE_REFERENCE && p->mode != BIT_MODE_CONSISTENT)
+    fail(BIT_ERR_INVALID_ARGUMENT, "unknown mode");
+  if (p->precision != BIT_PREC_FP64 && p->precision != BIT_PREC_MIXED)
+    fail(BIT_ERR_INVALID_ARGUMENT, "unknown precision");
+  if (!(p->acc >= 0) || !std::isfinite(p->acc)) fail(BIT_ERR_INVALID_ARGUMENT, "acc must be >= 0");
+  if (!(p->del >= 0) || !std::isfinite(p->del)) fail(BIT_ERR_INVALID_ARGUMENT, "del must be >= 0");
+  if (p->kernel != BIT_KERNEL_COULOMB && !(p->kappa >= 0))
+    fail(BIT_ERR_INVALID_ARGUMENT, "kappa must be >= 0");
+}
+
+// Phase timers on the context stream.
+enum { EV_BUILD = 0, EV_MOM = 2, EV_LIST = 4, EV_FAR = 6, EV_NEAR = 8, EV_ALL = 10 };
+
+void ev_init(Tree* t) {
+  for (auto& e : t->ev)
+    if (!e) BIT_CUDA(cudaEventCreate(&e));
+}
+void ev_rec(Tree* t, int i) { BIT_CUDA(cudaEventRecord(t->ev[i], t->ctx->stream)); }
+double ev_sec(Tree* t, int i) {
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, t->ev[i], t->ev[i + 1]) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.0;
+  }
+  return ms * 1e-3;
+}
+
+void ensure_particle_lists(Tree* t, const bit_eval_params& p) {
+  ListKey k = mac_key(p, t->gen, 0);
+  if (t->plists.valid && t->plists.key == k) return;
+  ev_rec(t, EV_LIST);
+  build_lists(t, &t->plists, k, t->n, t->sx.p, t->sy.p, t->sz.p, nullptr);
+  ev_rec(t, EV_LIST + 1);
+  t->stats.t_lists = -1;  // resolved in stats
+}
+
+void eval_particles_sorted(Tree* t, const bit_eval_params& p) {
+  if (!t->has_moments) fail(BIT_ERR_STATE, "moments not computed (call bit_tree_moments)");
+  ensure_particle_lists(t, p);
+  t->pot_sorted.ensure(t->ctx, t->n);
+  ev_rec(t, EV_FAR);
+  eval_far(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, t->pot_sorted.p);
+  ev_rec(t, EV_FAR + 1);
+  ev_rec(t, EV_NEAR);
+  eval_near(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, t->pot_sorted.p);
+  ev_rec(t, EV_NEAR + 1);
+  t->stats.far_pairs = t->plists.far_pairs;
+  t->stats.near_pairs = t->plists.near_pairs;
+  t->stats.far_entries = t->plists.nfar;
+  t->stats.near_entries = t->plists.nnear;
+  t->stats.batches = t->plists.nbatch;
+  t->stats.far_launches = 1;
+  t->stats.near_launches = 1;
+}
+
+uint64_t spread3(uint64_t v) {
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffULL;
+  v = (v | v << 16) & 0x1f0000ff0000ffULL;
+  v = (v | v << 8) & 0x100f00f00f00f00fULL;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+  v = (v | v << 2) & 0x1249249249249249ULL;
+  return v;
+}
+
+}  // namespace
+}  // namespace bit
+
+using namespace bit;
+
+extern "C" {
+
+const char* bit_status_string(bit_status s) {
+  switch (s) {
+    case BIT_OK: return "ok";
+    case BIT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case BIT_ERR_CUDA: return "CUDA error";
+    case BIT_ERR_OUT_OF_MEMORY: return "out of memory";
+    case BIT_ERR_CAPACITY: return "capacity exceeded";
+    case BIT_ERR_DEGENERATE: return "degenerate input (coincident particles)";
+    case BIT_ERR_BREAKDOWN: return "GMRES breakdown";
+    case BIT_ERR_NOT_CONVERGED: return "not converged";
+    case BIT_ERR_NO_DEVICE: return "no CUDA device";
+    case BIT_ERR_BUDGET: return "HBM budget exceeded";
+    case BIT_ERR_STATE: return "invalid call order";
+  }
+  return "unknown status";
+}
+
+int bit_abi_version(void) { return BIT_ABI_VERSION; }
+
+bit_status bit_ctx_create(bit_ctx** out, const bit_ctx_opts* opts) {
+  if (!out) return BIT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return BIT_ERR_NO_DEVICE;
+  }
+  bit_ctx* h = new (std::nothrow) bit_ctx;
+  if (!h) return BIT_ERR_OUT_OF_MEMORY;
+  bit_status st = guard(&h->c, [&] {
+    Ctx& c = h->c;
+    c.device = opts ? opts->device : 0;
+    if (c.device < 0 || c.device >= ndev) fail(BIT_ERR_INVALID_ARGUMENT, "bad device ordinal");
+    BIT_CUDA(cudaSetDevice(c.device));
+    c.budget = opts ? opts->hbm_budget : 0;
+    if (opts && opts->stream) {
+      c.stream = static_cast<cudaStream_t>(opts->stream);
+    } else {
+      BIT_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+      c.own_stream = true;
+    }
+    BIT_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, c.device));
+    BIT_CUDA(cudaMallocHost(&c.h_pinned, 64 * sizeof(long long)));
+  });
+  if (st != BIT_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return BIT_OK;
+}
+
+bit_status bit_ctx_destroy(bit_ctx* h) {
+  if (!h) return BIT_ERR_INVALID_ARGUMENT;
+  Ctx& c = h->c;
+  cudaSetDevice(c.device);
+  if (c.stream) cudaStreamSynchronize(c.stream);
+  // trees still held by the caller lose their device memory and their context; a later
+  // bit_tree_destroy on them only frees the handle
+  for (Tree* t : c.trees) {
+    for (auto& e : t->ev)
+      if (e) cudaEventDestroy(e);
+    t->~Tree();
+    new (t) Tree();
+  }
+  c.trees.clear();
+  c.scratch_ll.release();
+  if (c.h_pinned) cudaFreeHost(c.h_pinned);
+  if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+  delete h;
+  return BIT_OK;
+}
+
+const char* bit_ctx_last_error(const bit_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
+
+bit_status bit_ctx_synchronize(bit_ctx* h) {
+  if (!h) return BIT_ERR_INVALID_ARGUMENT;
+  return guard(&h->c, [&] { BIT_CUDA(cudaStreamSynchronize(h->c.stream)); });
+}
+
+bit_status bit_ctx_stream(const bit_ctx* h, void** stream) {
+  if (!h || !stream) return BIT_ERR_INVALID_ARGUMENT;
+  *stream = h->c.stream;
+  return BIT_OK;
+}
+
+bit_status bit_ctx_memory(const bit_ctx* h, size_t* in_use, size_t* peak) {
+  if (!h) return BIT_ERR_INVALID_ARGUMENT;
+  if (in_use) *in_use = h->c.in_use;
+  if (peak) *peak = h->c.peak;
+  return BIT_OK;
+}
+
+static bit_status build_common(bit_ctx* h, int n, const double* x, const double* y,
+                               const double* z, int maxmemb, bit_tree** out, bool host) {
+  if (!h || !out || !x || !y || !z) return BIT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  Ctx* c = &h->c;
+  if (n < 1 || maxmemb < 1) {
+    c->last_error = "n and maxmemb must be >= 1";
+    return BIT_ERR_INVALID_ARGUMENT;
+  }
+  bit_tree* th = new (std::nothrow) bit_tree;
+  if (!th) return BIT_ERR_OUT_OF_MEMORY;
+  bit_status st = guard(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    Tree* t = &th->t;
+    t->ctx = c;
+    t->n = n;
+    t->maxmemb = maxmemb;
+    ev_init(t);
+    ev_rec(t, EV_BUILD);
+    if (host) {
+      DBuf<double> dx, dy, dz;
+      dx.ensure(c, n); dy.ensure(c, n); dz.ensure(c, n);
+      BIT_CUDA(cudaMemcpyAsync(dx.p, x, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      BIT_CUDA(cudaMemcpyAsync(dy.p, y, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      BIT_CUDA(cudaMemcpyAsync(dz.p, z, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      tree_build(t, dx.p, dy.p, dz.p);
+    } else {
+      tree_build(t, x, y, z);
+    }
+    ev_rec(t, EV_BUILD + 1);
+    t->stats.numtree = t->numtree;
+    t->stats.nleaves = t->nleaves;
+    t->stats.depth = t->depth;
+  });
+  if (st != BIT_OK) {
+    for (auto& e : th->t.ev)
+      if (e) cudaEventDestroy(e);
+    delete th;
+    return st;
+  }
+  c->trees.push_back(&th->t);
+  *out = th;
+  return BIT_OK;
+}
+
+bit_status bit_tree_build(bit_ctx* h, int n, const double* x, const double* y, const double* z,
+                          int maxmemb, bit_tree** out) {
+  return build_common(h, n, x, y, z, maxmemb, out, true);
+}
+
+bit_status bit_tree_build_device(bit_ctx* h, int n, const double* x, const double* y,
+                                 const double* z, int maxmemb, bit_tree** out) {
+  return build_common(h, n, x, y, z, maxmemb, out, false);
+}
+
+bit_status bit_tree_destroy(bit_tree* th) {
+  if (!th) return BIT_ERR_INVALID_ARGUMENT;
+  Tree& t = th->t;
+  if (t.ctx) {
+    cudaSetDevice(t.ctx->device);
+    cudaStreamSynchronize(t.ctx->stream);
+    auto& v = t.ctx->trees;
+    v.erase(std::remove(v.begin(), v.end(), &t), v.end());
+  }
+  for (auto& e : t.ev)
+    if (e) cudaEventDestroy(e);
+  delete th;
+  return BIT_OK;
+}
+
+bit_status bit_tree_info(const bit_tree* th, int* numtree, int* nleaves, int* depth) {
+  if (!th) return BIT_ERR_INVALID_ARGUMENT;
+  if (numtree) *numtree = th->t.numtree;
+  if (nleaves) *nleaves = th->t.nleaves;
+  if (depth) *depth = th->t.depth;
+  return BIT_OK;
+}
+
+static bit_status set_charges(bit_tree* th, const double* q, const double* w, bool host) {
+  if (!th || !q) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  Ctx* c = t->ctx;
+  return guard(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    if (host) {
+      DBuf<double> dq, dw;
+      dq.ensure(c, t->n);
+      BIT_CUDA(cudaMemcpyAsync(dq.p, q, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      if (w) {
+        dw.ensure(c, t->n);
+        BIT_CUDA(cudaMemcpyAsync(dw.p, w, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      }
+      tree_set_charges(t, dq.p, w ? dw.p : nullptr);
+      BIT_CUDA(cudaStreamSynchronize(c->stream));
+    } else {
+      tree_set_charges(t, q, w);
+    }
+  });
+}
+
+bit_status bit_tree_set_charges(bit_tree* th, const double* q, const double* w) {
+  return set_charges(th, q, w, true);
+}
+bit_status bit_tree_set_charges_device(bit_tree* th, const double* q, const double* w) {
+  return set_charges(th, q, w, false);
+}
+
+bit_status bit_tree_moments(bit_tree* th, int nterms) {
+  if (!th) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  return guard(t->ctx, [&] {
+    BIT_CUDA(cudaSetDevice(t->ctx->device));
+    ev_rec(t, EV_MOM);
+    tree_moments(t, nterms);
+    ev_rec(t, EV_MOM + 1);
+    t->stats.nterms = nterms;
+  });
+}
+
+bit_status bit_tree_export(const bit_tree* th, int* nummemb, int* children, double* fields,
+                           int* members) {
+  if (!th) return BIT_ERR_INVALID_ARGUMENT;
+  const Tree* t = &th->t;
+  return guard(t->ctx, [&] {
+    const int b = t->numtree;
+    if (nummemb) std::memcpy(nummemb, t->h_nummemb.data(), b * sizeof(int));
+    if (children) std::memcpy(children, t->h_children.data(), 8LL * b * sizeof(int));
+    if (fields) std::memcpy(fields, t->h_fields.data(), 13LL * b * sizeof(double));
+    if (members) {
+      std::vector<int> perm(t->n);
+      BIT_CUDA(cudaMemcpy(perm.data(), t->perm.p, t->n * sizeof(int), cudaMemcpyDeviceToHost));
+      long long off = 0;
+      for (int i = 0; i < b; i++) {
+        int st = t->h_start[i], cnt = t->h_nummemb[i];
+        std::memcpy(members + off, perm.data() + st, cnt * sizeof(int));
+        std::sort(members + off, members + off + cnt);
+        off += cnt;
+      }
+    }
+  });
+}
+
+bit_status bit_tree_export_moments(const bit_tree* th, double* mom) {
+  if (!th || !mom) return BIT_ERR_INVALID_ARGUMENT;
+  const Tree* t = &th->t;
+  if (!t->has_moments) return BIT_ERR_STATE;
+  return guard(t->ctx, [&] {
+    BIT_CUDA(cudaMemcpy(mom, t->mom64.p, (size_t)t->numtree * num_terms(t->nterms) * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  });
+}
+
+bit_status bit_eval_particles_device(bit_tree* th, const bit_eval_params* prm, double* pot) {
+  if (!th || !pot) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  return guard(t->ctx, [&] {
+    check_params(prm);
+    BIT_CUDA(cudaSetDevice(t->ctx->device));
+    ev_rec(t, EV_ALL);
+    eval_particles_sorted(t, *prm);
+    count_launch(), k_scatter_out<<<grid_for(t->n, 256), 256, 0, t->ctx->stream>>>(t->n, t->perm.p,
+                                                                   t->pot_sorted.p, pot);
+    BIT_CHECK_LAUNCH();
+    ev_rec(t, EV_ALL + 1);
+  });
+}
+
+bit_status bit_eval_particles(bit_tree* th, const bit_eval_params* prm, double* pot) {
+  if (!th || !pot) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  Ctx* c = t->ctx;
+  return guard(c, [&] {
+    check_params(prm);
+    BIT_CUDA(cudaSetDevice(c->device));
+    DBuf<double> out;
+    out.ensure(c, t->n);
+    ev_rec(t, EV_ALL);
+    eval_particles_sorted(t, *prm);
+    count_launch(), k_scatter_out<<<grid_for(t->n, 256), 256, 0, c->stream>>>(t->n, t->perm.p, t->pot_sorted.p, out.p);
+    BIT_CHECK_LAUNCH();
+    ev_rec(t, EV_ALL + 1);
+    BIT_CUDA(cudaMemcpyAsync(pot, out.p, t->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    BIT_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+bit_status bit_eval_points(bit_tree* th, const bit_eval_params* prm, int m, const double* x,
+                           const double* y, const double* z, double* pot) {
+  if (!th || !x || !y || !z || !pot || m < 0) return BIT_ERR_INVALID_ARGUMENT;
+  if (m == 0) return BIT_OK;
+  Tree* t = &th->t;
+  Ctx* c = t->ctx;
+  return guard(c, [&] {
+    check_params(prm);
+    if (!t->has_moments) fail(BIT_ERR_STATE, "moments not computed");
+    BIT_CUDA(cudaSetDevice(c->device));
+    // spatial (Morton) order of the points so that a batch is compact
+    double lo[3] = {x[0], y[0], z[0]}, hi[3] = {x[0], y[0], z[0]};
+    for (int i = 0; i < m; i++) {
+      double v[3] = {x[i], y[i], z[i]};
+      for (int a = 0; a < 3; a++) {
+        if (std::isnan(v[a])) fail(BIT_ERR_INVALID_ARGUMENT, "point coordinates contain NaN");
+        lo[a] = std::min(lo[a], v[a]);
+        hi[a] = std::max(hi[a], v[a]);
+      }
+    }
+    std::vector<std::pair<uint64_t, int>> key(m);
+    for (int i = 0; i < m; i++) {
+      double v[3] = {x[i], y[i], z[i]};
+      uint64_t code = 0;
+      for (int a = 0; a < 3; a++) {
+        double s = hi[a] > lo[a] ? (v[a] - lo[a]) / (hi[a] - lo[a]) : 0.0;
+        uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, s * 2097151.0));
+        code |= spread3(q) << a;
+      }
+      key[i] = {code, i};
+    }
+    std::sort(key.begin(), key.end());
+    std::vector<double> sx(m), sy(m), sz(m);
+    std::vector<int> ord(m);
+    for (int i = 0; i < m; i++) {
+      ord[i] = key[i].second;
+      sx[i] = x[ord[i]]; sy[i] = y[ord[i]]; sz[i] = z[ord[i]];
+    }
+    DBuf<double> dx, dy, dz, out;
+    DBuf<int> dord;
+    dx.ensure(c, m); dy.ensure(c, m); dz.ensure(c, m); out.ensure(c, m); dord.ensure(c, m);
+    cudaStream_t s = c->stream;
+    BIT_CUDA(cudaMemcpyAsync(dx.p, sx.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dy.p, sy.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dz.p, sz.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dord.p, ord.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    Lists L;
+    build_lists(t, &L, mac_key(*prm, t->gen, 1), m, dx.p, dy.p, dz.p, nullptr);
+    eval_far(t, &L, *prm, 1, dx.p, dy.p, dz.p, out.p);
+    eval_near(t, &L, *prm, 1, dx.p, dy.p, dz.p, out.p);
+    DBuf<double> res;
+    res.ensure(c, m);
+    count_launch(), k_scatter_out<<<grid_for(m, 256), 256, 0, s>>>(m, dord.p, out.p, res.p);
+    BIT_CHECK_LAUNCH();
+    BIT_CUDA(cudaMemcpyAsync(pot, res.p, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+bit_status bit_eval_force(bit_tree* th, double del, double acc, bit_precision prec, double* fx,
+                          double* fy, double* fz) {
+  if (!th || !fx || !fy || !fz) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  Ctx* c = t->ctx;
+  return guard(c, [&] {
+    if (!t->has_moments) fail(BIT_ERR_STATE, "moments not computed");
+    if (t->nterms > kNtermsMax) fail(BIT_ERR_INVALID_ARGUMENT, "nterms too large for the force");
+    BIT_CUDA(cudaSetDevice(c->device));
+    bit_eval_params p{};
+    p.kernel = BIT_KERNEL_COULOMB;
+    p.del = del;
+    p.acc = acc;
+    p.precision = prec;
+    ensure_particle_lists(t, p);
+    const int n = t->n;
+    t->fx_sorted.ensure(c, n); t->fy_sorted.ensure(c, n); t->fz_sorted.ensure(c, n);
+    ev_rec(t, EV_FAR);
+    eval_far_force(t, &t->plists, del, prec, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
+    ev_rec(t, EV_FAR + 1);
+    ev_rec(t, EV_NEAR);
+    eval_near_force(t, &t->plists, del, prec, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
+    ev_rec(t, EV_NEAR + 1);
+    DBuf<double> o;
+    o.ensure(c, 3LL * n);
+    cudaStream_t s = c->stream;
+    count_launch(), k_scatter_out<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->fx_sorted.p, o.p);
+    count_launch(), k_scatter_out<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->fy_sorted.p, o.p + n);
+    count_launch(), k_scatter_out<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->fz_sorted.p, o.p + 2LL * n);
+    BIT_CHECK_LAUNCH();
+    BIT_CUDA(cudaMemcpyAsync(fx, o.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(fy, o.p + n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(fz, o.p + 2LL * n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+bit_status bit_treecode_potential(bit_ctx* h, int n, const double* x, const double* y,
+                                  const double* z, const double* q, const double* w, int nterms,
+                                  int maxmemb, const bit_eval_params* prm, double* pot) {
+  if (!h || !q || !pot || !prm) return BIT_ERR_INVALID_ARGUMENT;
+  bit_tree* t = nullptr;
+  bit_status st = bit_tree_build(h, n, x, y, z, maxmemb, &t);
+  if (st == BIT_OK) st = bit_tree_set_charges(t, q, w);
+  if (st == BIT_OK) st = bit_tree_moments(t, nterms);
+  if (st == BIT_OK) st = bit_eval_particles(t, prm, pot);
+  if (t) {
+    std::string keep = h->c.last_error;
+    bit_tree_destroy(t);
+    h->c.last_error = keep;
+  }
+  return st;
+}
+
+bit_status bit_tree_stats(const bit_tree* th, bit_stats* st) {
+  if (!th || !st) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = const_cast<Tree*>(&th->t);
+  return guard(t->ctx, [&] {
+    BIT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    bit_stats s = t->stats;
+    s.t_build = ev_sec(t, EV_BUILD);
+    s.t_moments = ev_sec(t, EV_MOM);
+    s.t_lists = ev_sec(t, EV_LIST);
+    s.t_far = ev_sec(t, EV_FAR);
+    s.t_near = ev_sec(t, EV_NEAR);
+    s.t_total = ev_sec(t, EV_ALL);
+    s.numtree = t->numtree;
+    s.nleaves = t->nleaves;
+    s.depth = t->depth;
+    s.nterms = t->nterms;
+    *st = s;
+  });
+}
+
+bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p, int* node,
+                                 int* kind, int cap, int* n) {
+  if (!th || !prm || !n || p < 0 || p >= th->t.n) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  return guard(t->ctx, [&] {
+    check_params(prm);
+    ensure_particle_lists(t, *prm);
+    Lists& L = t->plists;
+    int e = 0;
+    BIT_CUDA(cudaMemcpy(&e, t->iperm.p + p, sizeof(int), cudaMemcpyDeviceToHost));
+    // find the batch holding sorted position e
+    std::vector<int> ts(L.nbatch), tc(L.nbatch);
+    BIT_CUDA(cudaMemcpy(ts.data(), L.b_tstart.p, L.nbatch * sizeof(int), cudaMemcpyDeviceToHost));
+    BIT_CUDA(cudaMemcpy(tc.data(), L.b_tcount.p, L.nbatch * sizeof(int), cudaMemcpyDeviceToHost));
+    int b = -1;
+    for (int i = 0; i < L.nbatch; i++)
+      if (e >= ts[i] && e < ts[i] + tc[i]) { b = i; break; }
+    if (b < 0) fail(BIT_ERR_STATE, "target not found in batches");
+    const int lane = e - ts[b];
+    long long fo[2], no[2];
+    BIT_CUDA(cudaMemcpy(fo, L.far_off.p + b, 2 * sizeof(long long), cudaMemcpyDeviceToHost));
+    BIT_CUDA(cudaMemcpy(no, L.near_off.p + b, 2 * sizeof(long long), cudaMemcpyDeviceToHost));
+    std::vector<int2> fe(fo[1] - fo[0]), ne(no[1] - no[0]);
+    if (!fe.empty()) BIT_CUDA(cudaMemcpy(fe.data(), L.far_ent.p + fo[0], fe.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+    if (!ne.empty()) BIT_CUDA(cudaMemcpy(ne.data(), L.near_ent.p + no[0], ne.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+    // merge back into traversal order: far and near entries were emitted along one
+    // depth-first walk, so order them by the node's DFS preorder rank
+    std::vector<int> rank(t->numtree, 0);
+    {
+      int r = 0;
+      std::vector<int> stk{0};
+      while (!stk.empty()) {
+        int nd = stk.back();
+        stk.pop_back();
+        rank[nd] = r++;
+        for (int k = 7; k >= 0; k--) {
+          int ch = t->h_children[8LL * nd + k];
+          if (ch != -1) stk.push_back(ch);
+        }
+      }
+    }
+    std::vector<std::pair<int, int>> all;
+    for (auto& v : fe)
+      if ((unsigned(v.y) >> lane) & 1u) all.push_back({v.x, 0});
+    for (auto& v : ne)
+      if ((unsigned(v.y) >> lane) & 1u) all.push_back({v.x, 1});
+    std::sort(all.begin(), all.end(),
+              [&](const std::pair<int, int>& a, const std::pair<int, int>& b2) { return rank[a.first] < rank[b2.first]; });
+    for (int i = 0; i < (int)all.size() && i < cap; i++) {
+      if (node) node[i] = all[i].first;
+      if (kind) kind[i] = all[i].second;
+    }
+    *n = (int)all.size();
+  });
+}
+
+}  // extern "C"
+
+namespace bit {
+long long& launch_counter() {
+  static long long n = 0;
+  return n;
+}
+}  // namespace bit
+
+extern "C" long long bit_kernel_launches(void) { return bit::launch_counter(); }

@@ -1,0 +1,203 @@
+// Internal definitions shared by the CUDA sources of libbit_b200 (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "bit_b200.h"
+
+namespace bit {
+
+constexpr int kWarp = 32;
+constexpr int kNtermsMax = BIT_NTERMS_MAX;
+constexpr int kBatch = 32;        // targets per batch (one per lane of a warp)
+constexpr int kStackCap = 512;    // DFS stack entries per warp in the list builder
+constexpr double kEpsNear = 1e-14;  // src/constants.h:35
+
+__host__ __device__ constexpr int num_terms(int n) { return n * (n + 1) * (n + 2) / 6; }
+
+// ---- status plumbing ----------------------------------------------------------------
+struct Error {
+  bit_status code;
+  std::string msg;
+};
+
+#define BIT_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      throw ::bit::Error{e_ == cudaErrorMemoryAllocation ? BIT_ERR_OUT_OF_MEMORY        \
+                                                         : BIT_ERR_CUDA,                 \
+                         std::string(#call) + ": " + cudaGetErrorString(e_)};            \
+  } while (0)
+
+#define BIT_CHECK_LAUNCH() BIT_CUDA(cudaGetLastError())
+
+inline void fail(bit_status c, const std::string& m) { throw Error{c, m}; }
+
+// Kernels launched by this library in this process (every launch site counts itself).
+long long& launch_counter();
+inline void count_launch() { ++launch_counter(); }
+
+// ---- device memory with budget accounting ------------------------------------------
+struct Ctx;
+struct Tree;
+void* dev_alloc(Ctx* c, size_t bytes);
+void dev_free(Ctx* c, void* p);
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  Ctx* c = nullptr;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) dev_free(c, p);
+    p = nullptr;
+    n = 0;
+  }
+  // (Re)allocate to at least `count` elements; contents are not preserved.
+  void ensure(Ctx* ctx, size_t count) {
+    if (count <= n && p) return;
+    release();
+    c = ctx;
+    if (count == 0) count = 1;
+    p = static_cast<T*>(dev_alloc(ctx, count * sizeof(T)));
+    n = count;
+  }
+  // Grow keeping the first `keep` elements.
+  void grow(Ctx* ctx, size_t count, size_t keep, cudaStream_t s);
+  T* get() const { return p; }
+};
+
+// ---- interaction lists of one target set under one MAC --------------------------------
+struct ListKey {
+  double acc = -1, add_del = 0, sub_del = 0;
+  int points = 0;  // 0: particle targets, 1: external points
+  long long gen = -1;  // tree generation it was built for
+  bool operator==(const ListKey& o) const {
+    return acc == o.acc && add_del == o.add_del && sub_del == o.sub_del &&
+           points == o.points && gen == o.gen;
+  }
+};
+
+struct Lists {
+  ListKey key;
+  bool valid = false;
+  int nbatch = 0;
+  long long nfar = 0, nnear = 0;          // entries
+  long long far_pairs = 0, near_pairs = 0;  // interactions
+  DBuf<int> b_tstart, b_tcount, b_srcleaf;  // batch: first sorted target, count, leaf of targets
+  DBuf<long long> far_off, near_off;        // nbatch + 1
+  DBuf<int2> far_ent, near_ent;             // (node, lane mask)
+  DBuf<int> order;                          // batches sorted by decreasing work
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  size_t budget = 0, in_use = 0, peak = 0;
+  std::string last_error;
+  int num_sms = 148;
+  // small device scratch for flags / counters
+  DBuf<long long> scratch_ll;
+  long long* h_pinned = nullptr;  // pinned host staging for small read-backs (64 entries)
+  std::vector<std::pair<void*, size_t>> allocs;  // live device allocations and their sizes
+  std::vector<Tree*> trees;                       // trees built by this context
+  long long launches = 0;                         // kernels launched by this context
+};
+
+struct Tree {
+  Ctx* ctx = nullptr;
+  long long gen = 0;
+  int n = 0, maxmemb = 0, numtree = 0, nleaves = 0, depth = 0, cap = 0;
+  // particles in tree order (sorted position e); perm[e] = original index
+  DBuf<int> perm, iperm;
+  DBuf<double> sx, sy, sz, sq, sw;
+  DBuf<double4> src64;   // (x, y, z, q)
+  DBuf<float4> src32;    // leaf-centred (x-c, y-c, z-c, q)
+  DBuf<int> leaf_of;     // leaf node of each sorted position
+  // nodes
+  DBuf<int> nummemb, start, children, level, parent;
+  DBuf<double> fields;   // 13 per node
+  DBuf<double4> nodec;   // (xmid, ymid, zmid, sqradius)
+  DBuf<int> leaves;
+  // host mirror of the node structure
+  std::vector<int> h_nummemb, h_start, h_children, h_level, h_perm;
+  std::vector<double> h_fields;
+  // charges and moments
+  bool has_charges = false, has_weights = false;
+  int nterms = 0;
+  bool has_moments = false;
+  DBuf<double> mom64;
+  DBuf<float> mom32;
+  // moment work plan: (node, first, last) member chunks and per-chunk partial sums
+  long long mplan_gen = -1;
+  int mplan_nch = 0;
+  DBuf<int4> mplan_chunks;
+  DBuf<int> mplan_c0, mplan_c1;
+  DBuf<double> mplan_part;
+  // lists and outputs
+  Lists plists;            // particle targets
+  DBuf<double> pot_sorted, fx_sorted, fy_sorted, fz_sorted;
+  bit_stats stats{};
+  cudaEvent_t ev[12] = {};
+};
+
+// ---- exact FP64 helpers (no contraction) for the MAC and the tree fields -----------------
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// ---- entry points implemented in the .cu files -----------------------------------------
+void tree_build(Tree* t, const double* dx, const double* dy, const double* dz);
+void tree_sync_host(Tree* t);
+void tree_set_charges(Tree* t, const double* dq, const double* dw);
+void tree_moments(Tree* t, int nterms);
+void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const double* tx,
+                 const double* ty, const double* tz, const int* t_leaf);
+void eval_far(Tree* t, Lists* L, const bit_eval_params& p, int points, const double* tx,
+              const double* ty, const double* tz, double* out_sorted);
+void eval_near(Tree* t, Lists* L, const bit_eval_params& p, int points, const double* tx,
+               const double* ty, const double* tz, double* out_sorted);
+void eval_near_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
+                     double* fz);
+void eval_far_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
+                    double* fz);
+
+// MAC parameters of an evaluation: accept iff sqradius < acc * ((r^2 + add) - sub).
+inline ListKey mac_key(const bit_eval_params& p, long long gen, int points) {
+  ListKey k;
+  k.acc = p.acc;
+  k.points = points;
+  k.gen = gen;
+  if (p.kernel == BIT_KERNEL_SCREENED) {
+    k.add_del = 0.0;
+    k.sub_del = p.mac_del;
+  } else {
+    k.add_del = p.del;
+    k.sub_del = p.del;
+  }
+  return k;
+}
+
+inline unsigned grid_for(long long work, int per_block) {
+  long long g = (work + per_block - 1) / per_block;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace bit
+
+struct bit_ctx {
+  bit::Ctx c;
+};
+struct bit_tree {
+  bit::Tree t;
+};

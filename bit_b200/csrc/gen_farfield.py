@@ -1,0 +1,265 @@
+"""Generate farfield_gen.cuh: unrolled far-field Taylor recurrences for nterms = 1..10.
+
+For every nterms and kernel this writes one straight-line device function that evaluates
+the Taylor coefficients of the cluster kernel degree by degree and folds each one into
+the moment dot product as soon as it exists, so only the last two degree shells stay live
+in registers.  The coefficient of each index pattern follows the reference's recurrence
+for that pattern (constants 1/k etc. folded into literals):
+
+  Coulomb potential   treetaylorpotential, src/tree3d.cpp:4484-4629  (sum: :4632-4638,
+                      to degree nterms-1)
+  screened potential  shielded_treetaylorpot, src/tree3d.cpp:3042-3214 (sum: :3219-3225)
+  Coulomb force       treetaylorforce, src/tree3d.cpp:472-612 (sum: :794-808)
+
+Usage: python gen_farfield.py <out.cuh>
+"""
+import sys
+
+AX = "xyz"
+
+
+def lit(v):
+    return f"T({float(v)!r})"
+
+
+def name(p, v):
+    return f"{p}{v[0]}_{v[1]}_{v[2]}"
+
+
+def sub(v, a, by):
+    w = list(v)
+    w[a] -= by
+    return tuple(w)
+
+
+def shells(maxdeg):
+    for d in range(maxdeg + 1):
+        for i in range(d, -1, -1):
+            for j in range(d - i, -1, -1):
+                yield (i, j, d - i - j)
+
+
+def moment_index(nt):
+    idx, out = 0, {}
+    for i in range(nt):
+        for j in range(nt - i):
+            for k in range(nt - i - j):
+                out[(i, j, k)] = idx
+                idx += 1
+    return out
+
+
+def classify(v):
+    nz = sum(1 for a in v if a == 0)
+    n1 = sum(1 for a in v if a == 1)
+    ax = [a for a in range(3) if v[a] > 0]
+    return nz, n1, ax
+
+
+# ---------------------------------------------------------------------------- Coulomb
+def coul_expr(v):
+    b = lambda w: name("b", w)
+    d = lambda a: "d" + AX[a]
+    d2 = lambda a: "d" + AX[a] + "2"
+    nz, n1, ax = classify(v)
+    if nz == 3:
+        return "sqfac"
+    if nz == 2:
+        u, k = ax[0], v[ax[0]]
+        if k == 1:
+            return f"fac*{d(u)}*sqfac"
+        ik = 1.0 / k
+        return f"fac*({lit(2.0 - ik)}*{d(u)}*{b(sub(v, u, 1))} - {lit(1 - ik)}*{b(sub(v, u, 2))})"
+    if nz == 1 and n1 == 2:
+        u, w = ax
+        return f"fac*({d(u)}*{b(sub(v, u, 1))} + {d2(w)}*{b(sub(v, w, 1))})"
+    if nz == 1 and n1 == 0:
+        u, w = ax
+        ii = 1.0 / v[u]
+        return (f"fac*({lit(2.0 - ii)}*{d(u)}*{b(sub(v, u, 1))} + {d2(w)}*{b(sub(v, w, 1))}"
+                f" - {lit(1 - ii)}*{b(sub(v, u, 2))} - {b(sub(v, w, 2))})")
+    if n1 >= 1:
+        f = next(a for a in range(3) if v[a] == 1)
+        s = f"{d(f)}*{b(sub(v, f, 1))}"
+        for a in range(3):
+            if a != f and v[a] > 0:
+                s += f" + {d2(a)}*{b(sub(v, a, 1))}"
+        for a in range(3):
+            if a != f and v[a] >= 2:
+                s += f" - {b(sub(v, a, 2))}"
+        return f"fac*({s})"
+    ii = 1.0 / v[0]
+    return (f"fac*({lit(2.0 * (1 - 0.5 * ii))}*dx*{b(sub(v, 0, 1))} + dy2*{b(sub(v, 1, 1))}"
+            f" + dz2*{b(sub(v, 2, 1))} - {lit(1.0 - ii)}*{b(sub(v, 0, 2))}"
+            f" - {b(sub(v, 1, 2))} - {b(sub(v, 2, 2))})")
+
+
+def gen_coulomb(nt):
+    mi = moment_index(nt)
+    L = ["  const T dx2 = T(2)*dx, dy2 = T(2)*dy, dz2 = T(2)*dz;",
+         "  const T fac = T(1) / rs;",
+         "  const T sqfac = sqrt_t(fac);",
+         "  T s = T(0);"]
+    for v in shells(nt - 1):
+        L.append(f"  const T {name('b', v)} = {coul_expr(v)};")
+        L.append(f"  s = fma_t(M[{mi[v]}], {name('b', v)}, s);")
+    L.append("  return s;")
+    return L
+
+
+# ---------------------------------------------------------------------------- screened
+def scr_expr(v):
+    a_ = lambda w: name("a", w)
+    b_ = lambda w: name("c", w)
+    d = lambda a: "d" + AX[a]
+    dd = lambda a: "d" + AX[a] + "2"
+    kd = lambda a: "kd" + AX[a]
+    nz, n1, ax = classify(v)
+    if nz == 2 and n1 == 1:
+        u = ax[0]
+        return (f"{kd(u)}*a0_0_0", f"fac*{d(u)}*(a0_0_0 + kappa*c0_0_0)")
+    if n1 == 0:
+        u = ax[0]
+        i = v[u]
+        cf1, cf2, cf3 = 1.0 / i, 1.0 - 1.0 / (2.0 * i), 1.0 - 1.0 / i
+        bexp = f"(kappa*{lit(cf1)})*({d(u)}*{a_(sub(v, u, 1))} - {a_(sub(v, u, 2))})"
+        s = f"{dd(u)}*{lit(cf2)}*{a_(sub(v, u, 1))}"
+        for a in ax[1:]:
+            s += f" + {dd(a)}*{a_(sub(v, a, 1))}"
+        s += f" - {lit(cf3)}*{a_(sub(v, u, 2))}"
+        for a in ax[1:]:
+            s += f" - {a_(sub(v, a, 2))}"
+        s += f" + (kappa*{lit(cf1)})*({d(u)}*{b_(sub(v, u, 1))} - {b_(sub(v, u, 2))})"
+        return (bexp, f"fac*({s})")
+    f = next(a for a in range(3) if v[a] == 1)
+    bexp = f"{kd(f)}*{a_(sub(v, f, 1))}"
+    s = f"{d(f)}*{a_(sub(v, f, 1))}"
+    for a in range(3):
+        if a != f and v[a] > 0:
+            s += f" + {dd(a)}*{a_(sub(v, a, 1))}"
+    for a in range(3):
+        if a != f and v[a] >= 2:
+            s += f" - {a_(sub(v, a, 2))}"
+    s += f" + {kd(f)}*{b_(sub(v, f, 1))}"
+    return (bexp, f"fac*({s})")
+
+
+def gen_screened(nt):
+    mi = moment_index(nt)
+    L = ["  const T dx2 = T(2)*dx, dy2 = T(2)*dy, dz2 = T(2)*dz;",
+         "  const T kdx = kappa*dx, kdy = kappa*dy, kdz = kappa*dz;",
+         "  const T rinv = rsqrt_t(dist2);",
+         "  const T fac = rinv * rinv;",
+         "  const T c0_0_0 = exp_t(-kappa * (dist2 * rinv));",
+         "  const T a0_0_0 = c0_0_0 * rinv;",
+         "  T s = T(0);",
+         f"  s = fma_t(M[0], a0_0_0, s);"]
+    for v in shells(nt - 1):
+        if v == (0, 0, 0):
+            continue
+        bexp, aexp = scr_expr(v)
+        L.append(f"  const T {name('c', v)} = {bexp};")
+        L.append(f"  const T {name('a', v)} = {aexp};")
+        L.append(f"  s = fma_t(M[{mi[v]}], {name('a', v)}, s);")
+    L.append("  return s;")
+    return L
+
+
+# ---------------------------------------------------------------------------- force
+def force_expr(v):
+    b = lambda w: name("b", w)
+    d = lambda a: "d" + AX[a]
+    nz, n1, ax = classify(v)
+    deg = sum(v)
+    if nz == 3:
+        return "sqfac"
+    if nz == 2:
+        u, k = ax[0], v[ax[0]]
+        if k == 1:
+            return f"-fac*{d(u)}*sqfac"
+        ik = 1.0 / k
+        return f"fac*({lit(ik - 2.0)}*{b(sub(v, u, 1))}*{d(u)} + {lit(ik - 1.0)}*{b(sub(v, u, 2))})"
+    if nz == 1 and n1 == 2:
+        u, w = ax
+        return f"{lit(-1.5)}*fac*({d(u)}*{b(sub(v, u, 1))} + {d(w)}*{b(sub(v, w, 1))})"
+    if nz == 1 and n1 == 1:
+        u, w = ax
+        k = deg - 1
+        g = u if v[u] >= 2 else w
+        return (f"(fac*{lit(1.0 / (k + 1))})*({lit(-2 * k - 1.0)}*({d(u)}*{b(sub(v, u, 1))} + "
+                f"{d(w)}*{b(sub(v, w, 1))}) + {lit(-k)}*{b(sub(v, g, 2))})")
+    if nz == 1:
+        u, w = ax
+        s = v[u] + v[w]
+        return (f"(fac*{lit(1.0 / s)})*({lit(1 - 2 * s)}*({d(u)}*{b(sub(v, u, 1))} + "
+                f"{d(w)}*{b(sub(v, w, 1))}) + {lit(1 - s)}*({b(sub(v, u, 2))} + {b(sub(v, w, 2))}))")
+    s3 = f"(dx*{b(sub(v, 0, 1))} + dy*{b(sub(v, 1, 1))} + dz*{b(sub(v, 2, 1))})"
+    if n1 == 3:
+        return f"(fac*{lit(-5.0 / 3.0)})*{s3}"
+    if n1 == 2:
+        w = next(a for a in range(3) if v[a] >= 2)
+        i = v[w]
+        return f"(fac*{lit(1.0 / (2.0 + i))})*({lit(-3.0 - 2 * i)}*{s3} + {lit(-1.0 - i)}*{b(sub(v, w, 2))})"
+    if n1 == 1:
+        f = next(a for a in range(3) if v[a] == 1)
+        u, w = [a for a in range(3) if a != f]
+        s = v[u] + v[w]
+        return (f"(fac*{lit(1.0 / (1 + s))})*({lit(-1.0 - 2 * s)}*{s3} + {lit(-s)}*"
+                f"({b(sub(v, u, 2))} + {b(sub(v, w, 2))}))")
+    s = deg
+    return (f"(fac*{lit(1.0 / s)})*({lit(1 - 2 * s)}*{s3} + {lit(1 - s)}*({b(sub(v, 0, 2))} + "
+            f"{b(sub(v, 1, 2))} + {b(sub(v, 2, 2))}))")
+
+
+def gen_force(nt):
+    """Field sum of treetaylorforce: returns (fx, fy, fz) through references."""
+    mi = moment_index(nt)
+    L = ["  const T fac = T(1) / rs;",
+         "  const T sqfac = sqrt_t(fac);",
+         "  T sx = T(0), sy = T(0), sz = T(0);"]
+    # coefficient (i,j,k) of degree d is consumed by moments of degree d-1
+    for v in shells(nt):
+        L.append(f"  const T {name('b', v)} = {force_expr(v)};")
+        d = sum(v)
+        if d == 0:
+            continue
+        for a, acc in ((0, "sx"), (1, "sy"), (2, "sz")):
+            if v[a] == 0:
+                continue
+            m = sub(v, a, 1)  # moment index (i, k, m) with this coefficient on axis a
+            if sum(m) >= nt:
+                continue
+            sign = 1.0 if (sum(m) + 1) % 2 == 0 else -1.0
+            coef = sign * (m[a] + 1)
+            L.append(f"  {acc} = fma_t(M[{mi[m]}] * {lit(coef)}, {name('b', v)}, {acc});")
+    L.append("  fx += sx; fy += sy; fz += sz;")
+    return L
+
+
+def main(out):
+    parts = ["// GENERATED by gen_farfield.py -- do not edit.",
+             "#pragma once",
+             "namespace bit {",
+             "template <int NT> struct FarField;"]
+    for nt in range(1, 11):
+        parts.append(f"template <> struct FarField<{nt}> {{")
+        parts.append("  template <class T> static __device__ __forceinline__ T coulomb("
+                     "T dx, T dy, T dz, T rs, const T* __restrict__ M) {")
+        parts += gen_coulomb(nt)
+        parts.append("  }")
+        parts.append("  template <class T> static __device__ __forceinline__ T screened("
+                     "T dx, T dy, T dz, T dist2, T kappa, const T* __restrict__ M) {")
+        parts += gen_screened(nt)
+        parts.append("  }")
+        parts.append("  template <class T> static __device__ __forceinline__ void force("
+                     "T dx, T dy, T dz, T rs, const T* __restrict__ M, T& fx, T& fy, T& fz) {")
+        parts += gen_force(nt)
+        parts.append("  }")
+        parts.append("};")
+    parts.append("}  // namespace bit")
+    with open(out, "w") as f:
+        f.write("\n".join(parts) + "\n")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1])

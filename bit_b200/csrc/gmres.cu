@@ -1,0 +1,495 @@
+// GMRES on the device.
+//
+// bit_bie_solve: restarted GMRES(m) for (diag*I + K) s = f where K is the treecode with
+// charges w*s (no reference counterpart: the reference's solver::gmres takes a dense
+// matrix, src/solver.h:157-260).  Vectors live in tree order on the device; each matvec
+// rewrites the charges, recomputes the moments (FP64) and runs the far and near kernels
+// over the interaction lists built once for the tree.  Arnoldi is classical Gram-Schmidt
+// applied twice (FP64 dot products and updates on the device); the (m+1) x m Hessenberg
+// and its Givens rotations are FP64 on the host.  Mixed precision: FP32 matvecs inside an
+// FP64 iterative refinement whose residual f - A s is always recomputed with the FP64
+// treecode.
+//
+// bit_gmres_dense: solver::gmres itself (src/solver.h:157-310) for a dense matrix:
+// full GMRES from zero, modified Gram-Schmidt, least squares by Gram-Schmidt QR of the
+// Hessenberg re-done every step (minimize, :266-310), stop when the max relative change
+// of x is below 1e-5 on odd steps (:243-255), breakdown at h < 1e-14 (:220-225).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+
+namespace bit {
+
+void ensure_lists_for(Tree* t, const bit_eval_params& p);
+
+namespace {
+
+constexpr int RB = 256;
+
+__global__ void k_gather(int n, const int* perm, const double* src, double* dst) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) dst[e] = src[perm[e]];
+}
+__global__ void k_scatter(int n, const int* perm, const double* src, double* dst) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) dst[perm[e]] = src[e];
+}
+
+// charges q = w * s in tree order, written into every source representation
+__global__ void k_charges(int n, const double* w, const double* s, double* sq, double4* src64,
+                          float4* src32) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double q = w[e] * s[e];
+  sq[e] = q;
+  src64[e].w = q;
+  src32[e].w = (float)q;
+}
+
+__global__ void k_axpby(int n, double a, const double* x, double b, double* y) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) y[e] = a * x[e] + b * y[e];
+}
+
+// Sum over the block, returned to every thread.
+__device__ double block_sum(double v) {
+  __shared__ double sh[33];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[32] = v;
+  }
+  __syncthreads();
+  v = sh[32];
+  __syncthreads();
+  return v;
+}
+
+// partial[j * nblk + b] = sum over block b's elements of V[j] . w, j < k
+__global__ void k_dots(int n, int k, const double* V, const double* w, double* partial) {
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  for (int j = 0; j < k; j++) {
+    double a = 0.0;
+    const double* v = V + (long long)j * n;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) a += v[i] * w[i];
+    a = block_sum(a);
+    if (threadIdx.x == 0) partial[j * gridDim.x + blockIdx.x] = a;
+  }
+}
+__global__ void k_dots_finish(int k, int nblk, const double* partial, double* h) {
+  int j = blockIdx.x;
+  if (j >= k) return;
+  double a = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) a += partial[j * nblk + b];
+  a = block_sum(a);
+  if (threadIdx.x == 0) h[j] = a;
+}
+// w -= sum_j h[j] V[j]
+__global__ void k_orth_update(int n, int k, const double* V, const double* h, double* w) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = w[i];
+  for (int j = 0; j < k; j++) a -= h[j] * V[(long long)j * n + i];
+  w[i] = a;
+}
+// x += sum_j y[j] V[j]
+__global__ void k_combine(int n, int k, const double* V, const double* y, double* x) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a = x[i];
+  for (int j = 0; j < k; j++) a += y[j] * V[(long long)j * n + i];
+  x[i] = a;
+}
+
+struct Krylov {
+  Ctx* c;
+  int n;
+  int nblk;
+  DBuf<double> partial, hdev;
+  double* hh;  // pinned
+  Krylov(Ctx* ctx, int n_, int maxk) : c(ctx), n(n_) {
+    nblk = std::min(2 * c->num_sms, std::max(1, n / 2048));
+    partial.ensure(c, (size_t)nblk * (maxk + 2));
+    hdev.ensure(c, maxk + 2);
+    BIT_CUDA(cudaMallocHost(&hh, (maxk + 2) * sizeof(double)));
+  }
+  ~Krylov() { cudaFreeHost(hh); }
+  // h[0..k) = V[0..k) . w on the host
+  void dots(const double* V, int k, const double* w) {
+    cudaStream_t s = c->stream;
+    count_launch(), k_dots<<<nblk, RB, 0, s>>>(n, k, V, w, partial.p);
+    count_launch(), k_dots_finish<<<k, RB, 0, s>>>(k, nblk, partial.p, hdev.p);
+    BIT_CUDA(cudaMemcpyAsync(hh, hdev.p, k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+  }
+  double norm(const double* w) {
+    dots(w, 1, w);
+    return std::sqrt(hh[0]);
+  }
+};
+
+struct BieOp {
+  Tree* t;
+  bit_eval_params prm;
+  int nterms;
+  double diag;
+  DBuf<double> w_s;
+  int mv64 = 0, mv32 = 0;
+  // y = diag*x + K(w*x), everything in tree order
+  void apply(const double* x, double* y, bit_precision prec) {
+    Ctx* c = t->ctx;
+    cudaStream_t s = c->stream;
+    const int n = t->n;
+    count_launch(), k_charges<<<grid_for(n, 256), 256, 0, s>>>(n, w_s.p, x, t->sq.p, t->src64.p, t->src32.p);
+    tree_moments(t, nterms);
+    bit_eval_params p = prm;
+    p.precision = prec;
+    ensure_lists_for(t, p);
+    eval_far(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, y);
+    eval_near(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, y);
+    count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, diag, x, 1.0, y);
+    BIT_CHECK_LAUNCH();
+    (prec == BIT_PREC_FP64 ? mv64 : mv32)++;
+  }
+};
+
+// Restarted GMRES(m) on A x = b from x (device, tree order) with matvecs in `prec`; stops
+// when the recurrence residual reaches tol*||b|| or after maxit iterations.  Returns the
+// iterations used.
+int gmres_m(BieOp& A, Krylov& K, const double* b, double* x, int m, double tol, int maxit,
+            bit_precision prec, double bnorm, bool x_is_zero) {
+  Ctx* c = A.t->ctx;
+  cudaStream_t s = c->stream;
+  const int n = A.t->n;
+  DBuf<double> V, w;
+  V.ensure(c, (size_t)(m + 1) * n);
+  w.ensure(c, n);
+  std::vector<double> H((m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 1);
+  int it = 0;
+  while (it < maxit) {
+    // r = b - A x
+    if (x_is_zero) {
+      BIT_CUDA(cudaMemcpyAsync(w.p, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else {
+      A.apply(x, w.p, prec);
+      count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, b, -1.0, w.p);
+    }
+    x_is_zero = false;
+    double beta = K.norm(w.p);
+    if (beta <= tol * bnorm || beta == 0.0) break;
+    count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0 / beta, w.p, 0.0, V.p);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    int k = 0;
+    bool done = false;
+    for (; k < m && it < maxit; k++) {
+      it++;
+      double* vk1 = V.p + (long long)(k + 1) * n;
+      A.apply(V.p + (long long)k * n, vk1, prec);
+      // classical Gram-Schmidt, twice
+      std::fill(hcol.begin(), hcol.end(), 0.0);
+      for (int pass = 0; pass < 2; pass++) {
+        K.dots(V.p, k + 1, vk1);
+        for (int j = 0; j <= k; j++) hcol[j] += K.hh[j];
+        count_launch(), k_orth_update<<<grid_for(n, 256), 256, 0, s>>>(n, k + 1, V.p, K.hdev.p, vk1);
+      }
+      double hn = K.norm(vk1);
+      hcol[k + 1] = hn;
+      if (hn > 0) count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0 / hn, vk1, 0.0, vk1);
+      for (int j = 0; j < k; j++) {
+        double a = hcol[j], bb = hcol[j + 1];
+        hcol[j] = cs[j] * a + sn[j] * bb;
+        hcol[j + 1] = -sn[j] * a + cs[j] * bb;
+      }
+      double den = std::hypot(hcol[k], hcol[k + 1]);
+      cs[k] = den > 0 ? hcol[k] / den : 1.0;
+      sn[k] = den > 0 ? hcol[k + 1] / den : 0.0;
+      hcol[k] = den;
+      hcol[k + 1] = 0.0;
+      for (int j = 0; j <= k; j++) H[j * m + k] = hcol[j];
+      g[k + 1] = -sn[k] * g[k];
+      g[k] = cs[k] * g[k];
+      if (std::fabs(g[k + 1]) <= tol * bnorm || hn == 0.0) {
+        k++;
+        done = true;
+        break;
+      }
+    }
+    for (int i = k - 1; i >= 0; i--) {
+      double a = g[i];
+      for (int j = i + 1; j < k; j++) a -= H[i * m + j] * y[j];
+      y[i] = a / H[i * m + i];
+    }
+    BIT_CUDA(cudaMemcpyAsync(K.hdev.p, y.data(), k * sizeof(double), cudaMemcpyHostToDevice, s));
+    count_launch(), k_combine<<<grid_for(n, 256), 256, 0, s>>>(n, k, V.p, K.hdev.p, x);
+    BIT_CHECK_LAUNCH();
+    if (done) break;
+  }
+  BIT_CUDA(cudaStreamSynchronize(s));
+  return it;
+}
+
+// ---- dense solver::gmres ---------------------------------------------------------------
+// v = A q (row-major n x n), one warp per row
+__global__ void k_dense_gemv(int n, const double* A, const double* q, double* v) {
+  const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const double* a = A + (long long)row * n;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += a[j] * q[j];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) v[row] = s;
+}
+
+// Modified Gram-Schmidt of v against Q[0..k) in one block; h[0..k) and h[k] = ||v||,
+// then Q[k] = v / h[k].  (src/solver.h:203-230)
+__global__ void k_dense_mgs(int n, int k, const double* Q, double* v, double* h, double* qk) {
+  for (int j = 0; j < k; j++) {
+    const double* q = Q + (long long)j * n;
+    double a = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a += q[i] * v[i];
+    a = block_sum(a);
+    if (threadIdx.x == 0) h[j] = a;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) v[i] -= a * q[i];
+    __syncthreads();
+  }
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) t += v[i] * v[i];
+  t = block_sum(t);
+  const double hn = sqrt(t);
+  if (threadIdx.x == 0) h[k] = hn;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) qk[i] = v[i] / hn;
+}
+
+// x = Q y and max_i |(old_i - x_i) / old_i|  (src/solver.h:243-255), one block
+__global__ void k_dense_update(int n, int k, const double* Q, const double* y, double* x,
+                               double* maxerr) {
+  __shared__ double sh[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double old = x[i], a = 0.0;
+    for (int j = 0; j < k; j++) a += Q[(long long)j * n + i] * y[j];
+    x[i] = a;
+    double e = fabs((old - a) / old);
+    if (e > m) m = e;
+  }
+  for (int o = 16; o; o >>= 1) {
+    double u = __shfl_xor_sync(0xffffffffu, m, o);
+    m = u > m ? u : m;
+  }
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = sh[w] > r ? sh[w] : r;
+    *maxerr = r;
+  }
+}
+
+}  // namespace
+
+void ensure_lists_for(Tree* t, const bit_eval_params& p) {
+  ListKey k = mac_key(p, t->gen, 0);
+  if (t->plists.valid && t->plists.key == k) return;
+  build_lists(t, &t->plists, k, t->n, t->sx.p, t->sy.p, t->sz.p, nullptr);
+}
+
+}  // namespace bit
+
+using namespace bit;
+
+namespace {
+template <class F>
+bit_status guard2(Ctx* c, F&& f) {
+  try {
+    f();
+    c->last_error.clear();
+    return BIT_OK;
+  } catch (const Error& e) {
+    c->last_error = e.msg;
+    return e.code;
+  } catch (...) {
+    c->last_error = "unexpected internal error";
+    return BIT_ERR_CUDA;
+  }
+}
+}  // namespace
+
+extern "C" bit_status bit_bie_solve(bit_tree* th, const bit_eval_params* prm, int nterms,
+                                    double diag, const double* w, const double* f, double* sol,
+                                    const bit_gmres_opts* opts, bit_gmres_info* info) {
+  if (!th || !prm || !w || !f || !sol || !opts) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  Ctx* c = t->ctx;
+  bit_status result = BIT_OK;
+  bit_status st = guard2(c, [&] {
+    if (opts->restart < 1 || opts->maxit < 1 || !(opts->tol > 0))
+      fail(BIT_ERR_INVALID_ARGUMENT, "restart, maxit and tol must be positive");
+    if (nterms < 1 || nterms > kNtermsMax) fail(BIT_ERR_INVALID_ARGUMENT, "nterms out of range");
+    BIT_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const int n = t->n;
+    cudaEvent_t e0, e1;
+    BIT_CUDA(cudaEventCreate(&e0));
+    BIT_CUDA(cudaEventCreate(&e1));
+    BIT_CUDA(cudaEventRecord(e0, s));
+    DBuf<double> tmp, b, x, r, d;
+    tmp.ensure(c, n); b.ensure(c, n); x.ensure(c, n); r.ensure(c, n); d.ensure(c, n);
+    BieOp A;
+    A.t = t;
+    A.prm = *prm;
+    A.nterms = nterms;
+    A.diag = diag;
+    A.w_s.ensure(c, n);
+    BIT_CUDA(cudaMemcpyAsync(tmp.p, w, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    count_launch(), k_gather<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, tmp.p, A.w_s.p);
+    BIT_CUDA(cudaMemcpyAsync(tmp.p, f, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    count_launch(), k_gather<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, tmp.p, b.p);
+    BIT_CUDA(cudaMemsetAsync(x.p, 0, n * sizeof(double), s));
+    if (!t->has_charges) {
+      // first use of this tree for a solve: create the source arrays
+      tree_set_charges(t, tmp.p, nullptr);
+    }
+    Krylov K(c, n, opts->restart + 1);
+    const double bnorm = K.norm(b.p);
+    int iters = 0, refine = 0;
+    double relres = 0.0;
+    if (bnorm == 0.0) {
+      relres = 0.0;
+    } else if (opts->precision == BIT_PREC_FP64) {
+      iters = gmres_m(A, K, b.p, x.p, opts->restart, opts->tol, opts->maxit, BIT_PREC_FP64,
+                      bnorm, true);
+      A.apply(x.p, r.p, BIT_PREC_FP64);
+      count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, b.p, -1.0, r.p);
+      relres = K.norm(r.p) / bnorm;
+    } else {
+      const double itol = opts->inner_tol > 0 ? opts->inner_tol : 1e-4;
+      const int maxref = opts->max_refinements > 0 ? opts->max_refinements : 10;
+      BIT_CUDA(cudaMemcpyAsync(r.p, b.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      relres = 1.0;
+      while (refine < maxref && iters < opts->maxit) {
+        // inner: A32 d = r to itol relative to ||r||
+        const double rn = K.norm(r.p);
+        BIT_CUDA(cudaMemsetAsync(d.p, 0, n * sizeof(double), s));
+        iters += gmres_m(A, K, r.p, d.p, opts->restart, itol, opts->maxit - iters,
+                         BIT_PREC_MIXED, rn, true);
+        count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, d.p, 1.0, x.p);
+        refine++;
+        // true residual with the FP64 treecode
+        A.apply(x.p, r.p, BIT_PREC_FP64);
+        count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, b.p, -1.0, r.p);
+        relres = K.norm(r.p) / bnorm;
+        if (relres <= opts->tol) break;
+      }
+    }
+    count_launch(), k_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, x.p, tmp.p);
+    BIT_CUDA(cudaMemcpyAsync(sol, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaEventRecord(e1, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (info) {
+      info->iterations = iters;
+      info->refinements = refine;
+      info->matvecs_fp64 = A.mv64;
+      info->matvecs_fp32 = A.mv32;
+      info->relres = relres;
+      info->seconds = ms * 1e-3;
+    }
+    if (!(relres <= opts->tol)) result = BIT_ERR_NOT_CONVERGED;
+  });
+  return st != BIT_OK ? st : result;
+}
+
+extern "C" bit_status bit_gmres_dense(bit_ctx* h, int n, const double* a, const double* b,
+                                      double* x, int* iterations) {
+  if (!h || !a || !b || !x || n < 1) return BIT_ERR_INVALID_ARGUMENT;
+  Ctx* c = &h->c;
+  bit_status result = BIT_OK;
+  bit_status st = guard2(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    DBuf<double> A, Q, v, hd, y, xd, me;
+    A.ensure(c, (size_t)n * n);
+    Q.ensure(c, (size_t)(n + 1) * n);
+    v.ensure(c, n);
+    hd.ensure(c, n + 2);
+    y.ensure(c, n + 1);
+    xd.ensure(c, n);
+    me.ensure(c, 1);
+    BIT_CUDA(cudaMemcpyAsync(A.p, a, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(xd.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    double bnorm = 0.0;
+    for (int i = 0; i < n; i++) bnorm += b[i] * b[i];
+    bnorm = std::sqrt(bnorm);
+    std::vector<double> q0(n);
+    for (int i = 0; i < n; i++) q0[i] = b[i] / bnorm;
+    BIT_CUDA(cudaMemcpyAsync(Q.p, q0.data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    // Hessenberg, host, h[i][j] with ld n+1
+    const int ld = n + 1;
+    std::vector<double> H((size_t)(n + 2) * ld, 0.0), V2, Q2, R2, yv(n + 1), hc(n + 2);
+    int go = 1, nn = 0;
+    while (go) {
+      const int n1 = nn + 1;
+      count_launch(), k_dense_gemv<<<grid_for(n, 8), 256, 0, s>>>(n, A.p, Q.p + (long long)nn * n, v.p);
+      count_launch(), k_dense_mgs<<<1, 1024, 0, s>>>(n, n1, Q.p, v.p, hd.p, Q.p + (long long)n1 * n);
+      BIT_CUDA(cudaMemcpyAsync(hc.data(), hd.p, (n1 + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
+      BIT_CUDA(cudaStreamSynchronize(s));
+      for (int j = 0; j <= n1; j++) H[(size_t)j * ld + nn] = hc[j];
+      if (n1 < n && hc[n1] < 1e-14) {
+        go = 0;
+        result = BIT_ERR_BREAKDOWN;
+      }
+      // minimize(n1): Gram-Schmidt QR of the (n1+1) x n1 Hessenberg, back substitution
+      const int m = n1;
+      V2.assign((size_t)(m + 1) * m, 0.0);
+      Q2.assign((size_t)(m + 1) * m, 0.0);
+      R2.assign((size_t)m * m, 0.0);
+      for (int j = 0; j < m; j++)
+        for (int i = 0; i < j + 2; i++) V2[(size_t)i * m + j] = H[(size_t)i * ld + j];
+      for (int i = 0; i < m; i++) {
+        const int ind = i + 2;
+        double rr = 0.0;
+        for (int k = 0; k < ind; k++) rr += V2[(size_t)k * m + i] * V2[(size_t)k * m + i];
+        rr = std::sqrt(rr);
+        R2[(size_t)i * m + i] = rr;
+        for (int k = 0; k < ind; k++) Q2[(size_t)k * m + i] = V2[(size_t)k * m + i] / rr;
+        for (int j = i + 1; j < m; j++) {
+          double r = 0.0;
+          for (int k = 0; k < ind; k++) r += Q2[(size_t)k * m + i] * V2[(size_t)k * m + j];
+          R2[(size_t)i * m + j] = r;
+          for (int k = 0; k < ind; k++) V2[(size_t)k * m + j] -= r * Q2[(size_t)k * m + i];
+        }
+      }
+      for (int i = m - 1; i > -1; i--) {
+        double t = bnorm * Q2[i];
+        for (int j = i + 1; j < m; j++) t -= R2[(size_t)i * m + j] * yv[j];
+        yv[i] = t / R2[(size_t)i * m + i];
+      }
+      if (n1 == n) go = 0;
+      if (n1 % 2 || !go) {
+        BIT_CUDA(cudaMemcpyAsync(y.p, yv.data(), n1 * sizeof(double), cudaMemcpyHostToDevice, s));
+        count_launch(), k_dense_update<<<1, 1024, 0, s>>>(n, n1, Q.p, y.p, xd.p, me.p);
+        double maxerr = 0.0;
+        BIT_CUDA(cudaMemcpyAsync(&maxerr, me.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+        BIT_CUDA(cudaStreamSynchronize(s));
+        if (maxerr < 1e-5 && nn > 1) go = 0;
+      }
+      nn++;
+    }
+    BIT_CUDA(cudaMemcpyAsync(x, xd.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    if (iterations) *iterations = nn;
+  });
+  return st != BIT_OK ? st : result;
+}

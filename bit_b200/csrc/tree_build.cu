@@ -1,0 +1,708 @@
+// GPU tree build: the reference's aspect-ratio bisection tree (treemake,
+// src/tree3d.cpp:1345-1551), level by level.
+//
+// Nodes of one level are consecutive indices [a, b); their children become [b, c) in
+// parent order, which is the reference's breadth-first numbering.  Inside a node the
+// reference runs a short sequential program of up to seven bisections (treedivide,
+// src/tree3d.cpp:1163-1304), each needing the member count and bounding box of both
+// halves of the slot it splits.  Here every node keeps the results of its completed
+// bisections; a one-thread-per-node "decide" kernel replays the program from the start
+// on those cached results until it reaches the first bisection it has no result for,
+// and a "pass" kernel over all members of the level's nodes computes that bisection's
+// counts and bounding boxes (block reduction + atomics; min/max are order independent,
+// so the result is exact).  Members carry a slot label; a final stable counting scatter
+// lays each node's children out contiguously in slot order, members in ascending
+// original index (the reference's member order).  Field arithmetic (midpoints, aspect
+// ratios, sqradius) is the reference's, with no FMA contraction.
+#include <algorithm>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace bit {
+
+namespace {
+
+constexpr int CH = 2048;  // members per chunk (one block)
+constexpr int TB = 256;   // threads per block
+
+__device__ __forceinline__ unsigned long long okey(double v) {
+  long long b = __double_as_longlong(v);
+  if (b == (long long)0x8000000000000000ULL) b = 0;  // -0.0 -> +0.0
+  return b >= 0 ? ((unsigned long long)b | 0x8000000000000000ULL) : ~(unsigned long long)b;
+}
+__device__ __forceinline__ double okey_inv(unsigned long long k) {
+  long long b = (k & 0x8000000000000000ULL) ? (long long)(k & 0x7FFFFFFFFFFFFFFFULL)
+                                            : (long long)(~k);
+  return __longlong_as_double(b);
+}
+
+// treeinit (src/tree3d.cpp:1045-1073)
+__device__ void box_fields(double* f, double x0, double x1, double y0, double y1, double z0,
+                           double z1) {
+  double x = dmul(0.5, dadd(x1, x0)), y = dmul(0.5, dadd(y1, y0)), z = dmul(0.5, dadd(z1, z0));
+  f[0] = x0; f[1] = x1; f[2] = y0; f[3] = y1; f[4] = z0; f[5] = z1;
+  f[6] = x; f[7] = y; f[8] = z;
+  f[9] = fabs(__ddiv_rn(dsub(x1, x0), dsub(y1, y0)));
+  f[10] = fabs(__ddiv_rn(dsub(x1, x0), dsub(z1, z0)));
+  f[11] = fabs(__ddiv_rn(dsub(y1, y0), dsub(z1, z0)));
+  x = dsub(x1, x); y = dsub(y1, y); z = dsub(z1, z);
+  f[12] = dadd(dadd(dmul(x, x), dmul(y, y)), dmul(z, z));
+}
+
+struct Divide {
+  int dir, src, c1, c2;  // src -1: the node itself
+  double mid;
+};
+
+struct SplitState {
+  int active, finished, ndone, has_cur, has_prev, nchild, prev_c2eff, pad;
+  Divide cur, prev;
+  int res_cnt[7][2];
+  double res_bb[7][2][6];
+  int order[8];
+  int slot_n[8];
+  double slot_f[8][13];
+};
+
+struct SplitAcc {
+  int cnt[2];
+  unsigned long long mn[2][3], mx[2][3];
+};
+
+__device__ void acc_reset(SplitAcc* a) {
+  for (int h = 0; h < 2; h++) {
+    a->cnt[h] = 0;
+    for (int d = 0; d < 3; d++) { a->mn[h][d] = ~0ULL; a->mx[h][d] = 0ULL; }
+  }
+}
+
+// Replay of the split program on cached bisection results.
+struct Replay {
+  SplitState* S;
+  const double* pf;
+  int maxmemb;
+  double lim;
+  int d;
+  bool need;
+  int n[8];
+  double f[8][13];
+};
+
+__device__ int rp_bisect(Replay& r, int dir, int src, int c1, int c2) {
+  if (r.need) return 0;
+  const double* f = src < 0 ? r.pf : r.f[src];
+  if (r.d >= r.S->ndone) {
+    r.S->cur.dir = dir; r.S->cur.src = src; r.S->cur.c1 = c1; r.S->cur.c2 = c2;
+    r.S->cur.mid = f[6 + dir];
+    r.need = true;
+    return 0;
+  }
+  const int* cnt = r.S->res_cnt[r.d];
+  int dst[2] = {c1, cnt[0] > 0 ? c2 : c1};
+  int made = 0;
+  for (int h = 0; h < 2; h++) {
+    if (!cnt[h]) continue;
+    const double* bb = r.S->res_bb[r.d][h];
+    r.n[dst[h]] = cnt[h];
+    box_fields(r.f[dst[h]], bb[0], bb[1], bb[2], bb[3], bb[4], bb[5]);
+    made++;
+  }
+  r.d++;
+  return made;
+}
+
+__device__ __forceinline__ bool zsplit_ok(const Replay& r, int s) {
+  return r.f[s][10] < r.lim && r.f[s][11] < r.lim && r.n[s] > r.maxmemb;
+}
+
+// treemake's per-node program (src/tree3d.cpp:1412-1545) on slots relative to the first
+// free node index.  Returns nchild; order[] receives the children in recorded order.
+__device__ int split_program(Replay& r, int* order) {
+  const double lim = r.lim;
+  const double* P = r.pf;
+  int nchild = 0, nchild2 = 0, ind2;
+  for (int s = 0; s < 8; s++) r.n[s] = 0;
+  if (P[9] > lim && P[10] > lim) {
+    int xc = rp_bisect(r, 0, -1, 0, 1);
+    ind2 = xc;
+    for (int j = 0; j < xc; j++) {
+      order[nchild++] = j;
+      if (r.f[j][9] < lim && r.f[j][11] > lim && r.n[j] > r.maxmemb) {
+        int yc = rp_bisect(r, 1, j, j, ind2);
+        if (yc == 2) { order[nchild++] = ind2; ind2++; }
+        for (int k = 0; k < yc; k++) {
+          // the reference's numtree+j+k*(nchild2+1) (src/tree3d.cpp:1460), as written
+          int t = j + k * (nchild2 + 1);
+          if (t >= 8 || t >= ind2) continue;  // never-created slot: nummemb == 0
+          if (zsplit_ok(r, t)) {
+            int zc = rp_bisect(r, 2, t, t, ind2);
+            if (zc == 2) { order[nchild++] = ind2; nchild2++; ind2++; }
+          }
+        }
+      } else if (zsplit_ok(r, j)) {
+        int zc = rp_bisect(r, 2, j, j, ind2);
+        if (zc == 2) { order[nchild++] = ind2; ind2++; }
+      }
+    }
+  } else if (P[9] < lim && P[11] > lim) {
+    int yc = rp_bisect(r, 1, -1, 0, 1);
+    ind2 = yc;
+    for (int j = 0; j < yc; j++) {
+      order[nchild++] = j;
+      if (zsplit_ok(r, j)) {
+        int zc = rp_bisect(r, 2, j, j, ind2);
+        if (zc == 2) { order[nchild++] = ind2; ind2++; }
+      }
+    }
+  } else {
+    int zc = rp_bisect(r, 2, -1, 0, 1);
+    for (int j = 0; j < zc; j++) order[nchild++] = j;
+  }
+  return nchild;
+}
+
+__global__ void k_iota(int* p, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = i;
+}
+
+template <class T>
+__device__ __forceinline__ T warp_min(T v) {
+  for (int o = 16; o; o >>= 1) { T w = __shfl_xor_sync(0xffffffffu, v, o); v = w < v ? w : v; }
+  return v;
+}
+template <class T>
+__device__ __forceinline__ T warp_max(T v) {
+  for (int o = 16; o; o >>= 1) { T w = __shfl_xor_sync(0xffffffffu, v, o); v = w > v ? w : v; }
+  return v;
+}
+__device__ __forceinline__ int warp_sum(int v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Bounding box of all particles (the root, src/tree3d.cpp:1385-1403); flags NaNs.
+__global__ void k_root_bbox(int n, const double* x, const double* y, const double* z,
+                            SplitAcc* acc, int* err) {
+  unsigned long long mn[3] = {~0ULL, ~0ULL, ~0ULL}, mx[3] = {0, 0, 0};
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v[3] = {x[i], y[i], z[i]};
+    for (int d = 0; d < 3; d++) {
+      if (isnan(v[d])) bad = 1;
+      unsigned long long k = okey(v[d]);
+      mn[d] = k < mn[d] ? k : mn[d];
+      mx[d] = k > mx[d] ? k : mx[d];
+    }
+  }
+  for (int d = 0; d < 3; d++) {
+    mn[d] = warp_min(mn[d]);
+    mx[d] = warp_max(mx[d]);
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  if ((threadIdx.x & 31) == 0) {
+    for (int d = 0; d < 3; d++) {
+      atomicMin(&acc->mn[0][d], mn[d]);
+      atomicMax(&acc->mx[0][d], mx[d]);
+    }
+    if (bad) atomicOr(err, 1);
+  }
+}
+
+__global__ void k_acc_reset(SplitAcc* acc, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc_reset(&acc[i]);
+}
+
+__global__ void k_root_init(int n, const SplitAcc* acc, int* nummemb, int* start, int* children,
+                            int* level, int* parent, double* fields) {
+  double f[13];
+  box_fields(f, okey_inv(acc->mn[0][0]), okey_inv(acc->mx[0][0]), okey_inv(acc->mn[0][1]),
+             okey_inv(acc->mx[0][1]), okey_inv(acc->mn[0][2]), okey_inv(acc->mx[0][2]));
+  for (int k = 0; k < 13; k++) fields[k] = f[k];
+  nummemb[0] = n; start[0] = 0; level[0] = 0; parent[0] = -1;
+  for (int c = 0; c < 8; c++) children[c] = -1;
+}
+
+// Per level node: active flag and the number of member chunks it needs.
+__global__ void k_level_init(int a, int nlev, const int* nummemb, int maxmemb, SplitState* st,
+                             SplitAcc* acc, int* nchunk) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= nlev) return;
+  SplitState* S = &st[li];
+  int cnt = nummemb[a + li];
+  S->active = cnt > maxmemb;
+  S->finished = 0; S->ndone = 0; S->has_cur = 0; S->has_prev = 0; S->nchild = 0;
+  acc_reset(&acc[li]);
+  nchunk[li] = S->active ? (cnt + CH - 1) / CH : 0;
+}
+
+// Exclusive scan of a small int array in one block; total in out[n].
+__global__ void k_scan_small(const int* in, int* out, int n) {
+  __shared__ int ws[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < n; base += blockDim.x) {
+    int i = base + threadIdx.x;
+    int v = i < n ? in[i] : 0;
+    int s = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += t;
+    }
+    if (lane == 31) ws[w] = s;
+    __syncthreads();
+    if (w == 0) {
+      int t = lane < nw ? ws[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        int u = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += u;
+      }
+      if (lane < nw) ws[lane] = t;
+    }
+    __syncthreads();
+    int pre = carry + (w ? ws[w - 1] : 0) + s - v;
+    if (i < n) out[i] = pre;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = pre + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+__global__ void k_fill_chunks(int a, int nlev, const int* start, const int* nummemb,
+                              const int* cbeg, int2* chunks) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= nlev) return;
+  int s = start[a + li];
+  for (int c = cbeg[li]; c < cbeg[li + 1]; c++) chunks[c] = make_int2(li, s + (c - cbeg[li]) * CH);
+}
+
+__global__ void k_split_decide(int a, int nlev, const double* fields, SplitState* st,
+                               SplitAcc* acc, int maxmemb, double lim, int* err) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= nlev) return;
+  SplitState* S = &st[li];
+  if (!S->active) return;
+  SplitAcc* A = &acc[li];
+  if (S->has_cur) {
+    int d = S->ndone;
+    for (int h = 0; h < 2; h++) {
+      S->res_cnt[d][h] = A->cnt[h];
+      for (int q = 0; q < 3; q++) {
+        S->res_bb[d][h][2 * q] = okey_inv(A->mn[h][q]);
+        S->res_bb[d][h][2 * q + 1] = okey_inv(A->mx[h][q]);
+      }
+    }
+    S->ndone = d + 1;
+    S->prev = S->cur;
+    S->prev_c2eff = A->cnt[0] > 0 ? S->cur.c2 : S->cur.c1;
+    S->has_prev = 1;
+    S->has_cur = 0;
+    acc_reset(A);
+  } else {
+    S->has_prev = 0;
+  }
+  if (S->finished) return;
+  Replay r;
+  r.S = S; r.pf = fields + 13 * (long long)(a + li); r.maxmemb = maxmemb; r.lim = lim;
+  r.d = 0; r.need = false;
+  int order[8];
+  int nchild = split_program(r, order);
+  if (r.need) {
+    S->has_cur = 1;
+    if (S->ndone >= 7) atomicOr(err, 4);  // cannot happen: at most 7 bisections per node
+    return;
+  }
+  S->finished = 1;
+  S->nchild = nchild;
+  for (int c = 0; c < 8; c++) S->order[c] = c < nchild ? order[c] : -1;
+  for (int s = 0; s < 8; s++) {
+    S->slot_n[s] = s < nchild ? r.n[s] : 0;
+    if (s < nchild)
+      for (int k = 0; k < 13; k++) S->slot_f[s][k] = r.f[s][k];
+  }
+  if (nchild < 2) atomicOr(err, 2);  // one child == the node itself: never terminates
+}
+
+__device__ __forceinline__ double coord(int dir, const double* sx, const double* sy,
+                                        const double* sz, int e) {
+  return dir == 0 ? sx[e] : (dir == 1 ? sy[e] : sz[e]);
+}
+
+// One bisection step for every active node of the level: apply the previous step's
+// relabel, then reduce counts / bounding boxes of both halves of the current step.
+__global__ void __launch_bounds__(TB) k_split_pass(const int2* chunks, int a, const int* start,
+                                                   const int* nummemb, const double* sx,
+                                                   const double* sy, const double* sz,
+                                                   signed char* lab, const SplitState* st,
+                                                   SplitAcc* acc) {
+  const int2 ck = chunks[blockIdx.x];
+  const SplitState* S = &st[ck.x];
+  const int hp = S->has_prev, hc = S->has_cur;
+  if (!hp && !hc) return;
+  const Divide pv = S->prev, cu = S->cur;
+  const int pc2 = S->prev_c2eff;
+  const int node = a + ck.x;
+  const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
+  int cnt[2] = {0, 0};
+  unsigned long long mn[2][3], mx[2][3];
+  for (int h = 0; h < 2; h++)
+    for (int d = 0; d < 3; d++) { mn[h][d] = ~0ULL; mx[h][d] = 0ULL; }
+  for (int e = ck.y + threadIdx.x; e < e1; e += TB) {
+    int l = lab[e];
+    if (hp && l == pv.src) {
+      l = (coord(pv.dir, sx, sy, sz, e) <= pv.mid) ? pv.c1 : pc2;
+      lab[e] = (signed char)l;
+    }
+    if (hc && l == cu.src) {
+      int h = (coord(cu.dir, sx, sy, sz, e) <= cu.mid) ? 0 : 1;
+      double v[3] = {sx[e], sy[e], sz[e]};
+      cnt[h]++;
+      for (int d = 0; d < 3; d++) {
+        unsigned long long k = okey(v[d]);
+        mn[h][d] = k < mn[h][d] ? k : mn[h][d];
+        mx[h][d] = k > mx[h][d] ? k : mx[h][d];
+      }
+    }
+  }
+  if (!hc) return;
+  __shared__ int s_cnt[2];
+  if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int h = 0; h < 2; h++) {
+    int c = warp_sum(cnt[h]);
+    unsigned long long m[3], M[3];
+    for (int d = 0; d < 3; d++) { m[d] = warp_min(mn[h][d]); M[d] = warp_max(mx[h][d]); }
+    if ((threadIdx.x & 31) == 0 && c > 0) {
+      atomicAdd(&s_cnt[h], c);
+      for (int d = 0; d < 3; d++) {
+        atomicMin(&acc[ck.x].mn[h][d], m[d]);
+        atomicMax(&acc[ck.x].mx[h][d], M[d]);
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 && s_cnt[threadIdx.x]) atomicAdd(&acc[ck.x].cnt[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+__global__ void k_scatter_count(const int2* chunks, int a, const int* start, const int* nummemb,
+                                const signed char* lab, int* cc) {
+  const int2 ck = chunks[blockIdx.x];
+  const int node = a + ck.x;
+  const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
+  __shared__ int s[8];
+  if (threadIdx.x < 8) s[threadIdx.x] = 0;
+  __syncthreads();
+  int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int e = ck.y + threadIdx.x; e < e1; e += TB) {
+    int l = lab[e];
+#pragma unroll
+    for (int v = 0; v < 8; v++) c[v] += (l == v);
+  }
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    int t = warp_sum(c[v]);
+    if ((threadIdx.x & 31) == 0 && t) atomicAdd(&s[v], t);
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) cc[blockIdx.x * 8 + threadIdx.x] = s[threadIdx.x];
+}
+
+// Per node: destination offset of each chunk's members of each child slot.
+__global__ void k_scatter_offsets(int a, int nlev, const int* start, const int* cbeg,
+                                  const int* cc, int* coff, const SplitState* st, int* err) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= nlev) return;
+  const SplitState* S = &st[li];
+  if (!S->active) return;
+  int base[8], run[8];
+  int s0 = start[a + li], acc = 0;
+  for (int v = 0; v < 8; v++) { base[v] = acc; acc += S->slot_n[v]; run[v] = 0; }
+  for (int c = cbeg[li]; c < cbeg[li + 1]; c++)
+    for (int v = 0; v < 8; v++) {
+      coff[c * 8 + v] = s0 + base[v] + run[v];
+      run[v] += cc[c * 8 + v];
+    }
+  for (int v = 0; v < 8; v++)
+    if (run[v] != S->slot_n[v]) atomicOr(err, 8);
+}
+
+// Stable scatter of each chunk's members to their child's range (order kept).
+__global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, int a, const int* start,
+                                                const int* nummemb, const signed char* lab,
+                                                const int* coff, const int* perm,
+                                                const double* sx, const double* sy,
+                                                const double* sz, int* perm2, double* sx2,
+                                                double* sy2, double* sz2) {
+  const int2 ck = chunks[blockIdx.x];
+  const int node = a + ck.x;
+  const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
+  __shared__ int wcnt[TB / 32][8];
+  __shared__ int run[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x < 8) run[threadIdx.x] = coff[blockIdx.x * 8 + threadIdx.x];
+  __syncthreads();
+  const unsigned lt = (1u << lane) - 1u;
+  for (int t0 = ck.y; t0 < e1; t0 += TB) {
+    int e = t0 + threadIdx.x;
+    int l = e < e1 ? lab[e] : -2;
+    int my_rank = 0;
+    for (int v = 0; v < 8; v++) {
+      unsigned m = __ballot_sync(0xffffffffu, l == v);
+      if (l == v) my_rank = __popc(m & lt);
+      if (lane == 0) wcnt[w][v] = __popc(m);
+    }
+    __syncthreads();
+    if (l >= 0) {
+      int dst = run[l] + my_rank;
+      for (int q = 0; q < w; q++) dst += wcnt[q][l];
+      perm2[dst] = perm[e];
+      sx2[dst] = sx[e];
+      sy2[dst] = sy[e];
+      sz2[dst] = sz[e];
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+      int tot = 0;
+      for (int q = 0; q < TB / 32; q++) tot += wcnt[q][threadIdx.x];
+      run[threadIdx.x] += tot;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_copy_back(const int2* chunks, int a, const int* start, const int* nummemb,
+                            const int* perm2, const double* sx2, const double* sy2,
+                            const double* sz2, int* perm, double* sx, double* sy, double* sz) {
+  const int2 ck = chunks[blockIdx.x];
+  const int node = a + ck.x;
+  const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
+  for (int e = ck.y + threadIdx.x; e < e1; e += TB) {
+    perm[e] = perm2[e]; sx[e] = sx2[e]; sy[e] = sy2[e]; sz[e] = sz2[e];
+  }
+}
+
+__global__ void k_child_counts(int nlev, const SplitState* st, int* nch) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li < nlev) nch[li] = st[li].active ? st[li].nchild : 0;
+}
+
+__global__ void k_make_children(int a, int b, int nlev, const SplitState* st, const int* cscan,
+                                int* nummemb, int* start, int* children, int* level,
+                                int* parent, double* fields) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li >= nlev) return;
+  const SplitState* S = &st[li];
+  if (!S->active) return;
+  const int p = a + li, base = b + cscan[li];
+  int off = start[p];
+  for (int s = 0; s < S->nchild; s++) {
+    int node = base + s;
+    nummemb[node] = S->slot_n[s];
+    start[node] = off;
+    off += S->slot_n[s];
+    level[node] = level[p] + 1;
+    parent[node] = p;
+    for (int k = 0; k < 13; k++) fields[13LL * node + k] = S->slot_f[s][k];
+    for (int c = 0; c < 8; c++) children[8LL * node + c] = -1;
+  }
+  for (int c = 0; c < 8; c++) children[8LL * p + c] = c < S->nchild ? base + S->order[c] : -1;
+}
+
+__global__ void k_node_centres(int numtree, const double* fields, double4* nodec) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < numtree) {
+    const double* f = fields + 13LL * i;
+    nodec[i] = make_double4(f[6], f[7], f[8], f[12]);
+  }
+}
+
+__global__ void k_leaf_of(int nleaves, const int* leaves, const int* start, const int* nummemb,
+                          int* leaf_of) {
+  int l = blockIdx.x;
+  if (l >= nleaves) return;
+  int node = leaves[l];
+  for (int e = start[node] + threadIdx.x; e < start[node] + nummemb[node]; e += blockDim.x)
+    leaf_of[e] = node;
+}
+
+__global__ void k_iperm(int n, const int* perm, int* iperm) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) iperm[perm[e]] = e;
+}
+
+}  // namespace
+
+template <class T>
+void DBuf<T>::grow(Ctx* ctx, size_t count, size_t keep, cudaStream_t s) {
+  if (count <= n && p) return;
+  T* q = static_cast<T*>(dev_alloc(ctx, count * sizeof(T)));
+  if (p && keep) BIT_CUDA(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  BIT_CUDA(cudaStreamSynchronize(s));
+  release();
+  p = q;
+  n = count;
+  c = ctx;
+}
+template struct DBuf<int>;
+template struct DBuf<double>;
+
+void tree_build(Tree* t, const double* x, const double* y, const double* z) {
+  Ctx* c = t->ctx;
+  cudaStream_t s = c->stream;
+  const int n = t->n;
+  t->perm.ensure(c, n);
+  t->sx.ensure(c, n); t->sy.ensure(c, n); t->sz.ensure(c, n);
+  DBuf<int> perm2; DBuf<double> sx2, sy2, sz2;
+  perm2.ensure(c, n); sx2.ensure(c, n); sy2.ensure(c, n); sz2.ensure(c, n);
+  DBuf<signed char> lab;
+  lab.ensure(c, n);
+  int cap = std::max(64, 16 * (n / std::max(t->maxmemb, 1) + 1) + 64);
+  t->nummemb.ensure(c, cap); t->start.ensure(c, cap); t->level.ensure(c, cap);
+  t->parent.ensure(c, cap); t->children.ensure(c, 8LL * cap); t->fields.ensure(c, 13LL * cap);
+  DBuf<int> err;
+  err.ensure(c, 4);
+  BIT_CUDA(cudaMemsetAsync(err.p, 0, 4 * sizeof(int), s));
+  long long* hp = c->h_pinned;
+
+  count_launch(), k_iota<<<grid_for(n, 256), 256, 0, s>>>(t->perm.p, n);
+  BIT_CUDA(cudaMemcpyAsync(t->sx.p, x, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  BIT_CUDA(cudaMemcpyAsync(t->sy.p, y, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  BIT_CUDA(cudaMemcpyAsync(t->sz.p, z, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  BIT_CUDA(cudaMemsetAsync(lab.p, -1, n, s));
+
+  DBuf<SplitAcc> acc;
+  acc.ensure(c, 1);
+  count_launch(), k_acc_reset<<<1, 32, 0, s>>>(acc.p, 1);
+  count_launch(), k_root_bbox<<<std::min<unsigned>(grid_for(n, 256), 4 * c->num_sms), 256, 0, s>>>(
+      n, t->sx.p, t->sy.p, t->sz.p, acc.p, err.p);
+  count_launch(), k_root_init<<<1, 1, 0, s>>>(n, acc.p, t->nummemb.p, t->start.p, t->children.p, t->level.p,
+                             t->parent.p, t->fields.p);
+  BIT_CHECK_LAUNCH();
+
+  const double lim = 1.0 / std::sqrt(2.0);  // src/tree3d.cpp:1371
+  DBuf<SplitState> st;
+  DBuf<int> nchunk, cbeg, cc, coff, nch, cscan;
+  DBuf<int2> chunks;
+  int a = 0, b = 1, depth = 1;
+  while (true) {
+    const int nlev = b - a;
+    st.ensure(c, nlev);
+    acc.ensure(c, nlev);
+    nchunk.ensure(c, nlev);
+    cbeg.ensure(c, nlev + 1);
+    nch.ensure(c, nlev);
+    cscan.ensure(c, nlev + 1);
+    const unsigned gl = grid_for(nlev, 128);
+    count_launch(), k_level_init<<<gl, 128, 0, s>>>(a, nlev, t->nummemb.p, t->maxmemb, st.p, acc.p, nchunk.p);
+    count_launch(), k_scan_small<<<1, 1024, 0, s>>>(nchunk.p, cbeg.p, nlev);
+    BIT_CUDA(cudaMemcpyAsync(hp, cbeg.p + nlev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    const int nch_total = *reinterpret_cast<int*>(hp);
+    if (nch_total == 0) break;
+    chunks.ensure(c, nch_total);
+    cc.ensure(c, 8LL * nch_total);
+    coff.ensure(c, 8LL * nch_total);
+    count_launch(), k_fill_chunks<<<gl, 128, 0, s>>>(a, nlev, t->start.p, t->nummemb.p, cbeg.p, chunks.p);
+    count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, st.p, acc.p, t->maxmemb, lim, err.p);
+    for (int step = 0; step < 7; step++) {
+      count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
+                                            t->sy.p, t->sz.p, lab.p, st.p, acc.p);
+      count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, st.p, acc.p, t->maxmemb, lim,
+                                        err.p);
+    }
+    count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
+                                          t->sy.p, t->sz.p, lab.p, st.p, acc.p);
+    count_launch(), k_scatter_count<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, cc.p);
+    count_launch(), k_scatter_offsets<<<gl, 128, 0, s>>>(a, nlev, t->start.p, cbeg.p, cc.p, coff.p, st.p, err.p);
+    count_launch(), k_scatter<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, coff.p,
+                                       t->perm.p, t->sx.p, t->sy.p, t->sz.p, perm2.p, sx2.p,
+                                       sy2.p, sz2.p);
+    count_launch(), k_copy_back<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, perm2.p, sx2.p,
+                                         sy2.p, sz2.p, t->perm.p, t->sx.p, t->sy.p, t->sz.p);
+    // the next level's members start unlabelled
+    BIT_CUDA(cudaMemsetAsync(lab.p, -1, n, s));
+    count_launch(), k_child_counts<<<gl, 128, 0, s>>>(nlev, st.p, nch.p);
+    count_launch(), k_scan_small<<<1, 1024, 0, s>>>(nch.p, cscan.p, nlev);
+    BIT_CUDA(cudaMemcpyAsync(hp, cscan.p + nlev, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(hp + 1, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    const int total = *reinterpret_cast<int*>(hp);
+    const int e = *reinterpret_cast<int*>(hp + 1);
+    if (e & 1) fail(BIT_ERR_INVALID_ARGUMENT, "particle coordinates contain NaN");
+    if (e & 2)
+      fail(BIT_ERR_DEGENERATE,
+           "a node with more than maxmemb members cannot be split (coincident particles); "
+           "the reference's treemake would not terminate");
+    if (e & 12) fail(BIT_ERR_CUDA, "internal tree-build consistency check failed");
+    if (total == 0) break;
+    if (b + total > cap) {
+      int ncap = std::max(2 * cap, b + total + 64);
+      t->nummemb.grow(c, ncap, b, s); t->start.grow(c, ncap, b, s);
+      t->level.grow(c, ncap, b, s); t->parent.grow(c, ncap, b, s);
+      t->children.grow(c, 8LL * ncap, 8LL * b, s); t->fields.grow(c, 13LL * ncap, 13LL * b, s);
+      cap = ncap;
+    }
+    count_launch(), k_make_children<<<gl, 128, 0, s>>>(a, b, nlev, st.p, cscan.p, t->nummemb.p, t->start.p,
+                                       t->children.p, t->level.p, t->parent.p, t->fields.p);
+    BIT_CHECK_LAUNCH();
+    a = b;
+    b += total;
+    depth++;
+  }
+  {
+    // the root alone (n <= maxmemb) still has to report NaNs
+    BIT_CUDA(cudaMemcpyAsync(hp + 1, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    if (*reinterpret_cast<int*>(hp + 1) & 1)
+      fail(BIT_ERR_INVALID_ARGUMENT, "particle coordinates contain NaN");
+  }
+  t->numtree = b;
+  t->depth = depth;
+  t->cap = cap;
+  t->nodec.ensure(c, b);
+  count_launch(), k_node_centres<<<grid_for(b, 128), 128, 0, s>>>(b, t->fields.p, t->nodec.p);
+  tree_sync_host(t);
+  // leaves in node order
+  std::vector<int> leaves;
+  for (int i = 0; i < b; i++)
+    if (t->h_children[8LL * i] == -1) leaves.push_back(i);
+  t->nleaves = (int)leaves.size();
+  t->leaves.ensure(c, leaves.size());
+  BIT_CUDA(cudaMemcpyAsync(t->leaves.p, leaves.data(), leaves.size() * sizeof(int),
+                           cudaMemcpyHostToDevice, s));
+  t->leaf_of.ensure(c, n);
+  count_launch(), k_leaf_of<<<t->nleaves, 256, 0, s>>>(t->nleaves, t->leaves.p, t->start.p, t->nummemb.p,
+                                       t->leaf_of.p);
+  t->iperm.ensure(c, n);
+  count_launch(), k_iperm<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->iperm.p);
+  BIT_CHECK_LAUNCH();
+  BIT_CUDA(cudaStreamSynchronize(s));
+  t->gen++;
+  t->has_moments = false;
+  t->plists.valid = false;
+}
+
+template struct DBuf<signed char>;
+template struct DBuf<SplitState>;
+template struct DBuf<SplitAcc>;
+template struct DBuf<int2>;
+
+void tree_sync_host(Tree* t) {
+  cudaStream_t s = t->ctx->stream;
+  const int b = t->numtree;
+  t->h_nummemb.resize(b); t->h_start.resize(b); t->h_children.resize(8LL * b);
+  t->h_level.resize(b); t->h_fields.resize(13LL * b);
+  BIT_CUDA(cudaMemcpyAsync(t->h_nummemb.data(), t->nummemb.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(t->h_start.data(), t->start.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(t->h_children.data(), t->children.p, 8LL * b * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(t->h_level.data(), t->level.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(t->h_fields.data(), t->fields.p, 13LL * b * sizeof(double), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace bit

@@ -1,0 +1,200 @@
+/*
+ * bit_b200.h -- C ABI of the B200-native BIT treecode.
+ *
+ * Plain C types only (pointers, sizes, enums, POD structs); no CUDA or C++ types cross
+ * this boundary.  Every entry point returns a bit_status; none aborts or throws.  A
+ * context owns one CUDA stream on one device and is not thread-safe: use one context per
+ * host thread.  Trees are owned by the context that built them and keep their device
+ * memory (particles, nodes, moments, interaction lists) resident until destroyed.
+ *
+ * Each entry point names the reference (ongbw/bit) interface it replaces, as file:line.
+ */
+#ifndef BIT_B200_H
+#define BIT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BIT_ABI_VERSION 1
+#define BIT_NTERMS_MAX 10 /* nterms = p + 1; the reference caps it via MAXTERM=12 (src/constants.h:10) */
+
+typedef struct bit_ctx bit_ctx;
+typedef struct bit_tree bit_tree;
+
+typedef enum {
+  BIT_OK = 0,
+  BIT_ERR_INVALID_ARGUMENT = 1,
+  BIT_ERR_CUDA = 2,
+  BIT_ERR_OUT_OF_MEMORY = 3,
+  BIT_ERR_CAPACITY = 4,     /* a node / list / stack capacity was exceeded              */
+  BIT_ERR_DEGENERATE = 5,   /* > maxmemb coincident particles: the reference loops forever */
+  BIT_ERR_BREAKDOWN = 6,    /* GMRES breakdown (src/solver.h:220-225)                    */
+  BIT_ERR_NOT_CONVERGED = 7,
+  BIT_ERR_NO_DEVICE = 8,
+  BIT_ERR_BUDGET = 9,       /* the request does not fit the context's HBM budget         */
+  BIT_ERR_STATE = 10        /* call order violated (e.g. evaluation before moments)      */
+} bit_status;
+
+typedef enum {
+  BIT_KERNEL_COULOMB = 0,      /* 1/sqrt(r^2 + del)          treepotential, src/tree3d.cpp:4679 */
+  BIT_KERNEL_SCREENED = 1,     /* -exp(-kappa r)/r           shielded_treepot, src/tree3d.cpp:3448 */
+  BIT_KERNEL_SCREENED_REG = 2  /* exp(-kappa R)/R, R^2 = r^2 + del (new; no reference routine) */
+} bit_kernel;
+
+typedef enum {
+  BIT_PREC_FP64 = 0,  /* plain FP64 everywhere                                         */
+  BIT_PREC_MIXED = 1  /* FP32 near/far arithmetic in cluster-centred coordinates with
+                         compensated per-target accumulation; FP64 MAC and moments   */
+} bit_precision;
+
+typedef enum {
+  /* Exactly the reference's conventions: Coulomb particle targets drop del in the near
+   * field (src/tree3d.cpp:4765); screened particle targets add q*intg/w for themselves
+   * (:3575-3596); screened point targets add the near field with + (:3558). */
+  BIT_MODE_REFERENCE = 0,
+  /* One kernel everywhere: near field uses the same kernel as the far field and the
+   * direct sum (src/tree3d.cpp:298-330, 1966-2016); self excluded. */
+  BIT_MODE_CONSISTENT = 1
+} bit_mode;
+
+typedef struct {
+  int device;        /* CUDA device ordinal                                  */
+  void* stream;      /* cudaStream_t to use; NULL: the context creates one   */
+  size_t hbm_budget; /* bytes the context may allocate; 0 = no limit         */
+} bit_ctx_opts;
+
+typedef struct {
+  bit_kernel kernel;
+  bit_mode mode;
+  bit_precision precision;
+  double del;      /* delta^2 of the regularised kernels (the reference's DEL, src/problem.h:12) */
+  double mac_del;  /* screened kernel only: accept iff sqradius < acc*(r^2 - mac_del)
+                      (the reference subtracts DEL, src/tree3d.cpp:3473)                  */
+  double kappa;    /* screening parameter (the reference's alpha / kappa)                 */
+  double acc;      /* MAC: accept iff sqradius < acc * distance^2 (src/tree3d.cpp:866)    */
+  double intg;     /* reference-mode screened self term constant (src/tree3d.cpp:3585)    */
+} bit_eval_params;
+
+/* Device time (seconds, CUDA events on the context stream) of the last call's phases and
+ * the interaction counts of its lists. */
+typedef struct {
+  double t_build, t_moments, t_lists, t_far, t_near, t_total;
+  long long far_pairs;   /* (target, cluster) Taylor evaluations   */
+  long long near_pairs;  /* (target, source) direct interactions   */
+  long long far_entries, near_entries, batches;
+  int numtree, nleaves, depth, nterms;
+  int far_launches, near_launches;
+} bit_stats;
+
+const char* bit_status_string(bit_status s);
+int bit_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process (all contexts). */
+long long bit_kernel_launches(void);
+
+bit_status bit_ctx_create(bit_ctx** ctx, const bit_ctx_opts* opts);
+bit_status bit_ctx_destroy(bit_ctx* ctx);
+const char* bit_ctx_last_error(const bit_ctx* ctx);
+bit_status bit_ctx_synchronize(bit_ctx* ctx);
+bit_status bit_ctx_stream(const bit_ctx* ctx, void** stream);
+/* Bytes currently allocated by the context and its trees. */
+bit_status bit_ctx_memory(const bit_ctx* ctx, size_t* in_use, size_t* peak);
+
+/* treemake (src/tree3d.cpp:1345-1551): build the aspect-ratio bisection tree of the n
+ * particles.  x, y, z are host arrays (original order).  The node numbering, children
+ * order and member sets equal the reference's.  Returns BIT_ERR_DEGENERATE where the
+ * reference would never terminate. */
+bit_status bit_tree_build(bit_ctx* ctx, int n, const double* x, const double* y,
+                          const double* z, int maxmemb, bit_tree** tree);
+/* Same with device pointers (resident inputs). */
+bit_status bit_tree_build_device(bit_ctx* ctx, int n, const double* x, const double* y,
+                                 const double* z, int maxmemb, bit_tree** tree);
+/* treeempty (src/tree3d.cpp:990-1004). */
+bit_status bit_tree_destroy(bit_tree* tree);
+bit_status bit_tree_info(const bit_tree* tree, int* numtree, int* nleaves, int* depth);
+
+/* Charges (the reference's tot_charge) and weights (the reference's weight, used only by
+ * the reference-mode screened self term; NULL = 1) in original particle order. */
+bit_status bit_tree_set_charges(bit_tree* tree, const double* q, const double* w);
+bit_status bit_tree_set_charges_device(bit_tree* tree, const double* q, const double* w);
+/* treemoments (src/tree3d.cpp:2631-2711), FP64, for nterms = p + 1 (1..BIT_NTERMS_MAX). */
+bit_status bit_tree_moments(bit_tree* tree, int nterms);
+
+/* Copy the tree out in the reference's TREE terms (src/tree3d.h:51-74): per node
+ * nummemb, children[8] (-1 = none), 13 doubles (x0 x1 y0 y1 z0 z1 xmid ymid zmid aspectxy
+ * aspectxz aspectyz sqradius); members concatenated in node order, each node's list in
+ * ascending index (the reference's order).  Any output pointer may be NULL. */
+bit_status bit_tree_export(const bit_tree* tree, int* nummemb, int* children,
+                           double* fields, int* members);
+/* Moments, T = nterms(nterms+1)(nterms+2)/6 per node, packed with i (x power)
+ * outermost, then j, then k. */
+bit_status bit_tree_export_moments(const bit_tree* tree, double* mom);
+
+/* treepotential (src/tree3d.cpp:4679) / shielded_treepot (:3448) at every particle
+ * (targets = sources, p = particle index).  pot: host array, original order. */
+bit_status bit_eval_particles(bit_tree* tree, const bit_eval_params* prm, double* pot);
+bit_status bit_eval_particles_device(bit_tree* tree, const bit_eval_params* prm,
+                                     double* pot);
+/* Same at m external points (the reference's p = -1 path).  Host arrays. */
+bit_status bit_eval_points(bit_tree* tree, const bit_eval_params* prm, int m,
+                           const double* x, const double* y, const double* z, double* pot);
+/* treeforce (src/tree3d.cpp:851-971) at every particle: the field sum q grad G with the
+ * regularised Coulomb kernel (del), KERNEL_ORDER = 0.  Host arrays, original order. */
+bit_status bit_eval_force(bit_tree* tree, double del, double acc, bit_precision prec,
+                          double* fx, double* fy, double* fz);
+
+/* Whole pipeline through host buffers, the analogue of treemake + treemoments + a loop of
+ * treepotential / shielded_treepot over all particles (tests/treecode_mp.cpp:57-95). */
+bit_status bit_treecode_potential(bit_ctx* ctx, int n, const double* x, const double* y,
+                                  const double* z, const double* q, const double* w,
+                                  int nterms, int maxmemb, const bit_eval_params* prm,
+                                  double* pot);
+
+bit_status bit_tree_stats(const bit_tree* tree, bit_stats* st);
+
+/* Per-target interaction lists of the last evaluation, in the reference's traversal
+ * order, for particle index p: kind 0 = far (Taylor) cluster, 1 = near (direct) leaf.
+ * Returns the count in *n (entries beyond cap are dropped). */
+bit_status bit_tree_target_lists(bit_tree* tree, const bit_eval_params* prm, int p,
+                                 int* node, int* kind, int cap, int* n);
+
+/* ---------------------------------------------------------------------------------
+ * GMRES with the treecode as its matvec (no reference counterpart: the reference's
+ * solver::gmres, src/solver.h:157-260, takes a dense matrix).
+ * Solves (diag*I + K) s = f, (K s)_i = sum_{j != i} G(x_i, x_j) w_j s_j, G from prm.
+ * ------------------------------------------------------------------------------- */
+typedef struct {
+  int restart;             /* GMRES(m)                                                */
+  int maxit;               /* cap on inner iterations (matvecs)                       */
+  double tol;              /* target relative residual ||f - A s|| / ||f|| (FP64 A)   */
+  bit_precision precision; /* FP64: FP64 matvecs.  MIXED: FP32 matvecs inside FP64
+                              iterative refinement with FP64 true residuals            */
+  double inner_tol;        /* MIXED: relative tolerance of each inner solve (0: 1e-4) */
+  int max_refinements;     /* MIXED: outer refinement steps cap (0: 10)               */
+} bit_gmres_opts;
+
+typedef struct {
+  int iterations;  /* inner GMRES iterations (all refinement steps) */
+  int refinements; /* outer refinement steps (MIXED)                */
+  int matvecs_fp64, matvecs_fp32;
+  double relres;   /* final true relative residual in FP64          */
+  double seconds;  /* device time of the solve                      */
+} bit_gmres_info;
+
+bit_status bit_bie_solve(bit_tree* tree, const bit_eval_params* prm, int nterms, double diag,
+                         const double* w, const double* f, double* s,
+                         const bit_gmres_opts* opts, bit_gmres_info* info);
+
+/* solver::gmres (src/solver.h:157-310) on a dense row-major n x n matrix, on the device:
+ * full GMRES from zero, modified Gram-Schmidt, least squares by Gram-Schmidt QR of the
+ * Hessenberg, stop when the max relative change of x < 1e-5 every odd step.  x holds the
+ * initial values used by that stopping test.  Returns BIT_ERR_BREAKDOWN on h < 1e-14. */
+bit_status bit_gmres_dense(bit_ctx* ctx, int n, const double* a, const double* b, double* x,
+                           int* iterations);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BIT_B200_H */

@@ -1,0 +1,95 @@
+/*
+ * tree3d_b200.h -- drop-in replacement for the treecode surface of the reference's
+ * src/tree3d.h (ongbw/bit), implemented on the GPU by libtree3d_b200.so over the C ABI of
+ * bit_b200.h.  A program written against the reference's tree3d.h / constants.h /
+ * problem.h / solver.h switches by including this header instead and linking
+ * -ltree3d_b200 -lbit_b200.
+ *
+ * Types and signatures are the reference's (src/tree3d.h:33-74, 115-126, 197-298,
+ * src/solver.h:31-315); the physical constants are the values of src/constants.h:12-22 so
+ * that results scale identically.  DEL / ACC / KERNEL_ORDER are the reference's
+ * compile-time problem constants (src/problem.h:11-13); here DEL is read at run time from
+ * bit_tree3d_del (default 0.01, the reference's value).
+ *
+ * Semantics that differ (documented, never silent):
+ *  - treepotential / shielded_treepot / treeforce called with ind == 0 and a particle
+ *    index p evaluate ALL particles of the tree on the GPU on the first call for a given
+ *    (tree, acc, kernel) and serve later calls from that result; p == -1 evaluates the one
+ *    point on the GPU.  ind != 0 (an internal recursion step of the reference) returns -1
+ *    without touching *pot.
+ *  - treemake reports failure by returning -1 (the reference never returns on >maxmemb
+ *    coincident particles) and a message from bit_tree3d_last_error().
+ */
+#ifndef TREE3D_B200_H
+#define TREE3D_B200_H
+
+#include <cstdio>
+
+const int MAXPART = 1000000;  /* src/constants.h:8  */
+const int NUMCHILD = 8;       /* src/constants.h:9  */
+const int MAXTERM = 12;       /* src/constants.h:10 */
+const int MAXCHILD = 100000;  /* src/constants.h:11 */
+const double pi = 3.14159265359;
+const double inv2pi = 0.5 / pi;
+const double perm = 8.85418781762e-12;
+const double elec = 1.60217733e-19;
+const double charge_constant = inv2pi / perm;
+const double eps = 1e-14;
+
+/* src/tree3d.h:33-47 */
+struct PARTICLE {
+  double charge;
+  double x, y, z;
+  double u, v, w;
+  double xforce, yforce, zforce;
+  double weight;
+  double tot_charge;
+};
+
+/* src/tree3d.h:51-74 */
+struct TREE {
+  int nummemb;
+  double x0, x1, y0, y1, z0, z1;
+  double xmid, ymid, zmid;
+  double aspectxy, aspectxz, aspectyz;
+  double sqradius;
+  int children[NUMCHILD];
+  int* members;
+  double*** moments;
+  TREE() : nummemb(0), members(0x0), moments(0x0) {}
+};
+
+/* run-time problem constants (the reference's src/problem.h:11-13) */
+extern double bit_tree3d_del;
+extern double bit_tree3d_mac_del;   /* screened MAC offset; the reference uses DEL */
+extern int bit_tree3d_precision;    /* 0 = FP64 (default), 1 = mixed FP32 */
+const char* bit_tree3d_last_error();
+
+int treemake(int num, int nterms, int maxmemb, PARTICLE* part, TREE* tree);
+void treeempty(int numtree, TREE* tree);
+void treemoments(int numtree, int nterms, TREE* tree, PARTICLE* part);
+double treepotential(int ind, int p, int nterms, double x, double y, double z, double acc,
+                     double* pot, TREE* tree, PARTICLE* part);
+double shielded_treepot(int ind, int p, int nterms, double x, double y, double z,
+                        double alpha, double acc, double* pot, TREE* tree, PARTICLE* part,
+                        int Nx, int Ny, int Nz, double dlength, double dheight,
+                        double ddepth);
+double treeforce(int ind, int p, int nterms, double x, double y, double z, double acc,
+                 double* xfor, double* yfor, double* zfor, TREE* tree, PARTICLE* part);
+void freespace_particles_tree(int npart, PARTICLE* part, int nterms, double acc, TREE* tree,
+                              int numtree, int maxmemb);
+
+/* src/solver.h:31-315: dense GMRES, on the device */
+class solver {
+ public:
+  solver() {}
+  void makeFram(int) {}
+  int gmres(double** a, double* b, double* x, int num);
+  int minimize(int) { return 0; }
+  int iterations() const { return iters_; }
+
+ private:
+  int iters_ = 0;
+};
+
+#endif

@@ -1,0 +1,162 @@
+"""GPU evaluation (moments, lists, far and near field) against the oracle.
+
+Bars: the plain FP64 GPU path matches the FP64 CPU treecode to 1e-12 relative (L2 and
+max-norm relative to max |value|); the interaction lists match exactly; the mixed path
+stays within 1e-6 relative L2 of the FP64 path at the same lists.
+"""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL_MIXED = 1e-6
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return max(np.linalg.norm(a - b) / np.linalg.norm(b), np.abs(a - b).max() / np.abs(b).max())
+
+
+def both(ctx, orc, x, y, z, q, nterms, maxmemb, w=None):
+    t = ctx.treemake(x, y, z, maxmemb)
+    t.treemoments(q, nterms, w=w)
+    T = orc.Tree(x, y, z, maxmemb)
+    T.compute_moments(q, nterms, w=w)
+    return t, T
+
+
+def gp(bit_b200, **kw):
+    return bit_b200.params(**kw)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_reference_mode_matches_golden(ctx, name):
+    """Reference-mode potentials / force on the reference's own outputs."""
+    import bit_b200 as B
+    g = load_golden(name)
+    t = ctx.treemake(g["x"], g["y"], g["z"], int(g["maxmemb"]))
+    t.treemoments(g["q"], int(g["nterms"]), w=g["w"])
+    d, acc, kappa = float(g["del_"]), float(g["acc"]), float(g["kappa"])
+    np.testing.assert_allclose(t.export_moments(), g["moments"], rtol=1e-12,
+                               atol=1e-13 * np.abs(g["moments"]).max())
+    assert rel(t.treepotential(acc, d, mode=B.REFERENCE), g["coulomb"]) < TOL64
+    assert rel(t.shielded_treepot(kappa, acc, mode=B.REFERENCE, mac_del=d), g["screened"]) < TOL64
+    assert rel(t.treepotential(acc, d, mode=B.REFERENCE, points=g["points"]),
+               g["coulomb_points"]) < TOL64
+    assert rel(t.shielded_treepot(kappa, acc, mode=B.REFERENCE, mac_del=d, points=g["points"]),
+               g["screened_points"]) < TOL64
+    f = np.stack(t.treeforce(acc, d))
+    assert rel(f, g["force"]) < TOL64
+
+
+@pytest.mark.parametrize("nterms", range(1, 11))
+def test_every_order_matches_oracle(ctx, orc, nterms):
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.clustered_blobs(6000, seed=nterms)
+    t, T = both(ctx, orc, x, y, z, q, nterms, 150)
+    for kern, kw in [(B.COULOMB, dict(del_=1e-4)), (B.SCREENED, dict(kappa=1.5)),
+                     (B.SCREENED_REG, dict(kappa=0.7, del_=1e-3))]:
+        for mode in (B.REFERENCE, B.CONSISTENT):
+            p = B.params(kern, mode, B.FP64, acc=0.6, **kw)
+            po = orc.params(kern, mode, acc=0.6, **kw)
+            assert rel(t.evaluate(p), T.evaluate(po)) < TOL64, (kern, mode)
+    if nterms <= 10:
+        f = np.stack(t.treeforce(0.6, 1e-4))
+        fo = np.stack(T.evaluate_force(1e-4, 0.6))
+        assert rel(f, fo) < TOL64
+
+
+def test_lists_match_reference_traversal(ctx, orc):
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.clustered_blobs(20000, seed=5)
+    t, T = both(ctx, orc, x, y, z, q, 5, 200)
+    for kern, po, p in [
+        ("coulomb", orc.params(orc.COULOMB, acc=0.7, del_=2.5e-5),
+         B.params(B.COULOMB, acc=0.7, del_=2.5e-5)),
+        ("screened", orc.params(orc.SCREENED, acc=0.5, mac_del=0.01, kappa=1.0),
+         B.params(B.SCREENED, acc=0.5, mac_del=0.01, kappa=1.0)),
+    ]:
+        for tg in workloads.sample_targets(20000, 40, seed=3):
+            gn, gk = t.target_lists(p, int(tg))
+            on, ok = T.target_lists(po, int(tg))
+            np.testing.assert_array_equal(gn, on, err_msg=kern)
+            np.testing.assert_array_equal(gk, ok, err_msg=kern)
+    # interaction counts agree with the oracle's traversal
+    t.evaluate(B.params(B.COULOMB, acc=0.7, del_=2.5e-5))
+    st = t.stats()
+    nf, nn, nl = T.count(orc.params(orc.COULOMB, acc=0.7, del_=2.5e-5))
+    assert st["far_pairs"] == nf
+    assert st["near_pairs"] - 20000 == nn  # the GPU count includes each target's self pair
+
+
+@pytest.mark.parametrize("kern", ["coulomb", "screened"])
+def test_mixed_precision_close_to_fp64(ctx, kern):
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.clustered_blobs(100000, seed=7)
+    t = ctx.treemake(x, y, z, 1000)
+    t.treemoments(q, 9)
+    kw = dict(del_=2.5e-5) if kern == "coulomb" else dict(kappa=1.0)
+    k = B.COULOMB if kern == "coulomb" else B.SCREENED
+    p64 = t.evaluate(B.params(k, B.CONSISTENT, B.FP64, acc=0.7, **kw))
+    p32 = t.evaluate(B.params(k, B.CONSISTENT, B.MIXED, acc=0.7, **kw))
+    assert workloads.rel_l2(p32, p64) < TOL_MIXED
+
+
+def test_mixed_force_close_to_fp64(ctx):
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(30000, seed=8)
+    t = ctx.treemake(x, y, z, 300)
+    t.treemoments(q, 7)
+    f64 = np.stack(t.treeforce(0.5, 1e-4, B.FP64))
+    f32 = np.stack(t.treeforce(0.5, 1e-4, B.MIXED))
+    assert workloads.rel_l2(f32, f64) < 1e-5
+
+
+def test_error_against_direct_sum_decreases(ctx, orc):
+    """tests/treecode.cpp:84-127 on the GPU: error vs the direct sum shrinks with nterms."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(20000, seed=1)
+    tg = workloads.sample_targets(20000, 500, seed=1)
+    po = orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=1e-4, acc=0.5)
+    ds = orc.direct(x, y, z, q, po, tg)
+    t = ctx.treemake(x, y, z, 500)
+    errs = []
+    for nterms in (2, 4, 7, 10):
+        t.treemoments(q, nterms)
+        pot = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=1e-4, acc=0.5))
+        errs.append(workloads.rel_l2(pot[tg], ds))
+    assert all(b <= a for a, b in zip(errs, errs[1:])), errs
+
+
+def test_repeat_and_stats(ctx):
+    """Same inputs give bit-identical results; stats report the phases."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(20000, seed=2)
+    t = ctx.treemake(x, y, z, 500)
+    t.treemoments(q, 7)
+    p = B.params(B.COULOMB, B.CONSISTENT, B.MIXED, del_=1e-4, acc=0.5)
+    a = t.evaluate(p)
+    b = t.evaluate(p)
+    np.testing.assert_array_equal(a, b)
+    st = t.stats()
+    assert st["numtree"] == t.numtree and st["far_pairs"] > 0 and st["t_far"] > 0
+
+
+def test_whole_pipeline_host_buffers(ctx, orc):
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(20000, seed=1)
+    p = B.params(B.COULOMB, B.REFERENCE, B.FP64, del_=1e-4, acc=0.5)
+    pot = ctx.treecode_potential(x, y, z, q, 7, 500, p)
+    T = orc.Tree(x, y, z, 500)
+    T.compute_moments(q, 7)
+    assert rel(pot, T.evaluate(orc.params(orc.COULOMB, orc.MODE_REFERENCE, del_=1e-4, acc=0.5))) < TOL64
