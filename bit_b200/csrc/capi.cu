@@ -35,6 +35,13 @@ void dev_free(Ctx* c, void* p) {
   cudaFree(p);
 }
 
+// Blocking device-to-host copy ordered on the context's stream (the legacy default stream
+// does not order against the non-blocking context stream).
+void d2h(Ctx* c, void* dst, const void* src, size_t bytes) {
+  BIT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+  BIT_CUDA(cudaStreamSynchronize(c->stream));
+}
+
 namespace {
 
 __global__ void k_scatter_out(int n, const int* perm, const double* sorted, double* out) {
@@ -359,7 +366,7 @@ bit_status bit_tree_export(const bit_tree* th, int* nummemb, int* children, doub
     if (fields) std::memcpy(fields, t->h_fields.data(), 13LL * b * sizeof(double));
     if (members) {
       std::vector<int> perm(t->n);
-      BIT_CUDA(cudaMemcpy(perm.data(), t->perm.p, t->n * sizeof(int), cudaMemcpyDeviceToHost));
+      d2h(t->ctx, perm.data(), t->perm.p, t->n * sizeof(int));
       long long off = 0;
       for (int i = 0; i < b; i++) {
         int st = t->h_start[i], cnt = t->h_nummemb[i];
@@ -376,8 +383,7 @@ bit_status bit_tree_export_moments(const bit_tree* th, double* mom) {
   const Tree* t = &th->t;
   if (!t->has_moments) return BIT_ERR_STATE;
   return guard(t->ctx, [&] {
-    BIT_CUDA(cudaMemcpy(mom, t->mom64.p, (size_t)t->numtree * num_terms(t->nterms) * sizeof(double),
-                        cudaMemcpyDeviceToHost));
+    d2h(t->ctx, mom, t->mom64.p, (size_t)t->numtree * num_terms(t->nterms) * sizeof(double));
   });
 }
 
@@ -557,22 +563,22 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
     ensure_particle_lists(t, *prm);
     Lists& L = t->plists;
     int e = 0;
-    BIT_CUDA(cudaMemcpy(&e, t->iperm.p + p, sizeof(int), cudaMemcpyDeviceToHost));
+    d2h(t->ctx, &e, t->iperm.p + p, sizeof(int));
     // find the batch holding sorted position e
     std::vector<int> ts(L.nbatch), tc(L.nbatch);
-    BIT_CUDA(cudaMemcpy(ts.data(), L.b_tstart.p, L.nbatch * sizeof(int), cudaMemcpyDeviceToHost));
-    BIT_CUDA(cudaMemcpy(tc.data(), L.b_tcount.p, L.nbatch * sizeof(int), cudaMemcpyDeviceToHost));
+    d2h(t->ctx, ts.data(), L.b_tstart.p, L.nbatch * sizeof(int));
+    d2h(t->ctx, tc.data(), L.b_tcount.p, L.nbatch * sizeof(int));
     int b = -1;
     for (int i = 0; i < L.nbatch; i++)
       if (e >= ts[i] && e < ts[i] + tc[i]) { b = i; break; }
     if (b < 0) fail(BIT_ERR_STATE, "target not found in batches");
     const int lane = e - ts[b];
     long long fo[2], no[2];
-    BIT_CUDA(cudaMemcpy(fo, L.far_off.p + b, 2 * sizeof(long long), cudaMemcpyDeviceToHost));
-    BIT_CUDA(cudaMemcpy(no, L.near_off.p + b, 2 * sizeof(long long), cudaMemcpyDeviceToHost));
+    d2h(t->ctx, fo, L.far_off.p + b, 2 * sizeof(long long));
+    d2h(t->ctx, no, L.near_off.p + b, 2 * sizeof(long long));
     std::vector<int2> fe(fo[1] - fo[0]), ne(no[1] - no[0]);
-    if (!fe.empty()) BIT_CUDA(cudaMemcpy(fe.data(), L.far_ent.p + fo[0], fe.size() * sizeof(int2), cudaMemcpyDeviceToHost));
-    if (!ne.empty()) BIT_CUDA(cudaMemcpy(ne.data(), L.near_ent.p + no[0], ne.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+    if (!fe.empty()) d2h(t->ctx, fe.data(), L.far_ent.p + fo[0], fe.size() * sizeof(int2));
+    if (!ne.empty()) d2h(t->ctx, ne.data(), L.near_ent.p + no[0], ne.size() * sizeof(int2));
     // merge back into traversal order: far and near entries were emitted along one
     // depth-first walk, so order them by the node's DFS preorder rank
     std::vector<int> rank(t->numtree, 0);
