@@ -12,11 +12,45 @@
 
 namespace bit {
 
+// Device memory: a per-context cache of freed blocks.  All work of a context runs on its
+// one stream, so a block freed after a launch can be handed to a later launch on the same
+// stream without a device synchronisation (stream order protects it).  The HBM budget
+// bounds live + cached bytes; cached blocks are released first when it would be exceeded.
+static size_t round_block(size_t b) {
+  const size_t g = b < (1u << 20) ? 512 : (size_t)2 << 20;
+  return (b + g - 1) / g * g;
+}
+
+static void release_cache(Ctx* c) {
+  for (auto& kv : c->cache) cudaFree(kv.second);
+  c->cache.clear();
+  c->cached = 0;
+}
+
 void* dev_alloc(Ctx* c, size_t bytes) {
+  bytes = round_block(bytes);
+  auto it = c->cache.lower_bound(bytes);
+  if (it != c->cache.end() && it->first <= 2 * bytes) {
+    void* p = it->second;
+    size_t sz = it->first;
+    c->cache.erase(it);
+    c->cached -= sz;
+    c->in_use += sz;
+    c->peak = std::max(c->peak, c->in_use);
+    c->allocs.push_back({p, sz});
+    return p;
+  }
+  if (c->budget && c->in_use + c->cached + bytes > c->budget) release_cache(c);
   if (c->budget && c->in_use + bytes > c->budget)
     fail(BIT_ERR_BUDGET, "allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget");
   void* p = nullptr;
-  BIT_CUDA(cudaMalloc(&p, bytes));
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    release_cache(c);
+    e = cudaMalloc(&p, bytes);
+  }
+  BIT_CUDA(e);
   c->in_use += bytes;
   c->peak = std::max(c->peak, c->in_use);
   c->allocs.push_back({p, bytes});
@@ -27,10 +61,13 @@ void dev_free(Ctx* c, void* p) {
   if (!p) return;
   for (size_t i = 0; i < c->allocs.size(); i++)
     if (c->allocs[i].first == p) {
-      c->in_use -= c->allocs[i].second;
+      size_t sz = c->allocs[i].second;
+      c->in_use -= sz;
       c->allocs[i] = c->allocs.back();
       c->allocs.pop_back();
-      break;
+      c->cache.insert({sz, p});
+      c->cached += sz;
+      return;
     }
   cudaFree(p);
 }
@@ -98,6 +135,17 @@ double ev_sec(Tree* t, int i) {
   return ms * 1e-3;
 }
 
+// Errors raised on the device (a bounded wait that gave up) since the last check.
+void check_dev_err(Ctx* c) {
+  if (!c->err_flag) return;
+  int e = 0;
+  d2h(c, &e, c->err_flag, sizeof(int));
+  if (e) {
+    BIT_CUDA(cudaMemsetAsync(c->err_flag, 0, sizeof(int), c->stream));
+    fail(BIT_ERR_CUDA, "a device-side wait gave up (error flags " + std::to_string(e) + ")");
+  }
+}
+
 void ensure_particle_lists(Tree* t, const bit_eval_params& p) {
   ListKey k = mac_key(p, t->gen, 0);
   if (t->plists.valid && t->plists.key == k) return;
@@ -121,7 +169,7 @@ void eval_particles_sorted(Tree* t, const bit_eval_params& p) {
   t->stats.near_pairs = t->plists.near_pairs;
   t->stats.far_entries = t->plists.nfar;
   t->stats.near_entries = t->plists.nnear;
-  t->stats.batches = t->plists.nbatch;
+  t->stats.batches = t->plists.ngroups;
   t->stats.far_launches = 1;
   t->stats.near_launches = 1;
 }
@@ -210,6 +258,7 @@ bit_status bit_ctx_destroy(bit_ctx* h) {
   }
   c.trees.clear();
   c.scratch_ll.release();
+  release_cache(&c);
   if (c.h_pinned) cudaFreeHost(c.h_pinned);
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
   delete h;
@@ -418,6 +467,7 @@ bit_status bit_eval_particles(bit_tree* th, const bit_eval_params* prm, double* 
     ev_rec(t, EV_ALL + 1);
     BIT_CUDA(cudaMemcpyAsync(pot, out.p, t->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     BIT_CUDA(cudaStreamSynchronize(c->stream));
+    check_dev_err(c);
   });
 }
 
@@ -477,6 +527,7 @@ bit_status bit_eval_points(bit_tree* th, const bit_eval_params* prm, int m, cons
     BIT_CHECK_LAUNCH();
     BIT_CUDA(cudaMemcpyAsync(pot, res.p, m * sizeof(double), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
+    check_dev_err(c);
   });
 }
 
@@ -514,6 +565,7 @@ bit_status bit_eval_force(bit_tree* th, double del, double acc, bit_precision pr
     BIT_CUDA(cudaMemcpyAsync(fy, o.p + n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaMemcpyAsync(fz, o.p + 2LL * n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
+    check_dev_err(c);
   });
 }
 
@@ -539,6 +591,7 @@ bit_status bit_tree_stats(const bit_tree* th, bit_stats* st) {
   Tree* t = const_cast<Tree*>(&th->t);
   return guard(t->ctx, [&] {
     BIT_CUDA(cudaStreamSynchronize(t->ctx->stream));
+    check_dev_err(t->ctx);
     bit_stats s = t->stats;
     s.t_build = ev_sec(t, EV_BUILD);
     s.t_moments = ev_sec(t, EV_MOM);
@@ -562,25 +615,37 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
     check_params(prm);
     ensure_particle_lists(t, *prm);
     Lists& L = t->plists;
+    Ctx* c = t->ctx;
     int e = 0;
-    d2h(t->ctx, &e, t->iperm.p + p, sizeof(int));
-    // find the batch holding sorted position e
-    std::vector<int> ts(L.nbatch), tc(L.nbatch);
-    d2h(t->ctx, ts.data(), L.b_tstart.p, L.nbatch * sizeof(int));
-    d2h(t->ctx, tc.data(), L.b_tcount.p, L.nbatch * sizeof(int));
-    int b = -1;
-    for (int i = 0; i < L.nbatch; i++)
-      if (e >= ts[i] && e < ts[i] + tc[i]) { b = i; break; }
-    if (b < 0) fail(BIT_ERR_STATE, "target not found in batches");
-    const int lane = e - ts[b];
-    long long fo[2], no[2];
-    d2h(t->ctx, fo, L.far_off.p + b, 2 * sizeof(long long));
-    d2h(t->ctx, no, L.near_off.p + b, 2 * sizeof(long long));
-    std::vector<int2> fe(fo[1] - fo[0]), ne(no[1] - no[0]);
-    if (!fe.empty()) d2h(t->ctx, fe.data(), L.far_ent.p + fo[0], fe.size() * sizeof(int2));
-    if (!ne.empty()) d2h(t->ctx, ne.data(), L.near_ent.p + no[0], ne.size() * sizeof(int2));
-    // merge back into traversal order: far and near entries were emitted along one
-    // depth-first walk, so order them by the node's DFS preorder rank
+    d2h(c, &e, t->iperm.p + p, sizeof(int));
+    const int ng = L.ngroups;
+    std::vector<int> ts(ng), tc(ng);
+    d2h(c, ts.data(), L.g_tstart.p, ng * sizeof(int));
+    d2h(c, tc.data(), L.g_tcount.p, ng * sizeof(int));
+    int g = -1;
+    for (int i = 0; i < ng; i++)
+      if (e >= ts[i] && e < ts[i] + tc[i]) { g = i; break; }
+    if (g < 0) fail(BIT_ERR_STATE, "target not found in the groups");
+    const int lane = e - ts[g], W = (tc[g] + 31) / 32;
+    std::vector<std::pair<int, int>> all;
+    for (int kd = 0; kd < 2; kd++) {
+      const DBuf<long long>& off = kd ? L.near_off : L.far_off;
+      const DBuf<long long>& moff = kd ? L.near_moff : L.far_moff;
+      const DBuf<int>& nd = kd ? L.near_node : L.far_node;
+      const DBuf<unsigned>& mk = kd ? L.near_mask : L.far_mask;
+      long long o[2], mo = 0;
+      d2h(c, o, off.p + g, 2 * sizeof(long long));
+      d2h(c, &mo, moff.p + g, sizeof(long long));
+      const long long ne = o[1] - o[0];
+      if (!ne) continue;
+      std::vector<int> nodes(ne);
+      std::vector<unsigned> masks(ne * W);
+      d2h(c, nodes.data(), nd.p + o[0], ne * sizeof(int));
+      d2h(c, masks.data(), mk.p + mo, ne * W * sizeof(unsigned));
+      for (long long k = 0; k < ne; k++)
+        if ((masks[k * W + lane / 32] >> (lane % 32)) & 1u) all.push_back({nodes[k], kd});
+    }
+    // far and near entries were emitted along one depth-first walk: order by preorder rank
     std::vector<int> rank(t->numtree, 0);
     {
       int r = 0;
@@ -595,13 +660,9 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
         }
       }
     }
-    std::vector<std::pair<int, int>> all;
-    for (auto& v : fe)
-      if ((unsigned(v.y) >> lane) & 1u) all.push_back({v.x, 0});
-    for (auto& v : ne)
-      if ((unsigned(v.y) >> lane) & 1u) all.push_back({v.x, 1});
-    std::sort(all.begin(), all.end(),
-              [&](const std::pair<int, int>& a, const std::pair<int, int>& b2) { return rank[a.first] < rank[b2.first]; });
+    std::sort(all.begin(), all.end(), [&](const std::pair<int, int>& a, const std::pair<int, int>& b2) {
+      return rank[a.first] < rank[b2.first];
+    });
     for (int i = 0; i < (int)all.size() && i < cap; i++) {
       if (node) node[i] = all[i].first;
       if (kind) kind[i] = all[i].second;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -13,8 +14,8 @@ namespace bit {
 
 constexpr int kWarp = 32;
 constexpr int kNtermsMax = BIT_NTERMS_MAX;
-constexpr int kBatch = 32;        // targets per batch (one per lane of a warp)
-constexpr int kStackCap = 512;    // DFS stack entries per warp in the list builder
+constexpr int kGroupMax = 1024;   // targets per group (one CTA; 32 mask words)
+constexpr int kPointGroup = 256;  // external points per group
 constexpr double kEpsNear = 1e-14;  // src/constants.h:35
 
 __host__ __device__ constexpr int num_terms(int n) { return n * (n + 1) * (n + 2) / 6; }
@@ -90,13 +91,15 @@ struct ListKey {
 struct Lists {
   ListKey key;
   bool valid = false;
-  int nbatch = 0;
-  long long nfar = 0, nnear = 0;          // entries
+  int ngroups = 0;
+  long long nfar = 0, nnear = 0;            // entries
   long long far_pairs = 0, near_pairs = 0;  // interactions
-  DBuf<int> b_tstart, b_tcount, b_srcleaf;  // batch: first sorted target, count, leaf of targets
-  DBuf<long long> far_off, near_off;        // nbatch + 1
-  DBuf<int2> far_ent, near_ent;             // (node, lane mask)
-  DBuf<int> order;                          // batches sorted by decreasing work
+  DBuf<int> g_tstart, g_tcount, g_own;      // group: first target, count, own leaf (or -1)
+  DBuf<long long> far_off, near_off;        // first entry of each group (ngroups + 1)
+  DBuf<long long> far_moff, near_moff;      // first mask word of each group (ngroups + 1)
+  DBuf<int> far_node, near_node;            // entry -> node
+  DBuf<unsigned> far_mask, near_mask;       // (tcount+31)/32 words per entry
+  DBuf<int> order;                          // groups by decreasing work
 };
 
 struct Ctx {
@@ -110,8 +113,18 @@ struct Ctx {
   DBuf<long long> scratch_ll;
   long long* h_pinned = nullptr;  // pinned host staging for small read-backs (64 entries)
   std::vector<std::pair<void*, size_t>> allocs;  // live device allocations and their sizes
+  std::multimap<size_t, void*> cache;             // freed blocks kept for reuse, by size
+  size_t cached = 0;                              // bytes held in `cache`
   std::vector<Tree*> trees;                       // trees built by this context
   long long launches = 0;                         // kernels launched by this context
+  int* err_flag = nullptr;                        // device word kernels raise errors in
+  int* dev_err() {
+    if (!err_flag) {
+      err_flag = static_cast<int*>(dev_alloc(this, 64));
+      cudaMemsetAsync(err_flag, 0, 64, stream);
+    }
+    return err_flag;
+  }
 };
 
 struct Tree {

@@ -1,11 +1,17 @@
 // Far field: Taylor expansion about every accepted cluster (treetaylorpotential,
-// shielded_treetaylorpot, treetaylorforce; src/tree3d.cpp:4468-4640, 3004-3227, 456-810).
+// shielded_treetaylorpot, treetaylorforce; src/tree3d.cpp:4468-4640, 3004-3227, 456-810),
+// one CTA per target group.
 //
-// One warp per batch, one target per lane, walking the batch's far entries; every lane
-// whose bit is set evaluates the unrolled recurrence for its own offset from the cluster
-// centre (generated per nterms by gen_farfield.py) against the cluster's moments.  The
-// offset is formed in FP64; the mixed path rounds it once to FP32 and runs recurrence and
-// dot product in FP32 with compensated accumulation across clusters.
+// The CTA's warps take the group's far entries round-robin.  A warp packs the targets of
+// its entry (the set bits of the entry's mask) into a dense list and its lanes run the
+// unrolled recurrence (generated per nterms by gen_farfield.py) for one target each,
+// against the cluster's moments (warp-uniform loads).  Each warp accumulates into its own
+// shared-memory row; rows are summed in warp order at the end, so the result does not
+// depend on timing.  The target-centre offset is formed in FP64; the mixed path rounds it
+// once to FP32 and runs recurrence and dot product in FP32, accumulating with two-sum.
+#include <set>
+#include <utility>
+
 #include "common.cuh"
 
 namespace bit {
@@ -18,7 +24,6 @@ __device__ __forceinline__ double exp_t(double x) { return exp(x); }
 __device__ __forceinline__ float exp_t(float x) { return expf(x); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
-
 }  // namespace bit
 
 #include "generated/farfield_gen.cuh"
@@ -27,124 +32,222 @@ namespace bit {
 
 namespace {
 
-constexpr int FWARPS = 4;
+struct FarArgs {
+  const int *order, *g_tstart, *g_tcount;
+  const double *tx, *ty, *tz;
+  const long long *off, *moff;
+  const int* node;
+  const unsigned* mask;
+  const double4* nodec;
+  const void* mom;  // float or double, T(nterms) per node
+  double add, kappa, sign;
+  double *out, *out_y, *out_z;
+};
+
+// Pack the set bits of a group mask (W words, lane l holds word l) into tl; returns count.
+__device__ __forceinline__ int warp_pack(unsigned wd, unsigned short* tl) {
+  const int lane = threadIdx.x & 31;
+  const int c = __popc(wd);
+  int pre = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += t;
+  }
+  int base = pre - c;
+  while (wd) {
+    const int b = __ffs(wd) - 1;
+    wd &= wd - 1;
+    tl[base++] = (unsigned short)(32 * lane + b);
+  }
+  __syncwarp();
+  return __shfl_sync(0xffffffffu, pre, 31);
+}
 
 template <class T>
-struct Acc;
+struct WarpAcc;  // per-warp accumulator rows in shared memory
 template <>
-struct Acc<double> {
-  double s = 0.0;
-  __device__ void add(double v) { s += v; }
-  __device__ double value() const { return s; }
-};
-template <>
-struct Acc<float> {
-  float s = 0.f, e = 0.f;
-  __device__ void add(float v) {
+struct WarpAcc<float> {
+  static constexpr int words = 2;  // hi, lo
+  __device__ static void add(float* row, int i, float v) {
+    float& s = row[i];
+    float& e = row[kGroupMax + i];
     float t = s + v, bp = t - s;
     e += (s - (t - bp)) + (v - bp);
     s = t;
   }
-  __device__ double value() const { return (double)s + (double)e; }
+  __device__ static double get(const float* row, int i) {
+    return (double)row[i] + (double)row[kGroupMax + i];
+  }
+};
+template <>
+struct WarpAcc<double> {
+  static constexpr int words = 1;
+  __device__ static void add(double* row, int i, double v) { row[i] += v; }
+  __device__ static double get(const double* row, int i) { return row[i]; }
 };
 
+template <int NW>
+constexpr size_t far_smem(size_t acc_bytes_per_row_target, size_t moment_bytes) {
+  return 3 * kGroupMax * sizeof(double) + NW * kGroupMax * sizeof(unsigned short) +
+         NW * kGroupMax * acc_bytes_per_row_target + NW * moment_bytes;
+}
+
+constexpr int NWP = 8;  // warps per CTA, potential
+constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
+
 template <int NT, int KER, class T>
-__global__ void __launch_bounds__(32 * FWARPS)
-    k_far(int nbatch, const int* order, const int* b_tstart, const int* b_tcount,
-          const double* tx, const double* ty, const double* tz, const long long* off,
-          const int2* ent, const double4* nodec, const T* __restrict__ mom, double add,
-          double kappa, double sign, double* out) {
+__global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
   constexpr int TT = num_terms(NT);
-  const int lane = threadIdx.x & 31;
-  const int wi = blockIdx.x * FWARPS + (threadIdx.x >> 5);
-  if (wi >= nbatch) return;
-  const int b = order[wi];
-  const int t0 = b_tstart[b], tc = b_tcount[b];
-  const bool live = lane < tc;
-  double x = 0, y = 0, z = 0;
-  if (live) { x = tx[t0 + lane]; y = ty[t0 + lane]; z = tz[t0 + lane]; }
-  const T tadd = (T)add, tk = (T)kappa;
-  Acc<T> acc;
-  for (long long e = off[b]; e < off[b + 1]; e++) {
-    const int2 en = ent[e];
-    if (!((unsigned(en.y) >> lane) & 1u)) continue;
-    const double4 c = nodec[en.x];
-    const T dx = (T)(x - c.x), dy = (T)(y - c.y), dz = (T)(z - c.z);
-    const T r2 = dx * dx + dy * dy + dz * dz + tadd;
-    const T* M = mom + (long long)en.x * TT;
-    T v;
-    if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb<T>(dx, dy, dz, r2, M);
-    else v = FarField<NT>::template screened<T>(dx, dy, dz, r2, tk, M);
-    acc.add(v);
+  constexpr int NW = NWP;
+  extern __shared__ __align__(16) unsigned char sm[];
+  double* cx = reinterpret_cast<double*>(sm);
+  double* cy = cx + kGroupMax;
+  double* cz = cy + kGroupMax;
+  unsigned short* tlb = reinterpret_cast<unsigned short*>(cz + kGroupMax);
+  T* accb = reinterpret_cast<T*>(tlb + NW * kGroupMax);
+  constexpr int ROW = WarpAcc<T>::words * kGroupMax;
+  T* msb = accb + NW * ROW;  // one cluster's moments per warp
+
+  const int g = a.order[blockIdx.x];
+  const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
+  const int W = (tc + 31) >> 5;
+  const long long e0 = a.off[g], e1 = a.off[g + 1], m0 = a.moff[g];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int i = tid; i < tc; i += 32 * NW) {
+    cx[i] = a.tx[t0 + i]; cy[i] = a.ty[t0 + i]; cz[i] = a.tz[t0 + i];
   }
-  if (live) out[t0 + lane] = sign * acc.value();
+  for (int i = tid; i < NW * ROW; i += 32 * NW) accb[i] = T(0);
+  __syncthreads();
+  unsigned short* tl = tlb + w * kGroupMax;
+  T* row = accb + w * ROW;
+  const T* mom = reinterpret_cast<const T*>(a.mom);
+  const T tadd = (T)a.add, tk = (T)a.kappa;
+  for (long long e = e0 + w; e < e1; e += NW) {
+    const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
+    const int cnt = warp_pack(wd, tl);
+    const int node = a.node[e];
+    const double4 c = a.nodec[node];
+    T* M = msb + w * TT;
+    for (int k = lane; k < TT; k += 32) M[k] = mom[(long long)node * TT + k];
+    __syncwarp();
+    for (int r = lane; r < cnt; r += 32) {
+      const int i = tl[r];
+      const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
+      const T r2 = dx * dx + dy * dy + dz * dz + tadd;
+      T v;
+      if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb<T>(dx, dy, dz, r2, M);
+      else v = FarField<NT>::template screened<T>(dx, dy, dz, r2, tk, M);
+      WarpAcc<T>::add(row, i, v);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int i = tid; i < tc; i += 32 * NW) {
+    double s = 0.0;
+    for (int q = 0; q < NW; q++) s += WarpAcc<T>::get(accb + q * ROW, i);
+    a.out[t0 + i] = a.sign * s;
+  }
 }
 
 template <int NT, class T>
-__global__ void __launch_bounds__(32 * FWARPS)
-    k_far_force(int nbatch, const int* order, const int* b_tstart, const int* b_tcount,
-                const double* tx, const double* ty, const double* tz, const long long* off,
-                const int2* ent, const double4* nodec, const T* __restrict__ mom, double del,
-                double* fx, double* fy, double* fz) {
+__global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
   constexpr int TT = num_terms(NT);
-  const int lane = threadIdx.x & 31;
-  const int wi = blockIdx.x * FWARPS + (threadIdx.x >> 5);
-  if (wi >= nbatch) return;
-  const int b = order[wi];
-  const int t0 = b_tstart[b], tc = b_tcount[b];
-  const bool live = lane < tc;
-  double x = 0, y = 0, z = 0;
-  if (live) { x = tx[t0 + lane]; y = ty[t0 + lane]; z = tz[t0 + lane]; }
-  Acc<T> ax, ay, az;
-  for (long long e = off[b]; e < off[b + 1]; e++) {
-    const int2 en = ent[e];
-    if (!((unsigned(en.y) >> lane) & 1u)) continue;
-    const double4 c = nodec[en.x];
-    const T dx = (T)(x - c.x), dy = (T)(y - c.y), dz = (T)(z - c.z);
-    const T rs = dx * dx + dy * dy + dz * dz + (T)del;
-    T fxv = 0, fyv = 0, fzv = 0;
-    FarField<NT>::template force<T>(dx, dy, dz, rs, mom + (long long)en.x * TT, fxv, fyv, fzv);
-    ax.add(fxv); ay.add(fyv); az.add(fzv);
+  constexpr int NW = NWF;
+  extern __shared__ __align__(16) unsigned char sm[];
+  double* cx = reinterpret_cast<double*>(sm);
+  double* cy = cx + kGroupMax;
+  double* cz = cy + kGroupMax;
+  unsigned short* tlb = reinterpret_cast<unsigned short*>(cz + kGroupMax);
+  double* accb = reinterpret_cast<double*>(tlb + NW * kGroupMax);  // [NW][3][kGroupMax]
+  T* msb = reinterpret_cast<T*>(accb + NW * 3 * kGroupMax);         // moments, one per warp
+
+  const int g = a.order[blockIdx.x];
+  const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
+  const int W = (tc + 31) >> 5;
+  const long long e0 = a.off[g], e1 = a.off[g + 1], m0 = a.moff[g];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int i = tid; i < tc; i += 32 * NW) {
+    cx[i] = a.tx[t0 + i]; cy[i] = a.ty[t0 + i]; cz[i] = a.tz[t0 + i];
   }
-  if (live) {
-    fx[t0 + lane] = ax.value();
-    fy[t0 + lane] = ay.value();
-    fz[t0 + lane] = az.value();
+  for (int i = tid; i < NW * 3 * kGroupMax; i += 32 * NW) accb[i] = 0.0;
+  __syncthreads();
+  unsigned short* tl = tlb + w * kGroupMax;
+  double* row = accb + w * 3 * kGroupMax;
+  const T* mom = reinterpret_cast<const T*>(a.mom);
+  for (long long e = e0 + w; e < e1; e += NW) {
+    const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
+    const int cnt = warp_pack(wd, tl);
+    const int node = a.node[e];
+    const double4 c = a.nodec[node];
+    T* M = msb + w * TT;
+    for (int k = lane; k < TT; k += 32) M[k] = mom[(long long)node * TT + k];
+    __syncwarp();
+    for (int r = lane; r < cnt; r += 32) {
+      const int i = tl[r];
+      const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
+      const T rs = dx * dx + dy * dy + dz * dz + (T)a.add;
+      T fx = 0, fy = 0, fz = 0;
+      FarField<NT>::template force<T>(dx, dy, dz, rs, M, fx, fy, fz);
+      row[i] += (double)fx;
+      row[kGroupMax + i] += (double)fy;
+      row[2 * kGroupMax + i] += (double)fz;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int i = tid; i < tc; i += 32 * NW) {
+    double sx = 0, sy = 0, sz = 0;
+    for (int q = 0; q < NW; q++) {
+      sx += accb[q * 3 * kGroupMax + i];
+      sy += accb[q * 3 * kGroupMax + kGroupMax + i];
+      sz += accb[q * 3 * kGroupMax + 2 * kGroupMax + i];
+    }
+    a.out[t0 + i] = sx;
+    a.out_y[t0 + i] = sy;
+    a.out_z[t0 + i] = sz;
   }
 }
 
-template <int NT, int KER>
-void launch_far(Tree* t, Lists* L, bool f32, double add, double kappa, double sign,
-                const double* tx, const double* ty, const double* tz, double* out) {
-  const unsigned g = grid_for(L->nbatch, FWARPS);
-  cudaStream_t s = t->ctx->stream;
-  if (f32)
-    count_launch(), k_far<NT, KER, float><<<g, 32 * FWARPS, 0, s>>>(L->nbatch, L->order.p, L->b_tstart.p,
-                                                    L->b_tcount.p, tx, ty, tz, L->far_off.p,
-                                                    L->far_ent.p, t->nodec.p, t->mom32.p, add,
-                                                    kappa, sign, out);
-  else
-    count_launch(), k_far<NT, KER, double><<<g, 32 * FWARPS, 0, s>>>(L->nbatch, L->order.p, L->b_tstart.p,
-                                                     L->b_tcount.p, tx, ty, tz, L->far_off.p,
-                                                     L->far_ent.p, t->nodec.p, t->mom64.p, add,
-                                                     kappa, sign, out);
+template <class K>
+void set_smem(K kernel, size_t bytes) {
+  // once per (kernel, device)
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+  if (done.count(key)) return;
+  BIT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done.insert(key);
 }
 
-template <int NT>
-void launch_far_force(Tree* t, Lists* L, bool f32, double del, double* fx, double* fy,
-                      double* fz) {
-  const unsigned g = grid_for(L->nbatch, FWARPS);
-  cudaStream_t s = t->ctx->stream;
-  if (f32)
-    count_launch(), k_far_force<NT, float><<<g, 32 * FWARPS, 0, s>>>(L->nbatch, L->order.p, L->b_tstart.p,
-                                                     L->b_tcount.p, t->sx.p, t->sy.p, t->sz.p,
-                                                     L->far_off.p, L->far_ent.p, t->nodec.p,
-                                                     t->mom32.p, del, fx, fy, fz);
-  else
-    count_launch(), k_far_force<NT, double><<<g, 32 * FWARPS, 0, s>>>(L->nbatch, L->order.p, L->b_tstart.p,
-                                                      L->b_tcount.p, t->sx.p, t->sy.p, t->sz.p,
-                                                      L->far_off.p, L->far_ent.p, t->nodec.p,
-                                                      t->mom64.p, del, fx, fy, fz);
+template <int NT, int KER, class T>
+void launch_far(const FarArgs& a, int ng, cudaStream_t s) {
+  const size_t bytes = far_smem<NWP>(WarpAcc<T>::words * sizeof(T), num_terms(NT) * sizeof(T));
+  set_smem(k_far<NT, KER, T>, bytes);
+  count_launch(), k_far<NT, KER, T><<<ng, 32 * NWP, bytes, s>>>(a);
+}
+
+template <int NT, class T>
+void launch_force(const FarArgs& a, int ng, cudaStream_t s) {
+  const size_t bytes = far_smem<NWF>(3 * sizeof(double), num_terms(NT) * sizeof(T));
+  set_smem(k_far_force<NT, T>, bytes);
+  count_launch(), k_far_force<NT, T><<<ng, 32 * NWF, bytes, s>>>(a);
+}
+
+FarArgs far_args(Tree* t, Lists* L, const double* tx, const double* ty, const double* tz,
+                 bool f32) {
+  FarArgs a{};
+  a.order = L->order.p;
+  a.g_tstart = L->g_tstart.p;
+  a.g_tcount = L->g_tcount.p;
+  a.tx = tx; a.ty = ty; a.tz = tz;
+  a.off = L->far_off.p;
+  a.moff = L->far_moff.p;
+  a.node = L->far_node.p;
+  a.mask = L->far_mask.p;
+  a.nodec = t->nodec.p;
+  a.mom = f32 ? (const void*)t->mom32.p : (const void*)t->mom64.p;
+  return a;
 }
 
 }  // namespace
@@ -152,15 +255,25 @@ void launch_far_force(Tree* t, Lists* L, bool f32, double del, double* fx, doubl
 void eval_far(Tree* t, Lists* L, const bit_eval_params& p, int /*points*/, const double* tx,
               const double* ty, const double* tz, double* out) {
   const bool f32 = p.precision == BIT_PREC_MIXED;
+  FarArgs a = far_args(t, L, tx, ty, tz, f32);
   // distance^2 fed to the recurrence: r^2 + del (Coulomb, regularised screened) or r^2
-  const double add = p.kernel == BIT_KERNEL_SCREENED ? 0.0 : p.del;
-  const double sign = p.kernel == BIT_KERNEL_SCREENED ? -1.0 : 1.0;  // :3222 subtracts
+  a.add = p.kernel == BIT_KERNEL_SCREENED ? 0.0 : p.del;
+  a.kappa = p.kappa;
+  a.sign = p.kernel == BIT_KERNEL_SCREENED ? -1.0 : 1.0;  // src/tree3d.cpp:3222 subtracts
+  a.out = out;
   const bool coul = p.kernel == BIT_KERNEL_COULOMB;
+  cudaStream_t s = t->ctx->stream;
+  const int ng = L->ngroups;
   switch (t->nterms) {
-#define CASE(N)                                                                            \
-  case N:                                                                                  \
-    if (coul) launch_far<N, BIT_KERNEL_COULOMB>(t, L, f32, add, p.kappa, sign, tx, ty, tz, out); \
-    else launch_far<N, BIT_KERNEL_SCREENED>(t, L, f32, add, p.kappa, sign, tx, ty, tz, out); \
+#define CASE(N)                                                                   \
+  case N:                                                                         \
+    if (f32) {                                                                    \
+      if (coul) launch_far<N, BIT_KERNEL_COULOMB, float>(a, ng, s);               \
+      else launch_far<N, BIT_KERNEL_SCREENED, float>(a, ng, s);                   \
+    } else {                                                                      \
+      if (coul) launch_far<N, BIT_KERNEL_COULOMB, double>(a, ng, s);              \
+      else launch_far<N, BIT_KERNEL_SCREENED, double>(a, ng, s);                  \
+    }                                                                             \
     break;
     CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
 #undef CASE
@@ -173,8 +286,17 @@ void eval_far(Tree* t, Lists* L, const bit_eval_params& p, int /*points*/, const
 void eval_far_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
                     double* fz) {
   const bool f32 = prec == BIT_PREC_MIXED;
+  FarArgs a = far_args(t, L, t->sx.p, t->sy.p, t->sz.p, f32);
+  a.add = del;
+  a.out = fx; a.out_y = fy; a.out_z = fz;
+  cudaStream_t s = t->ctx->stream;
+  const int ng = L->ngroups;
   switch (t->nterms) {
-#define CASE(N) case N: launch_far_force<N>(t, L, f32, del, fx, fy, fz); break;
+#define CASE(N)                                           \
+  case N:                                                 \
+    if (f32) launch_force<N, float>(a, ng, s);            \
+    else launch_force<N, double>(a, ng, s);               \
+    break;
     CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
 #undef CASE
     default:

@@ -1,28 +1,53 @@
 // Near field: the leaf direct sums of treepotential / shielded_treepot / treeforce
-// (src/tree3d.cpp:4737-4774, 3539-3623, 923-967) over each batch's near entries.
+// (src/tree3d.cpp:4737-4774, 3539-3623, 923-967), one CTA per target group.
 //
-// One warp per batch, one target per lane; the leaf's sources are contiguous in tree
-// order and every active lane reads the same source at the same time (one broadcast
-// transaction).  FP64 path: the reference's arithmetic.  Mixed path: sources in FP32
-// relative to their leaf centre, the target's offset from that centre formed in FP64 and
-// rounded once, MUFU rsqrt / ex2, and per-target compensated (two-sum) accumulation of
-// 8-term partial sums.
+// For each near entry (source leaf, bitmask over the group's targets) the CTA packs the
+// targets that need the leaf into a dense list, and when fewer than half the threads
+// would be busy it splits the leaf's sources across 2..32 threads per target (partial
+// sums combined by warp shuffles).  Source tiles are staged in shared memory by TMA bulk
+// copies (cp.async.bulk with an mbarrier), double buffered so the next tile streams in
+// while the current one is consumed; every thread then reads each source from shared
+// memory, broadcast across the targets.  Accumulation per target is in shared memory in a
+// fixed order, so results are deterministic.
+//
+// FP64 path: the reference's arithmetic.  Mixed path: sources in FP32 relative to their
+// leaf centre, the target's offset from that centre formed in FP64 and rounded once, MUFU
+// rsqrt / ex2, and per-target compensated (two-sum) accumulation.
+#include <climits>
+
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace bit {
 
 namespace {
 
-constexpr int NWARPS = 4;
+constexpr int NT = 256;  // threads per CTA
 
 struct NearSpec {
-  double del;    // added to r^2
+  double del;     // added to r^2
   double kappa;
-  double intg;   // reference-mode screened self term
-  int eps_check; // skip r^2 <= 1e-14
-  int self_term; // 1: add q*intg/w for j == p
-  int sign;      // +1 / -1
-  int particles; // targets are the sources (self excluded by position)
+  double intg;    // reference-mode screened self term
+  int eps_check;  // skip r^2 <= 1e-14
+  int self_term;  // 1: add q*intg/w for j == p
+  int sign;       // +1 / -1
+  int particles;  // targets are the sources (self excluded by position)
+};
+
+struct NearArgs {
+  const int *order, *g_tstart, *g_tcount, *g_own;
+  const double *tx, *ty, *tz;
+  const long long *off, *moff;
+  const int* node;
+  const unsigned* mask;
+  const int *start, *nummemb;
+  const double4* nodec;
+  const void* src;  // float4 (mixed) or double4 (FP64) in tree order
+  const double4* src64;
+  const double* sw;
+  NearSpec sp;
+  double *out, *out_y, *out_z;  // potential, or the three field components
+  int* err;
 };
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
@@ -35,7 +60,7 @@ __device__ __forceinline__ float ex2_approx(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-// Knuth two-sum: s + e == a + b exactly.
+// Knuth two-sum: s + e accumulates b with the rounding error of each step kept in e.
 __device__ __forceinline__ void two_sum(float& s, float& e, float b) {
   float t = s + b;
   float bp = t - s;
@@ -43,11 +68,35 @@ __device__ __forceinline__ void two_sum(float& s, float& e, float b) {
   s = t;
 }
 
-// Self handling of particle targets: the batch's own leaf is the one near entry that
-// can contain the target itself; every other entry runs without a per-source check.
+template <bool F32>
+struct Prec;
+template <>
+struct Prec<true> {
+  using S = float4;
+  using T = float;
+  static constexpr int TILE = 1024;
+};
+template <>
+struct Prec<false> {
+  using S = double4;
+  using T = double;
+  static constexpr int TILE = 512;
+};
+
+// One pair's contribution.  Mixed: target and source relative to the source leaf centre.
 template <int KER, bool EPS>
-__device__ __forceinline__ double pair64(double x, double y, double z, double4 s, double del,
-                                         double kappa) {
+__device__ __forceinline__ float pair(float xt, float yt, float zt, float4 s, float del,
+                                      float kl2) {
+  const float dx = s.x - xt, dy = s.y - yt, dz = s.z - zt;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
+  const float ri = rsqrt_approx(r2);
+  float v = KER == BIT_KERNEL_COULOMB ? s.w * ri : s.w * ex2_approx(r2 * ri * kl2) * ri;
+  if (EPS && !(r2 > (float)kEpsNear)) v = 0.f;
+  return v;
+}
+template <int KER, bool EPS>
+__device__ __forceinline__ double pair(double x, double y, double z, double4 s, double del,
+                                       double kappa) {
   const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
   const double r2 = dx * dx + dy * dy + dz * dz + del;
   if (EPS && !(r2 > kEpsNear)) return 0.0;
@@ -55,208 +104,240 @@ __device__ __forceinline__ double pair64(double x, double y, double z, double4 s
   const double r = sqrt(r2);
   return s.w * exp(-kappa * r) / r;
 }
-
-template <int KER, bool EPS>
-__global__ void __launch_bounds__(32 * NWARPS)
-    k_near64(int nbatch, const int* order, const int* b_tstart, const int* b_tcount,
-             const int* b_leaf, const double* tx, const double* ty, const double* tz,
-             const long long* off, const int2* ent, const int* start, const int* nummemb,
-             const double4* src, const double* sw, NearSpec sp, double* out) {
-  const int lane = threadIdx.x & 31;
-  const int wi = blockIdx.x * NWARPS + (threadIdx.x >> 5);
-  if (wi >= nbatch) return;
-  const int b = order[wi];
-  const int t0 = b_tstart[b], tc = b_tcount[b];
-  const int own = sp.particles ? b_leaf[b] : -1;
-  const bool live = lane < tc;
-  const int tpos = sp.particles ? t0 + lane : -1;
-  double x = 0, y = 0, z = 0;
-  if (live) { x = tx[t0 + lane]; y = ty[t0 + lane]; z = tz[t0 + lane]; }
-  double acc = 0.0, self = 0.0;
-  for (long long e = off[b]; e < off[b + 1]; e++) {
-    const int2 en = ent[e];
-    if (!((unsigned(en.y) >> lane) & 1u)) continue;
-    const int j0 = start[en.x], j1 = j0 + nummemb[en.x];
-    if (en.x == own) {
-      for (int j = j0; j < j1; j++) {
-        const double4 s = src[j];
-        if (j == tpos) {
-          // added, not subtracted, by the reference (src/tree3d.cpp:3596)
-          if (sp.self_term) self += s.w * sp.intg / (sw ? sw[j] : 1.0);
-          continue;
-        }
-        acc += pair64<KER, EPS>(x, y, z, s, sp.del, sp.kappa);
-      }
-      continue;
-    }
-    int j = j0;
-    for (; j + 4 <= j1; j += 4) {
-      double4 s[4];
-#pragma unroll
-      for (int k = 0; k < 4; k++) s[k] = src[j + k];
-#pragma unroll
-      for (int k = 0; k < 4; k++) acc += pair64<KER, EPS>(x, y, z, s[k], sp.del, sp.kappa);
-    }
-    for (; j < j1; j++) acc += pair64<KER, EPS>(x, y, z, src[j], sp.del, sp.kappa);
-  }
-  if (live) out[t0 + lane] += sp.sign * acc + self;
+// Field of eval_grad_kernel_reg (src/tree3d.cpp:73-97), KERNEL_ORDER = 0:
+// q * (-(x_j - x) / (r * r^2)).
+__device__ __forceinline__ void fpair(float xt, float yt, float zt, float4 s, float del,
+                                      float& ax, float& ay, float& az) {
+  const float dx = xt - s.x, dy = yt - s.y, dz = zt - s.z;
+  const float rs = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
+  const float ri = rsqrt_approx(rs);
+  const float tq = s.w * ri * ri * ri;
+  ax = fmaf(dx, tq, ax); ay = fmaf(dy, tq, ay); az = fmaf(dz, tq, az);
+}
+__device__ __forceinline__ void fpair(double x, double y, double z, double4 s, double del,
+                                      double& ax, double& ay, double& az) {
+  const double dx = s.x - x, dy = s.y - y, dz = s.z - z;
+  const double rs = dx * dx + dy * dy + dz * dz + del;
+  const double r = sqrt(rs);
+  const double t = s.w / (r * rs);
+  ax -= dx * t; ay -= dy * t; az -= dz * t;
 }
 
-template <int KER, bool EPS>
-__device__ __forceinline__ float pair32(float xt, float yt, float zt, float4 s, float del,
-                                        float kl2) {
-  const float dx = s.x - xt, dy = s.y - yt, dz = s.z - zt;
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
-  const float ri = rsqrt_approx(r2);
-  float v;
-  if (KER == BIT_KERNEL_COULOMB) v = s.w * ri;
-  else v = s.w * ex2_approx(r2 * ri * kl2) * ri;
-  if (EPS && !(r2 > (float)kEpsNear)) v = 0.f;
+template <class T>
+__device__ __forceinline__ T shfl_sum(T v, int tpt) {
+  for (int o = tpt >> 1; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
-template <int KER, bool EPS>
-__global__ void __launch_bounds__(32 * NWARPS)
-    k_near32(int nbatch, const int* order, const int* b_tstart, const int* b_tcount,
-             const int* b_leaf, const double* tx, const double* ty, const double* tz,
-             const long long* off, const int2* ent, const int* start, const int* nummemb,
-             const double4* nodec, const float4* __restrict__ src, const double4* src64,
-             const double* sw, NearSpec sp, double* out) {
-  const int lane = threadIdx.x & 31;
-  const int wi = blockIdx.x * NWARPS + (threadIdx.x >> 5);
-  if (wi >= nbatch) return;
-  const int b = order[wi];
-  const int t0 = b_tstart[b], tc = b_tcount[b];
-  const int own = sp.particles ? b_leaf[b] : -1;
-  const bool live = lane < tc;
-  const int tpos = sp.particles ? t0 + lane : -1;
-  double x = 0, y = 0, z = 0;
-  if (live) { x = tx[t0 + lane]; y = ty[t0 + lane]; z = tz[t0 + lane]; }
-  const float del = (float)sp.del;
-  const float kl2 = (float)(-sp.kappa * 1.4426950408889634);  // -kappa * log2(e)
-  float hi = 0.f, lo = 0.f;
-  double self = 0.0;
-  for (long long e = off[b]; e < off[b + 1]; e++) {
-    const int2 en = ent[e];
-    if (!((unsigned(en.y) >> lane) & 1u)) continue;
-    const double4 c = nodec[en.x];
-    const float xt = (float)(x - c.x), yt = (float)(y - c.y), zt = (float)(z - c.z);
-    const int j0 = start[en.x], j1 = j0 + nummemb[en.x];
-    if (en.x == own) {
-      for (int jb = j0; jb < j1; jb += 8) {
-        float part = 0.f;
-        const int je = min(jb + 8, j1);
-        for (int j = jb; j < je; j++) {
-          if (j == tpos) {
-            if (sp.self_term) self += src64[j].w * sp.intg / (sw ? sw[j] : 1.0);
-            continue;
-          }
-          part += pair32<KER, EPS>(xt, yt, zt, src[j], del, kl2);
+// Shared-memory layout of one CTA.
+template <bool F32, bool FORCE>
+struct Smem {
+  using S = typename Prec<F32>::S;
+  static constexpr int TILE = Prec<F32>::TILE;
+  static constexpr int NACC = FORCE ? 3 : 1;
+  static constexpr size_t tiles = 2 * TILE * sizeof(S);
+  static constexpr size_t coords = 3 * kGroupMax * sizeof(double);
+  static constexpr size_t acc = 2 * NACC * kGroupMax * sizeof(double);
+  static constexpr size_t self = kGroupMax * sizeof(double);
+  static constexpr size_t list = kGroupMax * sizeof(int);
+  static constexpr size_t bars = 64;
+  static constexpr size_t total = tiles + coords + acc + self + list + bars;
+};
+
+// The whole near field of one group.  FORCE: the three field components instead of the
+// potential (Coulomb only).
+template <int KER, bool EPS, bool F32, bool FORCE>
+__global__ void __launch_bounds__(NT) k_near(NearArgs a) {
+  using P = Prec<F32>;
+  using S = typename P::S;
+  using T = typename P::T;
+  using L = Smem<F32, FORCE>;
+  constexpr int TILE = P::TILE;
+  extern __shared__ __align__(128) unsigned char sm[];
+  S* tiles = reinterpret_cast<S*>(sm);
+  double* cx = reinterpret_cast<double*>(sm + L::tiles);
+  double* cy = cx + kGroupMax;
+  double* cz = cy + kGroupMax;
+  double* accd = reinterpret_cast<double*>(sm + L::tiles + L::coords);
+  float* acch = reinterpret_cast<float*>(accd);  // mixed: hi [0,1024), lo [1024,2048)
+  double* selfv = reinterpret_cast<double*>(sm + L::tiles + L::coords + L::acc);
+  int* tl = reinterpret_cast<int*>(sm + L::tiles + L::coords + L::acc + L::self);
+  uint64_t* bar =
+      reinterpret_cast<uint64_t*>(sm + L::tiles + L::coords + L::acc + L::self + L::list);
+  __shared__ int s_cnt;
+
+  const int g = a.order[blockIdx.x];
+  const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
+  const int own = a.sp.particles ? a.g_own[g] : -1;
+  const int W = (tc + 31) >> 5;
+  const long long e0 = a.off[g], e1 = a.off[g + 1];
+  const long long m0 = a.moff[g];
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < tc; i += NT) {
+    cx[i] = a.tx[t0 + i]; cy[i] = a.ty[t0 + i]; cz[i] = a.tz[t0 + i];
+    selfv[i] = 0.0;
+  }
+  // the whole accumulator block (the mixed path views it as float hi / lo rows)
+  for (int k = tid; k < 2 * L::NACC * kGroupMax; k += NT) accd[k] = 0.0;
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (e0 < e1) {
+    const S* src = reinterpret_cast<const S*>(a.src);
+    const float del = (float)a.sp.del;
+    const float kl2 = (float)(-a.sp.kappa * 1.4426950408889634);  // -kappa*log2(e)
+    // job iterator: (entry e, first source of the tile in the entry's leaf)
+    long long e = e0;
+    int node = a.node[e];
+    int j0 = a.start[node], jn = a.nummemb[node];
+    int toff = 0;
+    if (tid == 0) {
+      const int cnt0 = min(TILE, jn);
+      fence_proxy_async();
+      mbar_expect_tx(&bar[0], cnt0 * (unsigned)sizeof(S));
+      tma_load_1d(tiles, src + j0, cnt0 * (unsigned)sizeof(S), &bar[0]);
+    }
+    int k = 0, tpt = 1, cnt = 0;
+    while (true) {
+      const int buf = k & 1;
+      const int ns = min(TILE, jn - toff);
+      if (toff == 0 && tid < 32) {
+        // pack the targets of this entry (warp 0)
+        unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
+        const int c = __popc(wd);
+        int pre = c;
+        for (int o = 1; o < 32; o <<= 1) {
+          int t = __shfl_up_sync(0xffffffffu, pre, o);
+          if (lane >= o) pre += t;
         }
-        two_sum(hi, lo, part);
+        int base = pre - c;
+        while (wd) {
+          const int b = __ffs(wd) - 1;
+          wd &= wd - 1;
+          tl[base++] = 32 * lane + b;
+        }
+        if (lane == 31) s_cnt = pre;
       }
-      continue;
-    }
-    int j = j0;
-    for (; j + 8 <= j1; j += 8) {
-      float4 s[8];
-#pragma unroll
-      for (int k = 0; k < 8; k++) s[k] = src[j + k];
-      float p0 = 0.f, p1 = 0.f;
-#pragma unroll
-      for (int k = 0; k < 8; k += 2) {
-        p0 += pair32<KER, EPS>(xt, yt, zt, s[k], del, kl2);
-        p1 += pair32<KER, EPS>(xt, yt, zt, s[k + 1], del, kl2);
+      // the next job streams into the other buffer while this one is consumed
+      long long ne = e;
+      int noff = toff + TILE;
+      if (noff >= jn) { ne = e + 1; noff = 0; }
+      if (tid == 0 && ne < e1) {
+        const int nd = a.node[ne];
+        const int cntn = min(TILE, a.nummemb[nd] - noff);
+        fence_proxy_async();
+        mbar_expect_tx(&bar[buf ^ 1], cntn * (unsigned)sizeof(S));
+        tma_load_1d(tiles + (buf ^ 1) * TILE, src + a.start[nd] + noff,
+                    cntn * (unsigned)sizeof(S), &bar[buf ^ 1]);
       }
-      two_sum(hi, lo, p0 + p1);
-    }
-    float part = 0.f;
-    for (; j < j1; j++) part += pair32<KER, EPS>(xt, yt, zt, src[j], del, kl2);
-    two_sum(hi, lo, part);
-  }
-  if (live) out[t0 + lane] += sp.sign * ((double)hi + (double)lo) + self;
-}
-
-// Field of the regularised Coulomb kernel, eval_grad_kernel_reg (src/tree3d.cpp:73-97)
-// with KERNEL_ORDER = 0: f += q * (-(x_j - x) / (r * r^2)), r^2 = |x_j - x|^2 + del.
-__global__ void __launch_bounds__(32 * NWARPS)
-    k_near_force64(int nbatch, const int* order, const int* b_tstart, const int* b_tcount,
-                   const double* tx, const double* ty, const double* tz, const long long* off,
-                   const int2* ent, const int* start, const int* nummemb, const double4* src,
-                   double del, int particles, double* fx, double* fy, double* fz) {
-  const int lane = threadIdx.x & 31;
-  const int wi = blockIdx.x * NWARPS + (threadIdx.x >> 5);
-  if (wi >= nbatch) return;
-  const int b = order[wi];
-  const int t0 = b_tstart[b], tc = b_tcount[b];
-  const bool live = lane < tc;
-  const int tpos = particles ? t0 + lane : -1;
-  double x = 0, y = 0, z = 0;
-  if (live) { x = tx[t0 + lane]; y = ty[t0 + lane]; z = tz[t0 + lane]; }
-  double ax = 0, ay = 0, az = 0;
-  for (long long e = off[b]; e < off[b + 1]; e++) {
-    const int2 en = ent[e];
-    if (!((unsigned(en.y) >> lane) & 1u)) continue;
-    const int j0 = start[en.x], j1 = j0 + nummemb[en.x];
-    for (int j = j0; j < j1; j++) {
-      if (j == tpos) continue;
-      const double4 s = src[j];
-      const double dx = s.x - x, dy = s.y - y, dz = s.z - z;
-      const double rs = dx * dx + dy * dy + dz * dz + del;
-      const double r = sqrt(rs);
-      const double temp = s.w / (r * rs);
-      ax -= dx * temp;
-      ay -= dy * temp;
-      az -= dz * temp;
-    }
-  }
-  if (live) { fx[t0 + lane] += ax; fy[t0 + lane] += ay; fz[t0 + lane] += az; }
-}
-
-__global__ void __launch_bounds__(32 * NWARPS)
-    k_near_force32(int nbatch, const int* order, const int* b_tstart, const int* b_tcount,
-                   const double* tx, const double* ty, const double* tz, const long long* off,
-                   const int2* ent, const int* start, const int* nummemb, const double4* nodec,
-                   const float4* src, double del, int particles, double* fx, double* fy,
-                   double* fz) {
-  const int lane = threadIdx.x & 31;
-  const int wi = blockIdx.x * NWARPS + (threadIdx.x >> 5);
-  if (wi >= nbatch) return;
-  const int b = order[wi];
-  const int t0 = b_tstart[b], tc = b_tcount[b];
-  const bool live = lane < tc;
-  const int tpos = particles ? t0 + lane : -1;
-  double x = 0, y = 0, z = 0;
-  if (live) { x = tx[t0 + lane]; y = ty[t0 + lane]; z = tz[t0 + lane]; }
-  const float d = (float)del;
-  float h[3] = {0, 0, 0}, l[3] = {0, 0, 0};
-  for (long long e = off[b]; e < off[b + 1]; e++) {
-    const int2 en = ent[e];
-    if (!((unsigned(en.y) >> lane) & 1u)) continue;
-    const double4 c = nodec[en.x];
-    const float xt = (float)(x - c.x), yt = (float)(y - c.y), zt = (float)(z - c.z);
-    const int j0 = start[en.x], j1 = j0 + nummemb[en.x];
-    for (int jb = j0; jb < j1; jb += 8) {
-      float p[3] = {0, 0, 0};
-      const int je = min(jb + 8, j1);
-      for (int j = jb; j < je; j++) {
-        if (j == tpos) continue;
-        const float4 s = src[j];
-        const float dx = s.x - xt, dy = s.y - yt, dz = s.z - zt;
-        const float rs = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, d)));
-        const float ri = rsqrt_approx(rs);
-        const float tq = s.w * ri * ri * ri;
-        p[0] = fmaf(-dx, tq, p[0]);
-        p[1] = fmaf(-dy, tq, p[1]);
-        p[2] = fmaf(-dz, tq, p[2]);
+      __syncthreads();
+      if (toff == 0) {
+        cnt = s_cnt;
+        tpt = 1;
+        while (tpt < 32 && cnt * tpt * 2 <= NT) tpt <<= 1;
       }
-      for (int a = 0; a < 3; a++) two_sum(h[a], l[a], p[a]);
+      if (!mbar_wait(&bar[buf], (k >> 1) & 1)) {
+        if (tid == 0) atomicOr(a.err, 2);
+        if (ne < e1) mbar_wait(&bar[buf ^ 1], ((k + 1) >> 1) & 1);  // let the other copy land
+        return;
+      }
+      const S* ts = tiles + buf * TILE;
+      const double4 c = a.nodec[node];
+      // tile index of target i's own source is i + selfbase (particle targets, own leaf)
+      const int selfbase = (node == own) ? (t0 - (j0 + toff)) : INT_MIN;
+      const int units = cnt * tpt;
+      const int lt = __ffs(tpt) - 1;
+      for (int u0 = 0; u0 < units; u0 += NT) {
+        const int u = u0 + tid;
+        const bool valid = u < units;
+        const int slot = u >> lt, slice = u & (tpt - 1);
+        const int i = valid ? tl[slot] : 0;
+        const int selfj = selfbase == INT_MIN ? -1 : i + selfbase;
+        if (!FORCE) {
+          T part = 0;
+          if (valid) {
+            if constexpr (F32) {
+              const float4* fs = reinterpret_cast<const float4*>(ts);
+              const float xt = (float)(cx[i] - c.x), yt = (float)(cy[i] - c.y),
+                          zt = (float)(cz[i] - c.z);
+              float p0 = 0.f, p1 = 0.f;
+              int j = slice;
+              for (; j + tpt < ns; j += 2 * tpt) {
+                const float v0 = pair<KER, EPS>(xt, yt, zt, fs[j], del, kl2);
+                const float v1 = pair<KER, EPS>(xt, yt, zt, fs[j + tpt], del, kl2);
+                p0 += (j == selfj) ? 0.f : v0;
+                p1 += (j + tpt == selfj) ? 0.f : v1;
+              }
+              if (j < ns && j != selfj) p0 += pair<KER, EPS>(xt, yt, zt, fs[j], del, kl2);
+              part = p0 + p1;
+            } else {
+              const double4* ds = reinterpret_cast<const double4*>(ts);
+              double p = 0.0;
+              for (int j = slice; j < ns; j += tpt)
+                if (j != selfj) p += pair<KER, EPS>(cx[i], cy[i], cz[i], ds[j], a.sp.del, a.sp.kappa);
+              part = p;
+            }
+            if (a.sp.self_term && selfj >= 0 && selfj < ns && ((selfj - slice) & (tpt - 1)) == 0) {
+              const int jg = j0 + toff + selfj;  // added, not subtracted (src/tree3d.cpp:3596)
+              selfv[i] = a.src64[jg].w * a.sp.intg / (a.sw ? a.sw[jg] : 1.0);
+            }
+          }
+          part = shfl_sum(part, tpt);
+          if (valid && slice == 0) {
+            if constexpr (F32) two_sum(acch[i], acch[kGroupMax + i], (float)part);
+            else accd[i] += (double)part;
+          }
+        } else {
+          T fx = 0, fy = 0, fz = 0;
+          if (valid) {
+            if constexpr (F32) {
+              const float4* fs = reinterpret_cast<const float4*>(ts);
+              const float xt = (float)(cx[i] - c.x), yt = (float)(cy[i] - c.y),
+                          zt = (float)(cz[i] - c.z);
+              for (int j = slice; j < ns; j += tpt)
+                if (j != selfj) fpair(xt, yt, zt, fs[j], del, fx, fy, fz);
+            } else {
+              const double4* ds = reinterpret_cast<const double4*>(ts);
+              for (int j = slice; j < ns; j += tpt)
+                if (j != selfj) fpair(cx[i], cy[i], cz[i], ds[j], a.sp.del, fx, fy, fz);
+            }
+          }
+          fx = shfl_sum(fx, tpt);
+          fy = shfl_sum(fy, tpt);
+          fz = shfl_sum(fz, tpt);
+          if (valid && slice == 0) {
+            accd[i] += (double)fx;
+            accd[kGroupMax + i] += (double)fy;
+            accd[2 * kGroupMax + i] += (double)fz;
+          }
+        }
+      }
+      __syncthreads();
+      k++;
+      if (ne >= e1) break;
+      if (ne != e) {
+        e = ne;
+        node = a.node[e];
+        j0 = a.start[node];
+        jn = a.nummemb[node];
+      }
+      toff = noff;
     }
   }
-  if (live) {
-    fx[t0 + lane] += (double)h[0] + (double)l[0];
-    fy[t0 + lane] += (double)h[1] + (double)l[1];
-    fz[t0 + lane] += (double)h[2] + (double)l[2];
+  __syncthreads();
+  for (int i = tid; i < tc; i += NT) {
+    if (FORCE) {
+      a.out[t0 + i] += accd[i];
+      a.out_y[t0 + i] += accd[kGroupMax + i];
+      a.out_z[t0 + i] += accd[2 * kGroupMax + i];
+    } else if (F32) {
+      a.out[t0 + i] += a.sp.sign * ((double)acch[i] + (double)acch[kGroupMax + i]) + selfv[i];
+    } else {
+      a.out[t0 + i] += a.sp.sign * accd[i] + selfv[i];
+    }
   }
 }
 
@@ -275,8 +356,8 @@ NearSpec make_spec(const bit_eval_params& p, int points) {
       break;
     case BIT_KERNEL_SCREENED:
       s.del = 0.0;
-      s.eps_check = points ? 1 : 0;          // :3557 / :3604-3619
-      s.sign = (points && ref) ? 1 : -1;     // :3558 adds, :3619 subtracts
+      s.eps_check = points ? 1 : 0;            // :3557 / :3604-3619
+      s.sign = (points && ref) ? 1 : -1;       // :3558 adds, :3619 subtracts
       s.self_term = (!points && ref) ? 1 : 0;  // :3575-3596
       break;
     default:
@@ -288,54 +369,75 @@ NearSpec make_spec(const bit_eval_params& p, int points) {
   return s;
 }
 
+template <int KER, bool EPS, bool F32, bool FORCE>
+void launch(const NearArgs& a, int ngroups, cudaStream_t s) {
+  constexpr size_t bytes = Smem<F32, FORCE>::total;
+  static int done[64] = {0};  // once per kernel and device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !done[dev]) {
+    BIT_CUDA(cudaFuncSetAttribute(k_near<KER, EPS, F32, FORCE>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done[dev] = 1;
+  }
+  count_launch(), k_near<KER, EPS, F32, FORCE><<<ngroups, NT, bytes, s>>>(a);
+}
+
+NearArgs base_args(Tree* t, Lists* L, const double* tx, const double* ty, const double* tz,
+                   bool f32) {
+  NearArgs a{};
+  a.order = L->order.p;
+  a.g_tstart = L->g_tstart.p;
+  a.g_tcount = L->g_tcount.p;
+  a.g_own = L->g_own.p;
+  a.tx = tx; a.ty = ty; a.tz = tz;
+  a.off = L->near_off.p;
+  a.moff = L->near_moff.p;
+  a.node = L->near_node.p;
+  a.mask = L->near_mask.p;
+  a.start = t->start.p;
+  a.nummemb = t->nummemb.p;
+  a.nodec = t->nodec.p;
+  a.src = f32 ? (const void*)t->src32.p : (const void*)t->src64.p;
+  a.src64 = t->src64.p;
+  a.sw = t->has_weights ? t->sw.p : nullptr;
+  a.err = t->ctx->dev_err();
+  return a;
+}
+
 }  // namespace
 
 void eval_near(Tree* t, Lists* L, const bit_eval_params& p, int points, const double* tx,
                const double* ty, const double* tz, double* out) {
   cudaStream_t s = t->ctx->stream;
-  const NearSpec sp = make_spec(p, points);
-  const unsigned g = grid_for(L->nbatch, NWARPS);
-  const double* sw = t->has_weights ? t->sw.p : nullptr;
   const bool f32 = p.precision == BIT_PREC_MIXED;
+  NearArgs a = base_args(t, L, tx, ty, tz, f32);
+  a.sp = make_spec(p, points);
+  a.out = out;
   const bool scr = p.kernel != BIT_KERNEL_COULOMB;
-#define ARGS64 L->nbatch, L->order.p, L->b_tstart.p, L->b_tcount.p, L->b_srcleaf.p, tx, ty, tz, \
-               L->near_off.p, L->near_ent.p, t->start.p, t->nummemb.p, t->src64.p, sw, sp, out
-#define ARGS32 L->nbatch, L->order.p, L->b_tstart.p, L->b_tcount.p, L->b_srcleaf.p, tx, ty, tz, \
-               L->near_off.p, L->near_ent.p, t->start.p, t->nummemb.p, t->nodec.p, t->src32.p, \
-               t->src64.p, sw, sp, out
-#define LAUNCH(K, E)                                                                   \
-  do {                                                                                 \
-    if (f32) k_near32<K, E><<<g, 32 * NWARPS, 0, s>>>(ARGS32);                         \
-    else k_near64<K, E><<<g, 32 * NWARPS, 0, s>>>(ARGS64);                             \
-  } while (0)
-  if (!scr) {
-    if (sp.eps_check) LAUNCH(BIT_KERNEL_COULOMB, true);
-    else LAUNCH(BIT_KERNEL_COULOMB, false);
+  const bool eps = a.sp.eps_check;
+#define GO(K, E, F) launch<K, E, F, false>(a, L->ngroups, s)
+  if (f32) {
+    if (!scr) { if (eps) GO(BIT_KERNEL_COULOMB, true, true); else GO(BIT_KERNEL_COULOMB, false, true); }
+    else { if (eps) GO(BIT_KERNEL_SCREENED, true, true); else GO(BIT_KERNEL_SCREENED, false, true); }
   } else {
-    if (sp.eps_check) LAUNCH(BIT_KERNEL_SCREENED, true);
-    else LAUNCH(BIT_KERNEL_SCREENED, false);
+    if (!scr) { if (eps) GO(BIT_KERNEL_COULOMB, true, false); else GO(BIT_KERNEL_COULOMB, false, false); }
+    else { if (eps) GO(BIT_KERNEL_SCREENED, true, false); else GO(BIT_KERNEL_SCREENED, false, false); }
   }
-#undef LAUNCH
-#undef ARGS64
-#undef ARGS32
-  count_launch();
+#undef GO
   BIT_CHECK_LAUNCH();
 }
 
 void eval_near_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
                      double* fz) {
   cudaStream_t s = t->ctx->stream;
-  const unsigned g = grid_for(L->nbatch, NWARPS);
-  if (prec == BIT_PREC_MIXED)
-    count_launch(), k_near_force32<<<g, 32 * NWARPS, 0, s>>>(L->nbatch, L->order.p, L->b_tstart.p, L->b_tcount.p,
-                                             t->sx.p, t->sy.p, t->sz.p, L->near_off.p,
-                                             L->near_ent.p, t->start.p, t->nummemb.p,
-                                             t->nodec.p, t->src32.p, del, 1, fx, fy, fz);
-  else
-    count_launch(), k_near_force64<<<g, 32 * NWARPS, 0, s>>>(L->nbatch, L->order.p, L->b_tstart.p, L->b_tcount.p,
-                                             t->sx.p, t->sy.p, t->sz.p, L->near_off.p,
-                                             L->near_ent.p, t->start.p, t->nummemb.p,
-                                             t->src64.p, del, 1, fx, fy, fz);
+  const bool f32 = prec == BIT_PREC_MIXED;
+  NearArgs a = base_args(t, L, t->sx.p, t->sy.p, t->sz.p, f32);
+  a.sp.del = del;
+  a.sp.particles = 1;
+  a.out = fx; a.out_y = fy; a.out_z = fz;
+  if (f32) launch<BIT_KERNEL_COULOMB, false, true, true>(a, L->ngroups, s);
+  else launch<BIT_KERNEL_COULOMB, false, false, true>(a, L->ngroups, s);
   BIT_CHECK_LAUNCH();
 }
 
