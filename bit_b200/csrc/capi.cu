@@ -630,13 +630,16 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
     std::vector<std::pair<int, int>> all;
     for (int kd = 0; kd < 2; kd++) {
       const DBuf<long long>& off = kd ? L.near_off : L.far_off;
+      const DBuf<int>& cntb = kd ? L.near_cnt : L.far_cnt;
       const DBuf<long long>& moff = kd ? L.near_moff : L.far_moff;
       const DBuf<int>& nd = kd ? L.near_node : L.far_node;
       const DBuf<unsigned>& mk = kd ? L.near_mask : L.far_mask;
-      long long o[2], mo = 0;
-      d2h(c, o, off.p + g, 2 * sizeof(long long));
+      long long o[1], mo = 0;
+      int ecount = 0;
+      d2h(c, o, off.p + g, sizeof(long long));
+      d2h(c, &ecount, cntb.p + g, sizeof(int));
       d2h(c, &mo, moff.p + g, sizeof(long long));
-      const long long ne = o[1] - o[0];
+      const long long ne = ecount;
       if (!ne) continue;
       std::vector<int> nodes(ne);
       std::vector<unsigned> masks(ne * W);

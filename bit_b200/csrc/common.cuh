@@ -95,8 +95,9 @@ struct Lists {
   long long nfar = 0, nnear = 0;            // entries
   long long far_pairs = 0, near_pairs = 0;  // interactions
   DBuf<int> g_tstart, g_tcount, g_own;      // group: first target, count, own leaf (or -1)
-  DBuf<long long> far_off, near_off;        // first entry of each group (ngroups + 1)
-  DBuf<long long> far_moff, near_moff;      // first mask word of each group (ngroups + 1)
+  DBuf<long long> far_off, near_off;        // first entry of each group
+  DBuf<int> far_cnt, near_cnt;              // entries of each group
+  DBuf<long long> far_moff, near_moff;      // first mask word of each group
   DBuf<int> far_node, near_node;            // entry -> node
   DBuf<unsigned> far_mask, near_mask;       // (tcount+31)/32 words per entry
   DBuf<int> order;                          // groups by decreasing work

@@ -24,6 +24,20 @@ __device__ __forceinline__ double exp_t(double x) { return exp(x); }
 __device__ __forceinline__ float exp_t(float x) { return expf(x); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+template <class T>
+struct V4 {
+  T x, y, z, w;
+};
+// Four consecutive moments; M is 16-byte aligned.
+__device__ __forceinline__ V4<float> ld4(const float* M, int q) {
+  const float4 v = reinterpret_cast<const float4*>(M)[q];
+  return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ V4<double> ld4(const double* M, int q) {
+  const double2 a = reinterpret_cast<const double2*>(M)[2 * q];
+  const double2 b = reinterpret_cast<const double2*>(M)[2 * q + 1];
+  return {a.x, a.y, b.x, b.y};
+}
 }  // namespace bit
 
 #include "generated/farfield_gen.cuh"
@@ -36,6 +50,7 @@ struct FarArgs {
   const int *order, *g_tstart, *g_tcount;
   const double *tx, *ty, *tz;
   const long long *off, *moff;
+  const int* cnt;
   const int* node;
   const unsigned* mask;
   const double4* nodec;
@@ -98,6 +113,7 @@ constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
 template <int NT, int KER, class T>
 __global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
   constexpr int TT = num_terms(NT);
+  constexpr int TP = FarField<NT>::kPadded;
   constexpr int NW = NWP;
   extern __shared__ __align__(16) unsigned char sm[];
   double* cx = reinterpret_cast<double*>(sm);
@@ -111,7 +127,7 @@ __global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
   const int g = a.order[blockIdx.x];
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int W = (tc + 31) >> 5;
-  const long long e0 = a.off[g], e1 = a.off[g + 1], m0 = a.moff[g];
+  const long long e0 = a.off[g], e1 = e0 + a.cnt[g], m0 = a.moff[g];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   for (int i = tid; i < tc; i += 32 * NW) {
     cx[i] = a.tx[t0 + i]; cy[i] = a.ty[t0 + i]; cz[i] = a.tz[t0 + i];
@@ -127,8 +143,9 @@ __global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
     const int cnt = warp_pack(wd, tl);
     const int node = a.node[e];
     const double4 c = a.nodec[node];
-    T* M = msb + w * TT;
-    for (int k = lane; k < TT; k += 32) M[k] = mom[(long long)node * TT + k];
+    T* M = msb + w * TP;
+    for (int k = lane; k < TP; k += 32)
+      M[k] = k < TT ? mom[(long long)node * TT + FarField<NT>::canon(k)] : T(0);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
       const int i = tl[r];
@@ -152,6 +169,7 @@ __global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
 template <int NT, class T>
 __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
   constexpr int TT = num_terms(NT);
+  constexpr int TP = FarField<NT>::kPadded;
   constexpr int NW = NWF;
   extern __shared__ __align__(16) unsigned char sm[];
   double* cx = reinterpret_cast<double*>(sm);
@@ -164,7 +182,7 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
   const int g = a.order[blockIdx.x];
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int W = (tc + 31) >> 5;
-  const long long e0 = a.off[g], e1 = a.off[g + 1], m0 = a.moff[g];
+  const long long e0 = a.off[g], e1 = e0 + a.cnt[g], m0 = a.moff[g];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   for (int i = tid; i < tc; i += 32 * NW) {
     cx[i] = a.tx[t0 + i]; cy[i] = a.ty[t0 + i]; cz[i] = a.tz[t0 + i];
@@ -179,8 +197,9 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
     const int cnt = warp_pack(wd, tl);
     const int node = a.node[e];
     const double4 c = a.nodec[node];
-    T* M = msb + w * TT;
-    for (int k = lane; k < TT; k += 32) M[k] = mom[(long long)node * TT + k];
+    T* M = msb + w * TP;
+    for (int k = lane; k < TP; k += 32)
+      M[k] = k < TT ? mom[(long long)node * TT + FarField<NT>::canon(k)] : T(0);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
       const int i = tl[r];
@@ -222,14 +241,14 @@ void set_smem(K kernel, size_t bytes) {
 
 template <int NT, int KER, class T>
 void launch_far(const FarArgs& a, int ng, cudaStream_t s) {
-  const size_t bytes = far_smem<NWP>(WarpAcc<T>::words * sizeof(T), num_terms(NT) * sizeof(T));
+  const size_t bytes = far_smem<NWP>(WarpAcc<T>::words * sizeof(T), FarField<NT>::kPadded * sizeof(T));
   set_smem(k_far<NT, KER, T>, bytes);
   count_launch(), k_far<NT, KER, T><<<ng, 32 * NWP, bytes, s>>>(a);
 }
 
 template <int NT, class T>
 void launch_force(const FarArgs& a, int ng, cudaStream_t s) {
-  const size_t bytes = far_smem<NWF>(3 * sizeof(double), num_terms(NT) * sizeof(T));
+  const size_t bytes = far_smem<NWF>(3 * sizeof(double), FarField<NT>::kPadded * sizeof(T));
   set_smem(k_far_force<NT, T>, bytes);
   count_launch(), k_far_force<NT, T><<<ng, 32 * NWF, bytes, s>>>(a);
 }
@@ -242,6 +261,7 @@ FarArgs far_args(Tree* t, Lists* L, const double* tx, const double* ty, const do
   a.g_tcount = L->g_tcount.p;
   a.tx = tx; a.ty = ty; a.tz = tz;
   a.off = L->far_off.p;
+  a.cnt = L->far_cnt.p;
   a.moff = L->far_moff.p;
   a.node = L->far_node.p;
   a.mask = L->far_mask.p;

@@ -1,5 +1,8 @@
 """Generate farfield_gen.cuh: unrolled far-field Taylor recurrences for nterms = 1..10.
 
+Moments are read in shell order (total degree, then i, then j descending: the order the
+coefficients are produced in) from a staging copy, four at a time.
+
 For every nterms and kernel this writes one straight-line device function that evaluates
 the Taylor coefficients of the cluster kernel degree by degree and folds each one into
 the moment dot product as soon as it exists, so only the last two degree shells stay live
@@ -49,6 +52,29 @@ def moment_index(nt):
     return out
 
 
+def shell_index(nt):
+    """Position of each (i, j, k), degree < nt, in the order the recurrences produce them."""
+    return {v: n for n, v in enumerate(shells(nt - 1))}
+
+
+def padded(n):
+    return (n + 3) // 4 * 4
+
+
+class MomentLoads:
+    """Moments are consumed in shell order: load them four at a time (16-byte vectors)."""
+
+    def __init__(self):
+        self.done = set()
+
+    def get(self, L, idx):
+        q = idx // 4
+        if q not in self.done:
+            L.append(f"  const V4<T> mv{q} = ld4(M, {q});")
+            self.done.add(q)
+        return f"mv{q}.{'xyzw'[idx % 4]}"
+
+
 def classify(v):
     nz = sum(1 for a in v if a == 0)
     n1 = sum(1 for a in v if a == 1)
@@ -95,14 +121,16 @@ def coul_expr(v):
 
 
 def gen_coulomb(nt):
-    mi = moment_index(nt)
+    mi = shell_index(nt)
+    ml = MomentLoads()
     L = ["  const T dx2 = T(2)*dx, dy2 = T(2)*dy, dz2 = T(2)*dz;",
          "  const T fac = T(1) / rs;",
          "  const T sqfac = sqrt_t(fac);",
          "  T s = T(0);"]
     for v in shells(nt - 1):
         L.append(f"  const T {name('b', v)} = {coul_expr(v)};")
-        L.append(f"  s = fma_t(M[{mi[v]}], {name('b', v)}, s);")
+        m = ml.get(L, mi[v])
+        L.append(f"  s = fma_t({m}, {name('b', v)}, s);")
     L.append("  return s;")
     return L
 
@@ -145,22 +173,25 @@ def scr_expr(v):
 
 
 def gen_screened(nt):
-    mi = moment_index(nt)
+    mi = shell_index(nt)
+    ml = MomentLoads()
     L = ["  const T dx2 = T(2)*dx, dy2 = T(2)*dy, dz2 = T(2)*dz;",
          "  const T kdx = kappa*dx, kdy = kappa*dy, kdz = kappa*dz;",
          "  const T rinv = rsqrt_t(dist2);",
          "  const T fac = rinv * rinv;",
          "  const T c0_0_0 = exp_t(-kappa * (dist2 * rinv));",
          "  const T a0_0_0 = c0_0_0 * rinv;",
-         "  T s = T(0);",
-         f"  s = fma_t(M[0], a0_0_0, s);"]
+         "  T s = T(0);"]
+    m = ml.get(L, 0)
+    L.append(f"  s = fma_t({m}, a0_0_0, s);")
     for v in shells(nt - 1):
         if v == (0, 0, 0):
             continue
         bexp, aexp = scr_expr(v)
         L.append(f"  const T {name('c', v)} = {bexp};")
         L.append(f"  const T {name('a', v)} = {aexp};")
-        L.append(f"  s = fma_t(M[{mi[v]}], {name('a', v)}, s);")
+        m = ml.get(L, mi[v])
+        L.append(f"  s = fma_t({m}, {name('a', v)}, s);")
     L.append("  return s;")
     return L
 
@@ -213,7 +244,7 @@ def force_expr(v):
 
 def gen_force(nt):
     """Field sum of treetaylorforce: returns (fx, fy, fz) through references."""
-    mi = moment_index(nt)
+    mi = shell_index(nt)
     L = ["  const T fac = T(1) / rs;",
          "  const T sqfac = sqrt_t(fac);",
          "  T sx = T(0), sy = T(0), sz = T(0);"]
@@ -242,7 +273,15 @@ def main(out):
              "namespace bit {",
              "template <int NT> struct FarField;"]
     for nt in range(1, 11):
+        canon = moment_index(nt)
+        order = list(shells(nt - 1))
+        table = [canon[v] for v in order] + [0] * (padded(len(order)) - len(order))
+        parts.append(f"__constant__ unsigned short kShellCanon{nt}[{len(table)}] = {{"
+                     + ", ".join(map(str, table)) + "};")
         parts.append(f"template <> struct FarField<{nt}> {{")
+        parts.append(f"  static constexpr int kPadded = {len(table)};")
+        parts.append("  // canonical (i outer, j, k inner) index of the k-th moment in shell order")
+        parts.append(f"  static __device__ __forceinline__ int canon(int k) {{ return kShellCanon{nt}[k]; }}")
         parts.append("  template <class T> static __device__ __forceinline__ T coulomb("
                      "T dx, T dy, T dz, T rs, const T* __restrict__ M) {")
         parts += gen_coulomb(nt)

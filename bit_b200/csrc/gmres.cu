@@ -48,9 +48,11 @@ __global__ void k_charges(int n, const double* w, const double* s, double* sq, d
   src32[e].w = (float)q;
 }
 
+// y = a x + b y; with b == 0, y is written without being read (it may be uninitialised,
+// e.g. a reused block holding NaN patterns).
 __global__ void k_axpby(int n, double a, const double* x, double b, double* y) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) y[e] = a * x[e] + b * y[e];
+  if (e < n) y[e] = b == 0.0 ? a * x[e] : a * x[e] + b * y[e];
 }
 
 // Sum over the block, returned to every thread.

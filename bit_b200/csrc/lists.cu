@@ -3,15 +3,18 @@
 //
 // A group is up to 1024 consecutive targets (a leaf, or a chunk of one; for external
 // points, 256 consecutive points in Morton order).  One CTA walks the tree for the group,
-// one thread per target, 32 mask words per node (one per warp).  At a node every active
-// target evaluates the reference's acceptance test in FP64 without contraction
+// one thread per target, one 32-bit mask word per warp.  At a node every active target
+// evaluates the reference's acceptance test in FP64 without contraction
 // (sqradius < acc * ((dx*dx + dy*dy + dz*dz + add) - sub)); the node becomes a far entry
 // for the accepting targets, and the others descend into the children in the reference's
 // children[] order, or get a near entry at a leaf.  Entries carry the group's bitmask.
 // Restricted to one target, the entries are exactly its reference traversal, in order.
 //
-// Two launches: one counts entries and mask words per group, the second writes them at
-// the prefix-summed offsets.
+// Single pass: each CTA stages its entries in shared memory, then reserves room in the
+// global lists with one atomic per list and copies them out (a group's entries stay
+// contiguous and in order; groups land in completion order, addressed by begin/count).
+// A group whose entries do not fit the staging area makes the whole build fall back to a
+// count pass, a prefix sum and a fill pass.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -22,26 +25,51 @@ namespace bit {
 
 namespace {
 
-constexpr int LT = 1024;   // threads of the list builder (one per target of a group)
-constexpr int LSTK = 256;  // traversal stack entries per group
+constexpr int LT = 1024;          // threads of the list builder (one per target of a group)
+constexpr int LSTK = 256;         // traversal stack entries per group
+constexpr int STAGE_FAR = 20480;  // staging words (node + mask words per entry), far list
+constexpr int STAGE_NEAR = 6144;  // staging words, near list
+constexpr size_t STAGE_BYTES = (STAGE_FAR + STAGE_NEAR) * sizeof(unsigned);
 
-template <bool FILL>
-__global__ void __launch_bounds__(LT)
-    k_lists(const int* g_tstart, const int* g_tcount, const double* tx, const double* ty,
-            const double* tz, const double4* nodec, const int* children, const int* nummemb,
-            double acc, double add, double sub, long long* far_cnt, long long* near_cnt,
-            long long* pair_cnt, const long long* far_off, const long long* near_off,
-            const long long* far_moff, const long long* near_moff, int* far_node,
-            unsigned* far_mask, int* near_node, unsigned* near_mask, int* err) {
+enum { MODE_COUNT = 0, MODE_FILL = 1, MODE_STAGE = 2 };
+
+struct ListArgs {
+  const int *g_tstart, *g_tcount;
+  const double *tx, *ty, *tz;
+  const double4* nodec;
+  const int *children, *nummemb;
+  double acc, add, sub;
+  // per group
+  long long *far_off, *near_off, *far_moff, *near_moff;
+  int *far_cnt, *near_cnt;
+  // lists
+  int *far_node, *near_node;
+  unsigned *far_mask, *near_mask;
+  unsigned long long* totals;  // far entries, far words, near entries, near words
+  unsigned long long* pairs;   // far pairs, near pairs
+  int* err;                    // 1: stack overflow, 2: staging overflow
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   __shared__ int s_node[LSTK];
   __shared__ unsigned s_mask[LSTK][32];
+  __shared__ unsigned s_am[32], s_rm[32];
+  __shared__ unsigned long long s_base[4];
+  extern __shared__ unsigned stage[];
   const int g = blockIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int t0 = g_tstart[g], tc = g_tcount[g];
+  const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int W = (tc + 31) >> 5;
   const int i = threadIdx.x;
+  // staging layout: far nodes | far masks, near nodes | near masks
+  const int fcap = STAGE_FAR / (W + 1), ncap = STAGE_NEAR / (W + 1);
+  int* sf_node = reinterpret_cast<int*>(stage);
+  unsigned* sf_mask = stage + fcap;
+  int* sn_node = reinterpret_cast<int*>(stage + STAGE_FAR);
+  unsigned* sn_mask = stage + STAGE_FAR + ncap;
   double x = 0, y = 0, z = 0;
-  if (i < tc) { x = tx[t0 + i]; y = ty[t0 + i]; z = tz[t0 + i]; }
+  if (i < tc) { x = a.tx[t0 + i]; y = a.ty[t0 + i]; z = a.tz[t0 + i]; }
   if (threadIdx.x == 0) s_node[0] = 0;
   if (lane == 0) {
     int live = tc - 32 * w;
@@ -49,43 +77,54 @@ __global__ void __launch_bounds__(LT)
   }
   int sp = 1;
   long long nf = 0, nn = 0, fpairs = 0, npairs = 0;
-  const long long fo = FILL ? far_off[g] : 0, no = FILL ? near_off[g] : 0;
-  const long long fmo = FILL ? far_moff[g] : 0, nmo = FILL ? near_moff[g] : 0;
-  bool overflow = false;
+  const long long fo = MODE == MODE_FILL ? a.far_off[g] : 0, no = MODE == MODE_FILL ? a.near_off[g] : 0;
+  const long long fmo = MODE == MODE_FILL ? a.far_moff[g] : 0, nmo = MODE == MODE_FILL ? a.near_moff[g] : 0;
+  bool overflow = false, full = false;
   __syncthreads();
+  // Two barriers per visited node: (1) after every warp has read the popped entry and
+  // published its accept / reject words, (2) after the pushes.
   while (sp > 0) {
     sp--;
     const int node = s_node[sp];
     const unsigned word = s_mask[sp][w];
-    __syncthreads();  // the popped slot may be overwritten below
     bool ok = false;
     if ((word >> lane) & 1u) {
-      const double4 c = nodec[node];
+      const double4 c = a.nodec[node];
       double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
       double s = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-      ok = c.w < dmul(acc, dsub(dadd(s, add), sub));
+      ok = c.w < dmul(a.acc, dsub(dadd(s, a.add), a.sub));
     }
     const unsigned am = __ballot_sync(0xffffffffu, ok) & word;
     const unsigned rm = word & ~am;
-    const int anyA = __syncthreads_or(lane == 0 && am != 0u);
-    const int anyR = __syncthreads_or(lane == 0 && rm != 0u);
+    if (lane == 0) { s_am[w] = am; s_rm[w] = rm; }
+    __syncthreads();
+    const bool anyA = __ballot_sync(0xffffffffu, s_am[lane] != 0u) != 0u;
+    const bool anyR = __ballot_sync(0xffffffffu, s_rm[lane] != 0u) != 0u;
     if (anyA) {
-      if (FILL) {
-        if (threadIdx.x == 0) far_node[fo + nf] = node;
-        if (lane == 0 && w < W) far_mask[fmo + nf * W + w] = am;
+      if (MODE == MODE_FILL) {
+        if (threadIdx.x == 0) a.far_node[fo + nf] = node;
+        if (lane == 0 && w < W) a.far_mask[fmo + nf * W + w] = am;
+      } else if (MODE == MODE_STAGE) {
+        if (nf >= fcap) { full = true; break; }
+        if (threadIdx.x == 0) sf_node[nf] = node;
+        if (lane == 0 && w < W) sf_mask[nf * W + w] = am;
       }
       nf++;
       if (lane == 0) fpairs += __popc(am);
     }
     if (anyR) {
-      const int* ch = children + 8LL * node;
+      const int* ch = a.children + 8LL * node;
       if (ch[0] == -1) {
-        if (FILL) {
-          if (threadIdx.x == 0) near_node[no + nn] = node;
-          if (lane == 0 && w < W) near_mask[nmo + nn * W + w] = rm;
+        if (MODE == MODE_FILL) {
+          if (threadIdx.x == 0) a.near_node[no + nn] = node;
+          if (lane == 0 && w < W) a.near_mask[nmo + nn * W + w] = rm;
+        } else if (MODE == MODE_STAGE) {
+          if (nn >= ncap) { full = true; break; }
+          if (threadIdx.x == 0) sn_node[nn] = node;
+          if (lane == 0 && w < W) sn_mask[nn * W + w] = rm;
         }
         nn++;
-        if (lane == 0) npairs += (long long)__popc(rm) * nummemb[node];
+        if (lane == 0) npairs += (long long)__popc(rm) * a.nummemb[node];
       } else {
         int cnt = 0;
         for (int k = 0; k < 8; k++) cnt += ch[k] != -1;
@@ -102,22 +141,40 @@ __global__ void __launch_bounds__(LT)
     }
     __syncthreads();
   }
+  if (threadIdx.x == 0 && (overflow || full)) atomicOr(a.err, overflow ? 1 : 2);
+  if (MODE != MODE_FILL && lane == 0 && (fpairs || npairs)) {
+    atomicAdd(&a.pairs[0], (unsigned long long)fpairs);
+    atomicAdd(&a.pairs[1], (unsigned long long)npairs);
+  }
+  if (MODE == MODE_COUNT && threadIdx.x == 0) {
+    a.far_cnt[g] = (int)nf;
+    a.near_cnt[g] = (int)nn;
+  }
+  if (MODE != MODE_STAGE || overflow || full) return;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    if (overflow) atomicOr(err, 1);
-    if (!FILL) {
-      far_cnt[g] = nf;
-      near_cnt[g] = nn;
-    }
+    s_base[0] = atomicAdd(&a.totals[0], (unsigned long long)nf);
+    s_base[1] = atomicAdd(&a.totals[1], (unsigned long long)(nf * W));
+    s_base[2] = atomicAdd(&a.totals[2], (unsigned long long)nn);
+    s_base[3] = atomicAdd(&a.totals[3], (unsigned long long)(nn * W));
+    a.far_off[g] = (long long)s_base[0];
+    a.far_moff[g] = (long long)s_base[1];
+    a.near_off[g] = (long long)s_base[2];
+    a.near_moff[g] = (long long)s_base[3];
+    a.far_cnt[g] = (int)nf;
+    a.near_cnt[g] = (int)nn;
   }
-  if (!FILL && lane == 0 && (fpairs || npairs)) {
-    atomicAdd((unsigned long long*)&pair_cnt[0], (unsigned long long)fpairs);
-    atomicAdd((unsigned long long*)&pair_cnt[1], (unsigned long long)npairs);
-  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nf; k += LT) a.far_node[s_base[0] + k] = sf_node[k];
+  for (int k = threadIdx.x; k < nf * W; k += LT) a.far_mask[s_base[1] + k] = sf_mask[k];
+  for (int k = threadIdx.x; k < nn; k += LT) a.near_node[s_base[2] + k] = sn_node[k];
+  for (int k = threadIdx.x; k < nn * W; k += LT) a.near_mask[s_base[3] + k] = sn_mask[k];
 }
 
-// Exclusive scan of long long counts times a per-element factor (one block), total in
-// out[n].  factor == nullptr: factor 1.
-__global__ void k_scan_ll(const long long* in, const int* tcount, long long* out, int n) {
+// Exclusive scan of int counts times a per-group factor (one block); the total goes to
+// *total.  tcount == nullptr: factor 1, else (tcount+31)/32 mask words per entry.
+__global__ void k_scan_cnt(const int* in, const int* tcount, long long* out, int n,
+                           unsigned long long* total) {
   __shared__ long long ws[32];
   __shared__ long long carry;
   if (threadIdx.x == 0) carry = 0;
@@ -125,7 +182,7 @@ __global__ void k_scan_ll(const long long* in, const int* tcount, long long* out
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int base = 0; base < n; base += blockDim.x) {
     int i = base + threadIdx.x;
-    long long v = i < n ? in[i] * (tcount ? (long long)((tcount[i] + 31) >> 5) : 1LL) : 0;
+    long long v = i < n ? (long long)in[i] * (tcount ? (long long)((tcount[i] + 31) >> 5) : 1LL) : 0;
     long long s = v;
     for (int o = 1; o < 32; o <<= 1) {
       long long t = __shfl_up_sync(0xffffffffu, s, o);
@@ -148,7 +205,17 @@ __global__ void k_scan_ll(const long long* in, const int* tcount, long long* out
     if (threadIdx.x == blockDim.x - 1) carry = pre + v;
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[n] = carry;
+  if (threadIdx.x == 0) *total = (unsigned long long)carry;
+}
+
+void set_stage_attr() {
+  static std::vector<int> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+  BIT_CUDA(cudaFuncSetAttribute(k_lists<MODE_STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)STAGE_BYTES));
+  done.push_back(dev);
 }
 
 }  // namespace
@@ -189,59 +256,91 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   BIT_CUDA(cudaMemcpyAsync(L->g_tstart.p, ts.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaMemcpyAsync(L->g_tcount.p, tc.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaMemcpyAsync(L->g_own.p, own.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
-  DBuf<long long> fcnt, ncnt, pairs;
-  DBuf<int> err;
-  fcnt.ensure(c, ng);
-  ncnt.ensure(c, ng);
-  pairs.ensure(c, 2);
-  err.ensure(c, 1);
-  L->far_off.ensure(c, ng + 1);
-  L->near_off.ensure(c, ng + 1);
-  L->far_moff.ensure(c, ng + 1);
-  L->near_moff.ensure(c, ng + 1);
-  BIT_CUDA(cudaMemsetAsync(pairs.p, 0, 2 * sizeof(long long), s));
-  BIT_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
-  count_launch(), k_lists<false><<<ng, LT, 0, s>>>(
-      L->g_tstart.p, L->g_tcount.p, tx, ty, tz, t->nodec.p, t->children.p, t->nummemb.p,
-      key.acc, key.add_del, key.sub_del, fcnt.p, ncnt.p, pairs.p, nullptr, nullptr, nullptr,
-      nullptr, nullptr, nullptr, nullptr, nullptr, err.p);
-  count_launch(), k_scan_ll<<<1, 1024, 0, s>>>(fcnt.p, nullptr, L->far_off.p, ng);
-  count_launch(), k_scan_ll<<<1, 1024, 0, s>>>(ncnt.p, nullptr, L->near_off.p, ng);
-  count_launch(), k_scan_ll<<<1, 1024, 0, s>>>(fcnt.p, L->g_tcount.p, L->far_moff.p, ng);
-  count_launch(), k_scan_ll<<<1, 1024, 0, s>>>(ncnt.p, L->g_tcount.p, L->near_moff.p, ng);
-  std::vector<long long> hf(ng), hn(ng);
-  long long* hp = c->h_pinned;
-  BIT_CUDA(cudaMemcpyAsync(hp, L->far_off.p + ng, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hp + 1, L->near_off.p + ng, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hp + 2, pairs.p, 2 * sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hp + 4, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hp + 5, L->far_moff.p + ng, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hp + 6, L->near_moff.p + ng, sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hf.data(), fcnt.p, ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hn.data(), ncnt.p, ng * sizeof(long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaStreamSynchronize(s));
-  if (*reinterpret_cast<int*>(hp + 4))
-    fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded (tree deeper than supported)");
-  L->nfar = hp[0];
-  L->nnear = hp[1];
-  L->far_pairs = hp[2];
-  L->near_pairs = hp[3];
-  L->far_node.ensure(c, L->nfar);
-  L->near_node.ensure(c, L->nnear);
-  L->far_mask.ensure(c, hp[5]);
-  L->near_mask.ensure(c, hp[6]);
-  count_launch(), k_lists<true><<<ng, LT, 0, s>>>(
-      L->g_tstart.p, L->g_tcount.p, tx, ty, tz, t->nodec.p, t->children.p, t->nummemb.p,
-      key.acc, key.add_del, key.sub_del, nullptr, nullptr, nullptr, L->far_off.p,
-      L->near_off.p, L->far_moff.p, L->near_moff.p, L->far_node.p, L->far_mask.p,
-      L->near_node.p, L->near_mask.p, err.p);
+  L->far_off.ensure(c, ng);
+  L->near_off.ensure(c, ng);
+  L->far_moff.ensure(c, ng);
+  L->near_moff.ensure(c, ng);
+  L->far_cnt.ensure(c, ng);
+  L->near_cnt.ensure(c, ng);
+  DBuf<unsigned long long> cnt;  // totals[4], pairs[2], err (as the 7th word)
+  cnt.ensure(c, 8);
+  BIT_CUDA(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s));
+  ListArgs a{};
+  a.g_tstart = L->g_tstart.p;
+  a.g_tcount = L->g_tcount.p;
+  a.tx = tx; a.ty = ty; a.tz = tz;
+  a.nodec = t->nodec.p;
+  a.children = t->children.p;
+  a.nummemb = t->nummemb.p;
+  a.acc = key.acc; a.add = key.add_del; a.sub = key.sub_del;
+  a.far_off = L->far_off.p; a.near_off = L->near_off.p;
+  a.far_moff = L->far_moff.p; a.near_moff = L->near_moff.p;
+  a.far_cnt = L->far_cnt.p; a.near_cnt = L->near_cnt.p;
+  a.totals = cnt.p;
+  a.pairs = cnt.p + 4;
+  a.err = reinterpret_cast<int*>(cnt.p + 6);
+  // worst case of the single pass: every group's staging area full
+  DBuf<int> snode_f, snode_n;
+  DBuf<unsigned> smask_f, smask_n;
+  snode_f.ensure(c, (size_t)ng * STAGE_FAR / 2);
+  smask_f.ensure(c, (size_t)ng * STAGE_FAR);
+  snode_n.ensure(c, (size_t)ng * STAGE_NEAR / 2);
+  smask_n.ensure(c, (size_t)ng * STAGE_NEAR);
+  a.far_node = snode_f.p; a.far_mask = smask_f.p;
+  a.near_node = snode_n.p; a.near_mask = smask_n.p;
+  set_stage_attr();
+  count_launch(), k_lists<MODE_STAGE><<<ng, LT, STAGE_BYTES, s>>>(a);
   BIT_CHECK_LAUNCH();
+  unsigned long long h[8];
+  std::vector<int> hf(ng), hn(ng);
+  BIT_CUDA(cudaMemcpyAsync(h, cnt.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(hf.data(), L->far_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(hn.data(), L->near_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaStreamSynchronize(s));
+  int err = (int)(h[6] & 0xffffffffu);
+  if (err & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded (tree deeper than supported)");
+  if (err & 2) {
+    // some group's lists exceed the staging area: count, scan, fill
+    BIT_CUDA(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s));
+    count_launch(), k_lists<MODE_COUNT><<<ng, LT, 0, s>>>(a);
+    count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->far_cnt.p, nullptr, L->far_off.p, ng, cnt.p + 0);
+    count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->far_cnt.p, L->g_tcount.p, L->far_moff.p, ng, cnt.p + 1);
+    count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->near_cnt.p, nullptr, L->near_off.p, ng, cnt.p + 2);
+    count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->near_cnt.p, L->g_tcount.p, L->near_moff.p, ng, cnt.p + 3);
+    BIT_CUDA(cudaMemcpyAsync(h, cnt.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(hf.data(), L->far_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(hn.data(), L->near_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    if ((int)(h[6] & 0xffffffffu) & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded");
+    L->far_node.ensure(c, h[0]);
+    L->far_mask.ensure(c, h[1]);
+    L->near_node.ensure(c, h[2]);
+    L->near_mask.ensure(c, h[3]);
+    a.far_node = L->far_node.p; a.far_mask = L->far_mask.p;
+    a.near_node = L->near_node.p; a.near_mask = L->near_mask.p;
+    count_launch(), k_lists<MODE_FILL><<<ng, LT, 0, s>>>(a);
+    BIT_CHECK_LAUNCH();
+  } else {
+    // exact-size copies of the staged lists
+    L->far_node.ensure(c, h[0]);
+    L->far_mask.ensure(c, h[1]);
+    L->near_node.ensure(c, h[2]);
+    L->near_mask.ensure(c, h[3]);
+    BIT_CUDA(cudaMemcpyAsync(L->far_node.p, snode_f.p, h[0] * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(L->far_mask.p, smask_f.p, h[1] * sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(L->near_node.p, snode_n.p, h[2] * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(L->near_mask.p, smask_n.p, h[3] * sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
+  }
+  L->nfar = (long long)h[0];
+  L->nnear = (long long)h[2];
+  L->far_pairs = (long long)h[4];
+  L->near_pairs = (long long)h[5];
   // heaviest groups first, so the evaluation kernels' tail is short
   std::vector<int> ord(ng);
   std::iota(ord.begin(), ord.end(), 0);
   std::vector<long long> wk(ng);
-  for (int g = 0; g < ng; g++) wk[g] = (40 * hf[g] + hn[g]) * (long long)tc[g];
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return wk[a] > wk[b]; });
+  for (int g = 0; g < ng; g++) wk[g] = (40LL * hf[g] + hn[g]) * (long long)tc[g];
+  std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return wk[x] > wk[y]; });
   L->order.ensure(c, ng);
   BIT_CUDA(cudaMemcpyAsync(L->order.p, ord.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaStreamSynchronize(s));

@@ -38,6 +38,7 @@ struct NearArgs {
   const int *order, *g_tstart, *g_tcount, *g_own;
   const double *tx, *ty, *tz;
   const long long *off, *moff;
+  const int* cnt;
   const int* node;
   const unsigned* mask;
   const int *start, *nummemb;
@@ -136,8 +137,9 @@ struct Smem {
   static constexpr int TILE = Prec<F32>::TILE;
   static constexpr int NACC = FORCE ? 3 : 1;
   static constexpr size_t tiles = 2 * TILE * sizeof(S);
-  static constexpr size_t coords = 3 * kGroupMax * sizeof(double);
-  static constexpr size_t acc = 2 * NACC * kGroupMax * sizeof(double);
+  static constexpr size_t coords = 0;  // target coordinates are read through L1
+  // mixed: float hi + lo per target; FP64: one double; force: three doubles
+  static constexpr size_t acc = (FORCE ? 3 : 1) * kGroupMax * sizeof(double);
   static constexpr size_t self = kGroupMax * sizeof(double);
   static constexpr size_t list = kGroupMax * sizeof(int);
   static constexpr size_t bars = 64;
@@ -155,9 +157,9 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
   constexpr int TILE = P::TILE;
   extern __shared__ __align__(128) unsigned char sm[];
   S* tiles = reinterpret_cast<S*>(sm);
-  double* cx = reinterpret_cast<double*>(sm + L::tiles);
-  double* cy = cx + kGroupMax;
-  double* cz = cy + kGroupMax;
+  const double* cx = a.tx + 0;  // group targets, indexed t0 + i below
+  const double* cy = a.ty + 0;
+  const double* cz = a.tz + 0;
   double* accd = reinterpret_cast<double*>(sm + L::tiles + L::coords);
   float* acch = reinterpret_cast<float*>(accd);  // mixed: hi [0,1024), lo [1024,2048)
   double* selfv = reinterpret_cast<double*>(sm + L::tiles + L::coords + L::acc);
@@ -170,15 +172,12 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int own = a.sp.particles ? a.g_own[g] : -1;
   const int W = (tc + 31) >> 5;
-  const long long e0 = a.off[g], e1 = a.off[g + 1];
+  const long long e0 = a.off[g], e1 = e0 + a.cnt[g];
   const long long m0 = a.moff[g];
   const int tid = threadIdx.x, lane = tid & 31;
-  for (int i = tid; i < tc; i += NT) {
-    cx[i] = a.tx[t0 + i]; cy[i] = a.ty[t0 + i]; cz[i] = a.tz[t0 + i];
-    selfv[i] = 0.0;
-  }
+  for (int i = tid; i < tc; i += NT) selfv[i] = 0.0;
   // the whole accumulator block (the mixed path views it as float hi / lo rows)
-  for (int k = tid; k < 2 * L::NACC * kGroupMax; k += NT) accd[k] = 0.0;
+  for (int k = tid; k < L::NACC * kGroupMax; k += NT) accd[k] = 0.0;
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
@@ -261,8 +260,8 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
           if (valid) {
             if constexpr (F32) {
               const float4* fs = reinterpret_cast<const float4*>(ts);
-              const float xt = (float)(cx[i] - c.x), yt = (float)(cy[i] - c.y),
-                          zt = (float)(cz[i] - c.z);
+              const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
+                          zt = (float)(cz[t0 + i] - c.z);
               float p0 = 0.f, p1 = 0.f;
               int j = slice;
               for (; j + tpt < ns; j += 2 * tpt) {
@@ -276,8 +275,9 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
             } else {
               const double4* ds = reinterpret_cast<const double4*>(ts);
               double p = 0.0;
+              const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
               for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) p += pair<KER, EPS>(cx[i], cy[i], cz[i], ds[j], a.sp.del, a.sp.kappa);
+                if (j != selfj) p += pair<KER, EPS>(x, y, z, ds[j], a.sp.del, a.sp.kappa);
               part = p;
             }
             if (a.sp.self_term && selfj >= 0 && selfj < ns && ((selfj - slice) & (tpt - 1)) == 0) {
@@ -295,14 +295,15 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
           if (valid) {
             if constexpr (F32) {
               const float4* fs = reinterpret_cast<const float4*>(ts);
-              const float xt = (float)(cx[i] - c.x), yt = (float)(cy[i] - c.y),
-                          zt = (float)(cz[i] - c.z);
+              const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
+                          zt = (float)(cz[t0 + i] - c.z);
               for (int j = slice; j < ns; j += tpt)
                 if (j != selfj) fpair(xt, yt, zt, fs[j], del, fx, fy, fz);
             } else {
               const double4* ds = reinterpret_cast<const double4*>(ts);
+              const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
               for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) fpair(cx[i], cy[i], cz[i], ds[j], a.sp.del, fx, fy, fz);
+                if (j != selfj) fpair(x, y, z, ds[j], a.sp.del, fx, fy, fz);
             }
           }
           fx = shfl_sum(fx, tpt);
@@ -392,6 +393,7 @@ NearArgs base_args(Tree* t, Lists* L, const double* tx, const double* ty, const 
   a.g_own = L->g_own.p;
   a.tx = tx; a.ty = ty; a.tz = tz;
   a.off = L->near_off.p;
+  a.cnt = L->near_cnt.p;
   a.moff = L->near_moff.p;
   a.node = L->near_node.p;
   a.mask = L->near_mask.p;

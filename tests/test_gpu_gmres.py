@@ -80,3 +80,19 @@ def test_bie_solution_is_the_same_alone_and_after_other_work(ctx):
     u.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.MIXED, del_=1e-4, acc=0.6))
     b, _, _ = t.bie_solve(p, 7, 0.5, area, f, tol=1e-8)
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("level,maxmemb", [(3, 100), (4, 200), (5, 500)])
+def test_bie_operator_matches_oracle(ctx, orc, level, maxmemb):
+    """The regularised-screened treecode on icosphere nodes (the BIE matvec) vs the oracle."""
+    import bit_b200 as B
+    cen, area, h, f = bie_problem(level)
+    q = area * np.random.default_rng(level).standard_normal(len(area))
+    t = ctx.treemake(cen[:, 0], cen[:, 1], cen[:, 2], maxmemb)
+    t.treemoments(q, 7)
+    T = orc.Tree(cen[:, 0], cen[:, 1], cen[:, 2], maxmemb)
+    T.compute_moments(q, 7)
+    for prec, tol in ((B.FP64, 1e-12), (B.MIXED, 1e-6)):
+        got = t.evaluate(B.params(B.SCREENED_REG, B.CONSISTENT, prec, del_=h * h, kappa=1.0, acc=0.5))
+        ref = T.evaluate(orc.params(orc.SCREENED_REG, orc.MODE_CONSISTENT, del_=h * h, kappa=1.0, acc=0.5))
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < tol, prec
