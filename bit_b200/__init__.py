@@ -114,6 +114,13 @@ SIGNATURES = [
     ("bit_bie_solve", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, C.c_double, _dp, _dp, _dp,
                                 C.POINTER(GmresOpts), C.POINTER(GmresInfo)]),
     ("bit_gmres_dense", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip]),
+    ("bit_forest_build", C.c_int, [_vp, C.c_int, _ip, _ip, _dp, _dp, _dp, C.POINTER(_vp)]),
+    ("bit_forest_build_device", C.c_int, [_vp, C.c_int, _ip, _ip, _vp, _vp, _vp,
+                                          C.POINTER(_vp)]),
+    ("bit_forest_moments", C.c_int, [_vp, _ip]),
+    ("bit_forest_eval", C.c_int, [_vp, C.POINTER(EvalParams), _dp]),
+    ("bit_forest_eval_device", C.c_int, [_vp, C.POINTER(EvalParams), _vp]),
+    ("bit_forest_systems", C.c_int, [_vp, _ip]),
 ]
 
 _lib = None
@@ -210,6 +217,10 @@ class Context:
                                           C.byref(prm), _d(out))
         self.check(st, "bit_treecode_potential")
         return out
+
+    def forest(self, x, y, z, sizes, maxmemb):
+        """Independent systems in one tree: system s is the next sizes[s] particles."""
+        return Forest(self, x, y, z, sizes, maxmemb)
 
     def gmres_dense(self, A, b, x0=None):
         """solver::gmres (src/solver.h:157) on the device."""
@@ -351,3 +362,63 @@ class Tree:
         if st not in (0, 7):
             self.ctx.check(st, "bit_bie_solve")
         return s, info.as_dict(), st
+
+
+class Forest(Tree):
+    """Many independent systems in one tree (bit_forest_build): system s owns the next
+    sizes[s] particles, is split with maxmemb[s] and rooted at node s.  Each system is
+    evaluated with its own parameters and expansion order, and its result equals a
+    separate single-system evaluation."""
+
+    def __init__(self, ctx, x, y, z, sizes, maxmemb):
+        self.ctx = ctx
+        self.h = _vp()
+        self.x, self.y, self.z = map(_f64, (x, y, z))
+        self.sizes = np.ascontiguousarray(sizes, dtype=np.int32)
+        self.nsys = len(self.sizes)
+        mm = np.broadcast_to(np.asarray(maxmemb, dtype=np.int32), (self.nsys,))
+        self.maxmembs = np.ascontiguousarray(mm)
+        self.n = int(self.sizes.sum())
+        if self.n != len(self.x):
+            raise ValueError("sizes must add up to the number of particles")
+        st = lib().bit_forest_build(ctx.h, self.nsys, self.sizes.ctypes.data_as(_ip),
+                                    self.maxmembs.ctypes.data_as(_ip), _d(self.x), _d(self.y),
+                                    _d(self.z), C.byref(self.h))
+        ctx.check(st, "bit_forest_build")
+        ctx._trees.add(self)
+        self.maxmemb = int(self.maxmembs.min())
+        self.nterms = 0
+        self.nterms_sys = np.zeros(self.nsys, np.int32)
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        lib().bit_tree_info(self.h, C.byref(a), C.byref(b), C.byref(c))
+        self.numtree, self.nleaves, self.depth = a.value, b.value, c.value
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+
+    def moments(self, nterms):
+        nt = np.ascontiguousarray(np.broadcast_to(np.asarray(nterms, np.int32), (self.nsys,)))
+        self.ctx.check(lib().bit_forest_moments(self.h, nt.ctypes.data_as(_ip)),
+                       "bit_forest_moments")
+        self.nterms_sys = nt.copy()
+        self.nterms = int(nt.max())
+
+    def export_moments(self):
+        raise NotImplementedError("forest moments differ in size per system; use export()")
+
+    def evaluate(self, prm, points=None):
+        """prm: one EvalParams for all systems, or a sequence of one per system."""
+        if points is not None:
+            raise ValueError("external points need a single-system tree")
+        arr = (EvalParams * self.nsys)()
+        if isinstance(prm, EvalParams):
+            prm = [prm] * self.nsys
+        if len(prm) != self.nsys:
+            raise ValueError("one parameter set per system expected")
+        for i, p in enumerate(prm):
+            arr[i] = p
+        out = np.zeros(self.n)
+        self.ctx.check(lib().bit_forest_eval(self.h, arr, _d(out)), "bit_forest_eval")
+        return out
+
+    def system(self, s, a):
+        """System s's slice of a per-particle array."""
+        return a[self.offsets[s]:self.offsets[s + 1]]

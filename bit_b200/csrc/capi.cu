@@ -1,6 +1,7 @@
 // The extern "C" boundary (include/bit_b200.h): argument checking, status codes, device
 // memory accounting, and the order of kernel phases for each entry point.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -146,32 +147,22 @@ void check_dev_err(Ctx* c) {
   }
 }
 
-void ensure_particle_lists(Tree* t, const bit_eval_params& p) {
-  ListKey k = mac_key(p, t->gen, 0);
-  if (t->plists.valid && t->plists.key == k) return;
-  ev_rec(t, EV_LIST);
-  build_lists(t, &t->plists, k, t->n, t->sx.p, t->sy.p, t->sz.p, nullptr);
-  ev_rec(t, EV_LIST + 1);
-  t->stats.t_lists = -1;  // resolved in stats
-}
-
-void eval_particles_sorted(Tree* t, const bit_eval_params& p) {
-  if (!t->has_moments) fail(BIT_ERR_STATE, "moments not computed (call bit_tree_moments)");
-  ensure_particle_lists(t, p);
+void eval_particles_sorted(Tree* t, const std::vector<bit_eval_params>& prm) {
+  prepare_particles(t, prm, 0);
   t->pot_sorted.ensure(t->ctx, t->n);
   ev_rec(t, EV_FAR);
-  eval_far(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, t->pot_sorted.p);
+  eval_far(t, &t->plists, t->pplan, t->sx.p, t->sy.p, t->sz.p, t->pot_sorted.p);
   ev_rec(t, EV_FAR + 1);
   ev_rec(t, EV_NEAR);
-  eval_near(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, t->pot_sorted.p);
+  eval_near(t, &t->plists, t->pplan, t->sx.p, t->sy.p, t->sz.p, t->pot_sorted.p);
   ev_rec(t, EV_NEAR + 1);
   t->stats.far_pairs = t->plists.far_pairs;
   t->stats.near_pairs = t->plists.near_pairs;
   t->stats.far_entries = t->plists.nfar;
   t->stats.near_entries = t->plists.nnear;
   t->stats.batches = t->plists.ngroups;
-  t->stats.far_launches = 1;
-  t->stats.near_launches = 1;
+  t->stats.far_launches = (int)t->pplan.far_classes.size();
+  t->stats.near_launches = (int)t->pplan.near_classes.size();
 }
 
 uint64_t spread3(uint64_t v) {
@@ -285,15 +276,27 @@ bit_status bit_ctx_memory(const bit_ctx* h, size_t* in_use, size_t* peak) {
   return BIT_OK;
 }
 
-static bit_status build_common(bit_ctx* h, int n, const double* x, const double* y,
-                               const double* z, int maxmemb, bit_tree** out, bool host) {
-  if (!h || !out || !x || !y || !z) return BIT_ERR_INVALID_ARGUMENT;
+static bit_status build_common(bit_ctx* h, int nsys, const int* ns, const int* mm,
+                               const double* x, const double* y, const double* z,
+                               bit_tree** out, bool host) {
+  if (!h || !out || !x || !y || !z || !ns || !mm || nsys < 1) return BIT_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   Ctx* c = &h->c;
-  if (n < 1 || maxmemb < 1) {
-    c->last_error = "n and maxmemb must be >= 1";
+  long long total = 0;
+  int mmin = INT_MAX;
+  for (int s = 0; s < nsys; s++) {
+    if (ns[s] < 1 || mm[s] < 1) {
+      c->last_error = "n and maxmemb must be >= 1 (every system)";
+      return BIT_ERR_INVALID_ARGUMENT;
+    }
+    total += ns[s];
+    mmin = std::min(mmin, mm[s]);
+  }
+  if (total > INT_MAX / 2) {
+    c->last_error = "too many particles";
     return BIT_ERR_INVALID_ARGUMENT;
   }
+  const int n = (int)total;
   bit_tree* th = new (std::nothrow) bit_tree;
   if (!th) return BIT_ERR_OUT_OF_MEMORY;
   bit_status st = guard(c, [&] {
@@ -301,7 +304,12 @@ static bit_status build_common(bit_ctx* h, int n, const double* x, const double*
     Tree* t = &th->t;
     t->ctx = c;
     t->n = n;
-    t->maxmemb = maxmemb;
+    t->maxmemb = mmin;
+    t->nsys = nsys;
+    t->h_sys_start.resize(nsys);
+    t->h_sys_n.assign(ns, ns + nsys);
+    t->h_sys_maxmemb.assign(mm, mm + nsys);
+    for (int s = 0, o = 0; s < nsys; o += ns[s], s++) t->h_sys_start[s] = o;
     ev_init(t);
     ev_rec(t, EV_BUILD);
     if (host) {
@@ -332,12 +340,75 @@ static bit_status build_common(bit_ctx* h, int n, const double* x, const double*
 
 bit_status bit_tree_build(bit_ctx* h, int n, const double* x, const double* y, const double* z,
                           int maxmemb, bit_tree** out) {
-  return build_common(h, n, x, y, z, maxmemb, out, true);
+  return build_common(h, 1, &n, &maxmemb, x, y, z, out, true);
 }
 
 bit_status bit_tree_build_device(bit_ctx* h, int n, const double* x, const double* y,
                                  const double* z, int maxmemb, bit_tree** out) {
-  return build_common(h, n, x, y, z, maxmemb, out, false);
+  return build_common(h, 1, &n, &maxmemb, x, y, z, out, false);
+}
+
+bit_status bit_forest_build(bit_ctx* h, int nsys, const int* n, const int* maxmemb,
+                            const double* x, const double* y, const double* z, bit_tree** out) {
+  return build_common(h, nsys, n, maxmemb, x, y, z, out, true);
+}
+
+bit_status bit_forest_build_device(bit_ctx* h, int nsys, const int* n, const int* maxmemb,
+                                   const double* x, const double* y, const double* z,
+                                   bit_tree** out) {
+  return build_common(h, nsys, n, maxmemb, x, y, z, out, false);
+}
+
+bit_status bit_forest_systems(const bit_tree* th, int* nsys) {
+  if (!th || !nsys) return BIT_ERR_INVALID_ARGUMENT;
+  *nsys = th->t.nsys;
+  return BIT_OK;
+}
+
+bit_status bit_forest_moments(bit_tree* th, const int* nterms) {
+  if (!th || !nterms) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  return guard(t->ctx, [&] {
+    BIT_CUDA(cudaSetDevice(t->ctx->device));
+    ev_rec(t, EV_MOM);
+    tree_moments_sys(t, std::vector<int>(nterms, nterms + t->nsys));
+    ev_rec(t, EV_MOM + 1);
+    t->stats.nterms = t->nterms;
+  });
+}
+
+static bit_status forest_eval(bit_tree* th, const bit_eval_params* prm, double* pot, bool host) {
+  if (!th || !prm || !pot) return BIT_ERR_INVALID_ARGUMENT;
+  Tree* t = &th->t;
+  Ctx* c = t->ctx;
+  return guard(c, [&] {
+    for (int s = 0; s < t->nsys; s++) check_params(prm + s);
+    BIT_CUDA(cudaSetDevice(c->device));
+    DBuf<double> out;
+    double* dst = pot;
+    if (host) {
+      out.ensure(c, t->n);
+      dst = out.p;
+    }
+    ev_rec(t, EV_ALL);
+    eval_particles_sorted(t, std::vector<bit_eval_params>(prm, prm + t->nsys));
+    count_launch(), k_scatter_out<<<grid_for(t->n, 256), 256, 0, c->stream>>>(t->n, t->perm.p,
+                                                                             t->pot_sorted.p, dst);
+    BIT_CHECK_LAUNCH();
+    ev_rec(t, EV_ALL + 1);
+    if (host) {
+      BIT_CUDA(cudaMemcpyAsync(pot, out.p, t->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      BIT_CUDA(cudaStreamSynchronize(c->stream));
+      check_dev_err(c);
+    }
+  });
+}
+
+bit_status bit_forest_eval(bit_tree* th, const bit_eval_params* prm, double* pot) {
+  return forest_eval(th, prm, pot, true);
+}
+bit_status bit_forest_eval_device(bit_tree* th, const bit_eval_params* prm, double* pot) {
+  return forest_eval(th, prm, pot, false);
 }
 
 bit_status bit_tree_destroy(bit_tree* th) {
@@ -432,7 +503,7 @@ bit_status bit_tree_export_moments(const bit_tree* th, double* mom) {
   const Tree* t = &th->t;
   if (!t->has_moments) return BIT_ERR_STATE;
   return guard(t->ctx, [&] {
-    d2h(t->ctx, mom, t->mom64.p, (size_t)t->numtree * num_terms(t->nterms) * sizeof(double));
+    d2h(t->ctx, mom, t->mom64.p, (size_t)t->mom_total * sizeof(double));
   });
 }
 
@@ -443,7 +514,7 @@ bit_status bit_eval_particles_device(bit_tree* th, const bit_eval_params* prm, d
     check_params(prm);
     BIT_CUDA(cudaSetDevice(t->ctx->device));
     ev_rec(t, EV_ALL);
-    eval_particles_sorted(t, *prm);
+    eval_particles_sorted(t, {*prm});
     count_launch(), k_scatter_out<<<grid_for(t->n, 256), 256, 0, t->ctx->stream>>>(t->n, t->perm.p,
                                                                    t->pot_sorted.p, pot);
     BIT_CHECK_LAUNCH();
@@ -461,7 +532,7 @@ bit_status bit_eval_particles(bit_tree* th, const bit_eval_params* prm, double* 
     DBuf<double> out;
     out.ensure(c, t->n);
     ev_rec(t, EV_ALL);
-    eval_particles_sorted(t, *prm);
+    eval_particles_sorted(t, {*prm});
     count_launch(), k_scatter_out<<<grid_for(t->n, 256), 256, 0, c->stream>>>(t->n, t->perm.p, t->pot_sorted.p, out.p);
     BIT_CHECK_LAUNCH();
     ev_rec(t, EV_ALL + 1);
@@ -518,9 +589,12 @@ bit_status bit_eval_points(bit_tree* th, const bit_eval_params* prm, int m, cons
     BIT_CUDA(cudaMemcpyAsync(dz.p, sz.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
     BIT_CUDA(cudaMemcpyAsync(dord.p, ord.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
     Lists L;
-    build_lists(t, &L, mac_key(*prm, t->gen, 1), m, dx.p, dy.p, dz.p, nullptr);
-    eval_far(t, &L, *prm, 1, dx.p, dy.p, dz.p, out.p);
-    eval_near(t, &L, *prm, 1, dx.p, dy.p, dz.p, out.p);
+    EvalPlan P;
+    plan_sys(t, &P, {*prm}, 1, 0);
+    build_lists(t, &L, plan_key(t, P, 1), m, dx.p, dy.p, dz.p, P.sys.p);
+    plan_classes(t, &L, &P);
+    eval_far(t, &L, P, dx.p, dy.p, dz.p, out.p);
+    eval_near(t, &L, P, dx.p, dy.p, dz.p, out.p);
     DBuf<double> res;
     res.ensure(c, m);
     count_launch(), k_scatter_out<<<grid_for(m, 256), 256, 0, s>>>(m, dord.p, out.p, res.p);
@@ -545,14 +619,14 @@ bit_status bit_eval_force(bit_tree* th, double del, double acc, bit_precision pr
     p.del = del;
     p.acc = acc;
     p.precision = prec;
-    ensure_particle_lists(t, p);
+    prepare_particles(t, {p}, 1);
     const int n = t->n;
     t->fx_sorted.ensure(c, n); t->fy_sorted.ensure(c, n); t->fz_sorted.ensure(c, n);
     ev_rec(t, EV_FAR);
-    eval_far_force(t, &t->plists, del, prec, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
+    eval_far_force(t, &t->plists, t->pplan, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
     ev_rec(t, EV_FAR + 1);
     ev_rec(t, EV_NEAR);
-    eval_near_force(t, &t->plists, del, prec, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
+    eval_near_force(t, &t->plists, t->pplan, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
     ev_rec(t, EV_NEAR + 1);
     DBuf<double> o;
     o.ensure(c, 3LL * n);
@@ -613,7 +687,7 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
   Tree* t = &th->t;
   return guard(t->ctx, [&] {
     check_params(prm);
-    ensure_particle_lists(t, *prm);
+    prepare_particles(t, {*prm}, 0);
     Lists& L = t->plists;
     Ctx* c = t->ctx;
     int e = 0;
@@ -652,7 +726,8 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
     std::vector<int> rank(t->numtree, 0);
     {
       int r = 0;
-      std::vector<int> stk{0};
+      std::vector<int> stk;
+      for (int sy = t->nsys - 1; sy >= 0; sy--) stk.push_back(sy);
       while (!stk.empty()) {
         int nd = stk.back();
         stk.pop_back();

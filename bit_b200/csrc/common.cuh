@@ -77,14 +77,47 @@ struct DBuf {
   T* get() const { return p; }
 };
 
+// ---- per-system evaluation parameters (device copy) ------------------------------------
+// Everything a kernel needs to know about the system a target group belongs to.
+struct SysEval {
+  double acc, mac_add, mac_sub;  // MAC: sqradius < acc * ((r^2 + mac_add) - mac_sub)
+  double far_add;                // distance^2 fed to the far recurrence: r^2 + far_add
+  double far_sign;               // +1, or -1 for the screened potential
+  double kappa;
+  double near_del;               // added to r^2 in the near field
+  double intg;                   // reference-mode screened self term
+  int kernel, nterms;
+  int near_sign, eps_check, self_term, particles;
+};
+
+// One launch of a far / near kernel: the groups of one (nterms, kernel) class.
+struct LaunchClass {
+  int nterms, kernel, eps;  // eps: near field skips r^2 <= 1e-14
+  int begin, count;         // range in the class-ordered group array
+};
+
+struct EvalPlan {
+  std::vector<SysEval> h_sys;
+  DBuf<SysEval> sys;
+  bool f32 = false;
+  int force = 0;
+  std::vector<LaunchClass> far_classes, near_classes;
+  DBuf<int> far_order, near_order;   // used when there is more than one class
+  const int* far_ord = nullptr;      // group order of the far / near launches
+  const int* near_ord = nullptr;
+  long long lists_version = -1;      // lists the classes were planned for
+  std::vector<long long> class_key;  // per system: far and near class of the last plan
+};
+
 // ---- interaction lists of one target set under one MAC --------------------------------
 struct ListKey {
   double acc = -1, add_del = 0, sub_del = 0;
   int points = 0;  // 0: particle targets, 1: external points
   long long gen = -1;  // tree generation it was built for
+  std::vector<double> sysmac;  // forests: (acc, add, sub) of every system
   bool operator==(const ListKey& o) const {
     return acc == o.acc && add_del == o.add_del && sub_del == o.sub_del &&
-           points == o.points && gen == o.gen;
+           points == o.points && gen == o.gen && sysmac == o.sysmac;
   }
 };
 
@@ -95,12 +128,16 @@ struct Lists {
   long long nfar = 0, nnear = 0;            // entries
   long long far_pairs = 0, near_pairs = 0;  // interactions
   DBuf<int> g_tstart, g_tcount, g_own;      // group: first target, count, own leaf (or -1)
+  DBuf<int> g_sys;                          // group: system (its root node)
+  std::vector<int> h_g_sys;
   DBuf<long long> far_off, near_off;        // first entry of each group
   DBuf<int> far_cnt, near_cnt;              // entries of each group
   DBuf<long long> far_moff, near_moff;      // first mask word of each group
   DBuf<int> far_node, near_node;            // entry -> node
   DBuf<unsigned> far_mask, near_mask;       // (tcount+31)/32 words per entry
   DBuf<int> order;                          // groups by decreasing work
+  std::vector<long long> h_work;            // estimated work of each group
+  long long version = 0;                    // bumped by every build
 };
 
 struct Ctx {
@@ -132,6 +169,11 @@ struct Tree {
   Ctx* ctx = nullptr;
   long long gen = 0;
   int n = 0, maxmemb = 0, numtree = 0, nleaves = 0, depth = 0, cap = 0;
+  // A tree holds nsys independent systems (a forest): system s owns particles
+  // [sys_start[s], sys_start[s] + sys_n[s]) and its root is node s.
+  int nsys = 1;
+  std::vector<int> h_sys_start, h_sys_n, h_sys_maxmemb, h_sys_nterms, h_node_sys;
+  DBuf<int> sys_start, sys_n, sys_maxmemb, node_sys;
   // particles in tree order (sorted position e); perm[e] = original index
   DBuf<int> perm, iperm;
   DBuf<double> sx, sy, sz, sq, sw;
@@ -152,14 +194,19 @@ struct Tree {
   bool has_moments = false;
   DBuf<double> mom64;
   DBuf<float> mom32;
+  std::vector<long long> h_mom_off;  // first moment of each node (systems may differ in nterms)
+  DBuf<long long> mom_off;
   // moment work plan: (node, first, last) member chunks and per-chunk partial sums
   long long mplan_gen = -1;
   int mplan_nch = 0;
+  long long mom_total = 0;
+  std::vector<int> mplan_cls;  // chunk range of each nterms class
   DBuf<int4> mplan_chunks;
-  DBuf<int> mplan_c0, mplan_c1;
+  DBuf<int> mplan_c0, mplan_c1, mplan_T;
   DBuf<double> mplan_part;
   // lists and outputs
   Lists plists;            // particle targets
+  EvalPlan pplan;          // plan of the last particle-target evaluation
   DBuf<double> pot_sorted, fx_sorted, fy_sorted, fz_sorted;
   bit_stats stats{};
   cudaEvent_t ev[12] = {};
@@ -175,32 +222,30 @@ void tree_build(Tree* t, const double* dx, const double* dy, const double* dz);
 void tree_sync_host(Tree* t);
 void tree_set_charges(Tree* t, const double* dq, const double* dw);
 void tree_moments(Tree* t, int nterms);
+void tree_moments_sys(Tree* t, const std::vector<int>& nterms_per_system);
 void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const double* tx,
-                 const double* ty, const double* tz, const int* t_leaf);
-void eval_far(Tree* t, Lists* L, const bit_eval_params& p, int points, const double* tx,
-              const double* ty, const double* tz, double* out_sorted);
-void eval_near(Tree* t, Lists* L, const bit_eval_params& p, int points, const double* tx,
-               const double* ty, const double* tz, double* out_sorted);
-void eval_near_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
-                     double* fz);
-void eval_far_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
-                    double* fz);
+                 const double* ty, const double* tz, const SysEval* d_sys);
+// Evaluation plan of one call: per-system parameters on the device and the groups of
+// each launch class, ordered by class and then by decreasing work.
+void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
+              const double* tz, double* out_sorted);
+void eval_near(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
+               const double* tz, double* out_sorted);
+void eval_far_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz);
+void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz);
 
-// MAC parameters of an evaluation: accept iff sqradius < acc * ((r^2 + add) - sub).
-inline ListKey mac_key(const bit_eval_params& p, long long gen, int points) {
-  ListKey k;
-  k.acc = p.acc;
-  k.points = points;
-  k.gen = gen;
-  if (p.kernel == BIT_KERNEL_SCREENED) {
-    k.add_del = 0.0;
-    k.sub_del = p.mac_del;
-  } else {
-    k.add_del = p.del;
-    k.sub_del = p.del;
-  }
-  return k;
-}
+// Per-system parameters of a potential (force = 0) or field (force = 1) evaluation.
+SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int force);
+// Fill P->h_sys (one entry per system; prm holds one entry for all or one per system) and
+// its device copy.
+void plan_sys(Tree* t, EvalPlan* P, const std::vector<bit_eval_params>& prm, int points,
+              int force);
+// Key of the lists the plan's MAC needs.
+ListKey plan_key(const Tree* t, const EvalPlan& P, int points);
+// Launch classes and class-ordered groups of P over the lists L.
+void plan_classes(Tree* t, Lists* L, EvalPlan* P);
+// Particle-target lists and plan of a tree (t->plists, t->pplan) for these parameters.
+void prepare_particles(Tree* t, const std::vector<bit_eval_params>& prm, int force);
 
 inline unsigned grid_for(long long work, int per_block) {
   long long g = (work + per_block - 1) / per_block;

@@ -54,8 +54,10 @@ struct FarArgs {
   const int* node;
   const unsigned* mask;
   const double4* nodec;
-  const void* mom;  // float or double, T(nterms) per node
-  double add, kappa, sign;
+  const void* mom;  // float or double, T(nterms of the node's system) per node
+  const long long* mom_off;  // first moment of each node
+  const SysEval* sys;        // per system: far_add, kappa, far_sign
+  const int* g_sys;          // per group: system
   double *out, *out_y, *out_z;
 };
 
@@ -137,15 +139,17 @@ __global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
   unsigned short* tl = tlb + w * kGroupMax;
   T* row = accb + w * ROW;
   const T* mom = reinterpret_cast<const T*>(a.mom);
-  const T tadd = (T)a.add, tk = (T)a.kappa;
+  const SysEval* se = a.sys + a.g_sys[g];
+  const T tadd = (T)se->far_add, tk = (T)se->kappa;
+  const double sign = se->far_sign;
   for (long long e = e0 + w; e < e1; e += NW) {
     const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
     const int cnt = warp_pack(wd, tl);
     const int node = a.node[e];
     const double4 c = a.nodec[node];
     T* M = msb + w * TP;
-    for (int k = lane; k < TP; k += 32)
-      M[k] = k < TT ? mom[(long long)node * TT + FarField<NT>::canon(k)] : T(0);
+    const T* mn = mom + a.mom_off[node];
+    for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
       const int i = tl[r];
@@ -162,7 +166,7 @@ __global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
   for (int i = tid; i < tc; i += 32 * NW) {
     double s = 0.0;
     for (int q = 0; q < NW; q++) s += WarpAcc<T>::get(accb + q * ROW, i);
-    a.out[t0 + i] = a.sign * s;
+    a.out[t0 + i] = sign * s;
   }
 }
 
@@ -192,19 +196,20 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
   unsigned short* tl = tlb + w * kGroupMax;
   double* row = accb + w * 3 * kGroupMax;
   const T* mom = reinterpret_cast<const T*>(a.mom);
+  const T tadd = (T)a.sys[a.g_sys[g]].far_add;
   for (long long e = e0 + w; e < e1; e += NW) {
     const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
     const int cnt = warp_pack(wd, tl);
     const int node = a.node[e];
     const double4 c = a.nodec[node];
     T* M = msb + w * TP;
-    for (int k = lane; k < TP; k += 32)
-      M[k] = k < TT ? mom[(long long)node * TT + FarField<NT>::canon(k)] : T(0);
+    const T* mn = mom + a.mom_off[node];
+    for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
       const int i = tl[r];
       const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
-      const T rs = dx * dx + dy * dy + dz * dz + (T)a.add;
+      const T rs = dx * dx + dy * dy + dz * dz + tadd;
       T fx = 0, fy = 0, fz = 0;
       FarField<NT>::template force<T>(dx, dy, dz, rs, M, fx, fy, fz);
       row[i] += (double)fx;
@@ -253,10 +258,9 @@ void launch_force(const FarArgs& a, int ng, cudaStream_t s) {
   count_launch(), k_far_force<NT, T><<<ng, 32 * NWF, bytes, s>>>(a);
 }
 
-FarArgs far_args(Tree* t, Lists* L, const double* tx, const double* ty, const double* tz,
-                 bool f32) {
+FarArgs far_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
+                 const double* tz) {
   FarArgs a{};
-  a.order = L->order.p;
   a.g_tstart = L->g_tstart.p;
   a.g_tcount = L->g_tcount.p;
   a.tx = tx; a.ty = ty; a.tz = tz;
@@ -266,25 +270,27 @@ FarArgs far_args(Tree* t, Lists* L, const double* tx, const double* ty, const do
   a.node = L->far_node.p;
   a.mask = L->far_mask.p;
   a.nodec = t->nodec.p;
-  a.mom = f32 ? (const void*)t->mom32.p : (const void*)t->mom64.p;
+  a.mom = P.f32 ? (const void*)t->mom32.p : (const void*)t->mom64.p;
+  a.mom_off = t->mom_off.p;
+  a.sys = P.sys.p;
+  a.g_sys = L->g_sys.p;
   return a;
 }
 
 }  // namespace
 
-void eval_far(Tree* t, Lists* L, const bit_eval_params& p, int /*points*/, const double* tx,
-              const double* ty, const double* tz, double* out) {
-  const bool f32 = p.precision == BIT_PREC_MIXED;
-  FarArgs a = far_args(t, L, tx, ty, tz, f32);
-  // distance^2 fed to the recurrence: r^2 + del (Coulomb, regularised screened) or r^2
-  a.add = p.kernel == BIT_KERNEL_SCREENED ? 0.0 : p.del;
-  a.kappa = p.kappa;
-  a.sign = p.kernel == BIT_KERNEL_SCREENED ? -1.0 : 1.0;  // src/tree3d.cpp:3222 subtracts
+// One launch per (nterms, kernel) class, each over its groups (P.far_ord + begin).
+void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
+              const double* tz, double* out) {
+  FarArgs a = far_args(t, L, P, tx, ty, tz);
   a.out = out;
-  const bool coul = p.kernel == BIT_KERNEL_COULOMB;
   cudaStream_t s = t->ctx->stream;
-  const int ng = L->ngroups;
-  switch (t->nterms) {
+  const bool f32 = P.f32;
+  for (const LaunchClass& k : P.far_classes) {
+    a.order = P.far_ord + k.begin;
+    const int ng = k.count;
+    const bool coul = k.kernel == BIT_KERNEL_COULOMB;
+    switch (k.nterms) {
 #define CASE(N)                                                                   \
   case N:                                                                         \
     if (f32) {                                                                    \
@@ -295,34 +301,36 @@ void eval_far(Tree* t, Lists* L, const bit_eval_params& p, int /*points*/, const
       else launch_far<N, BIT_KERNEL_SCREENED, double>(a, ng, s);                  \
     }                                                                             \
     break;
-    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
+      CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
 #undef CASE
-    default:
-      fail(BIT_ERR_STATE, "moments not computed");
+      default:
+        fail(BIT_ERR_STATE, "moments not computed");
+    }
+    BIT_CHECK_LAUNCH();
   }
-  BIT_CHECK_LAUNCH();
 }
 
-void eval_far_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
-                    double* fz) {
-  const bool f32 = prec == BIT_PREC_MIXED;
-  FarArgs a = far_args(t, L, t->sx.p, t->sy.p, t->sz.p, f32);
-  a.add = del;
+void eval_far_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz) {
+  FarArgs a = far_args(t, L, P, t->sx.p, t->sy.p, t->sz.p);
   a.out = fx; a.out_y = fy; a.out_z = fz;
   cudaStream_t s = t->ctx->stream;
-  const int ng = L->ngroups;
-  switch (t->nterms) {
+  const bool f32 = P.f32;
+  for (const LaunchClass& k : P.far_classes) {
+    a.order = P.far_ord + k.begin;
+    const int ng = k.count;
+    switch (k.nterms) {
 #define CASE(N)                                           \
   case N:                                                 \
     if (f32) launch_force<N, float>(a, ng, s);            \
     else launch_force<N, double>(a, ng, s);               \
     break;
-    CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
+      CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
 #undef CASE
-    default:
-      fail(BIT_ERR_STATE, "moments not computed");
+      default:
+        fail(BIT_ERR_STATE, "moments not computed");
+    }
+    BIT_CHECK_LAUNCH();
   }
-  BIT_CHECK_LAUNCH();
 }
 
 }  // namespace bit

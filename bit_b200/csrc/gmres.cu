@@ -22,8 +22,6 @@
 
 namespace bit {
 
-void ensure_lists_for(Tree* t, const bit_eval_params& p);
-
 namespace {
 
 constexpr int RB = 256;
@@ -153,9 +151,9 @@ struct BieOp {
     tree_moments(t, nterms);
     bit_eval_params p = prm;
     p.precision = prec;
-    ensure_lists_for(t, p);
-    eval_far(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, y);
-    eval_near(t, &t->plists, p, 0, t->sx.p, t->sy.p, t->sz.p, y);
+    prepare_particles(t, {p}, 0);
+    eval_far(t, &t->plists, t->pplan, t->sx.p, t->sy.p, t->sz.p, y);
+    eval_near(t, &t->plists, t->pplan, t->sx.p, t->sy.p, t->sz.p, y);
     count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, diag, x, 1.0, y);
     BIT_CHECK_LAUNCH();
     (prec == BIT_PREC_FP64 ? mv64 : mv32)++;
@@ -297,12 +295,6 @@ __global__ void k_dense_update(int n, int k, const double* Q, const double* y, d
 }
 
 }  // namespace
-
-void ensure_lists_for(Tree* t, const bit_eval_params& p) {
-  ListKey k = mac_key(p, t->gen, 0);
-  if (t->plists.valid && t->plists.key == k) return;
-  build_lists(t, &t->plists, k, t->n, t->sx.p, t->sy.p, t->sz.p, nullptr);
-}
 
 }  // namespace bit
 

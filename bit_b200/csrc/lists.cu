@@ -9,6 +9,7 @@
 // for the accepting targets, and the others descend into the children in the reference's
 // children[] order, or get a near entry at a leaf.  Entries carry the group's bitmask.
 // Restricted to one target, the entries are exactly its reference traversal, in order.
+// In a forest the walk starts at the root of the group's system, with that system's MAC.
 //
 // Single pass: each CTA stages its entries in shared memory, then reserves room in the
 // global lists with one atomic per list and copies them out (a group's entries stay
@@ -38,7 +39,8 @@ struct ListArgs {
   const double *tx, *ty, *tz;
   const double4* nodec;
   const int *children, *nummemb;
-  double acc, add, sub;
+  const SysEval* sys;  // per system: MAC parameters
+  const int* g_sys;    // per group: system (its root is node g_sys[g])
   // per group
   long long *far_off, *near_off, *far_moff, *near_moff;
   int *far_cnt, *near_cnt;
@@ -62,6 +64,8 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int W = (tc + 31) >> 5;
   const int i = threadIdx.x;
+  const int root = a.g_sys[g];
+  const double macc = a.sys[root].acc, madd = a.sys[root].mac_add, msub = a.sys[root].mac_sub;
   // staging layout: far nodes | far masks, near nodes | near masks
   const int fcap = STAGE_FAR / (W + 1), ncap = STAGE_NEAR / (W + 1);
   int* sf_node = reinterpret_cast<int*>(stage);
@@ -70,7 +74,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   unsigned* sn_mask = stage + STAGE_FAR + ncap;
   double x = 0, y = 0, z = 0;
   if (i < tc) { x = a.tx[t0 + i]; y = a.ty[t0 + i]; z = a.tz[t0 + i]; }
-  if (threadIdx.x == 0) s_node[0] = 0;
+  if (threadIdx.x == 0) s_node[0] = root;
   if (lane == 0) {
     int live = tc - 32 * w;
     s_mask[0][w] = live >= 32 ? 0xffffffffu : (live > 0 ? (1u << live) - 1u : 0u);
@@ -92,7 +96,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
       const double4 c = a.nodec[node];
       double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
       double s = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
-      ok = c.w < dmul(a.acc, dsub(dadd(s, a.add), a.sub));
+      ok = c.w < dmul(macc, dsub(dadd(s, madd), msub));
     }
     const unsigned am = __ballot_sync(0xffffffffu, ok) & word;
     const unsigned rm = word & ~am;
@@ -222,7 +226,7 @@ void set_stage_attr() {
 
 // Groups for particle targets: each leaf, in chunks of at most kGroupMax members.
 static void particle_groups(Tree* t, std::vector<int>& ts, std::vector<int>& tc,
-                            std::vector<int>& own) {
+                            std::vector<int>& own, std::vector<int>& sys) {
   for (int i = 0; i < t->numtree; i++) {
     if (t->h_children[8LL * i] != -1) continue;
     int st = t->h_start[i], en = st + t->h_nummemb[i];
@@ -230,23 +234,26 @@ static void particle_groups(Tree* t, std::vector<int>& ts, std::vector<int>& tc,
       ts.push_back(e);
       tc.push_back(std::min(kGroupMax, en - e));
       own.push_back(i);
+      sys.push_back(t->h_node_sys[i]);
     }
   }
 }
 
 void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const double* tx,
-                 const double* ty, const double* tz, const int* /*unused*/) {
+                 const double* ty, const double* tz, const SysEval* d_sys) {
   Ctx* c = t->ctx;
   cudaStream_t s = c->stream;
-  std::vector<int> ts, tc, own;
+  std::vector<int> ts, tc, own, gsys;
   if (key.points) {
+    if (t->nsys != 1) fail(BIT_ERR_INVALID_ARGUMENT, "external points need a single-system tree");
     for (int e = 0; e < ntargets; e += kPointGroup) {
       ts.push_back(e);
       tc.push_back(std::min(kPointGroup, ntargets - e));
       own.push_back(-1);
+      gsys.push_back(0);
     }
   } else {
-    particle_groups(t, ts, tc, own);
+    particle_groups(t, ts, tc, own, gsys);
   }
   const int ng = (int)ts.size();
   L->ngroups = ng;
@@ -256,6 +263,9 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   BIT_CUDA(cudaMemcpyAsync(L->g_tstart.p, ts.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaMemcpyAsync(L->g_tcount.p, tc.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaMemcpyAsync(L->g_own.p, own.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
+  L->g_sys.ensure(c, ng);
+  BIT_CUDA(cudaMemcpyAsync(L->g_sys.p, gsys.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
+  L->h_g_sys = gsys;
   L->far_off.ensure(c, ng);
   L->near_off.ensure(c, ng);
   L->far_moff.ensure(c, ng);
@@ -272,7 +282,8 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   a.nodec = t->nodec.p;
   a.children = t->children.p;
   a.nummemb = t->nummemb.p;
-  a.acc = key.acc; a.add = key.add_del; a.sub = key.sub_del;
+  a.sys = d_sys;
+  a.g_sys = L->g_sys.p;
   a.far_off = L->far_off.p; a.near_off = L->near_off.p;
   a.far_moff = L->far_moff.p; a.near_moff = L->near_moff.p;
   a.far_cnt = L->far_cnt.p; a.near_cnt = L->near_cnt.p;
@@ -341,11 +352,13 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   std::vector<long long> wk(ng);
   for (int g = 0; g < ng; g++) wk[g] = (40LL * hf[g] + hn[g]) * (long long)tc[g];
   std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return wk[x] > wk[y]; });
+  L->h_work = wk;
   L->order.ensure(c, ng);
   BIT_CUDA(cudaMemcpyAsync(L->order.p, ord.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaStreamSynchronize(s));
   L->key = key;
   L->valid = true;
+  L->version++;
 }
 
 }  // namespace bit

@@ -24,16 +24,6 @@ namespace {
 
 constexpr int NT = 256;  // threads per CTA
 
-struct NearSpec {
-  double del;     // added to r^2
-  double kappa;
-  double intg;    // reference-mode screened self term
-  int eps_check;  // skip r^2 <= 1e-14
-  int self_term;  // 1: add q*intg/w for j == p
-  int sign;       // +1 / -1
-  int particles;  // targets are the sources (self excluded by position)
-};
-
 struct NearArgs {
   const int *order, *g_tstart, *g_tcount, *g_own;
   const double *tx, *ty, *tz;
@@ -46,7 +36,8 @@ struct NearArgs {
   const void* src;  // float4 (mixed) or double4 (FP64) in tree order
   const double4* src64;
   const double* sw;
-  NearSpec sp;
+  const SysEval* sys;  // per system: near_del, kappa, intg, near_sign, self_term, particles
+  const int* g_sys;    // per group: system
   double *out, *out_y, *out_z;  // potential, or the three field components
   int* err;
 };
@@ -170,7 +161,9 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
 
   const int g = a.order[blockIdx.x];
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
-  const int own = a.sp.particles ? a.g_own[g] : -1;
+  const SysEval* se = a.sys + a.g_sys[g];
+  const double sdel = se->near_del, skappa = se->kappa;
+  const int own = se->particles ? a.g_own[g] : -1;
   const int W = (tc + 31) >> 5;
   const long long e0 = a.off[g], e1 = e0 + a.cnt[g];
   const long long m0 = a.moff[g];
@@ -186,8 +179,8 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
   __syncthreads();
   if (e0 < e1) {
     const S* src = reinterpret_cast<const S*>(a.src);
-    const float del = (float)a.sp.del;
-    const float kl2 = (float)(-a.sp.kappa * 1.4426950408889634);  // -kappa*log2(e)
+    const float del = (float)sdel;
+    const float kl2 = (float)(-skappa * 1.4426950408889634);  // -kappa*log2(e)
     // job iterator: (entry e, first source of the tile in the entry's leaf)
     long long e = e0;
     int node = a.node[e];
@@ -277,12 +270,12 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
               double p = 0.0;
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
               for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) p += pair<KER, EPS>(x, y, z, ds[j], a.sp.del, a.sp.kappa);
+                if (j != selfj) p += pair<KER, EPS>(x, y, z, ds[j], sdel, skappa);
               part = p;
             }
-            if (a.sp.self_term && selfj >= 0 && selfj < ns && ((selfj - slice) & (tpt - 1)) == 0) {
+            if (se->self_term && selfj >= 0 && selfj < ns && ((selfj - slice) & (tpt - 1)) == 0) {
               const int jg = j0 + toff + selfj;  // added, not subtracted (src/tree3d.cpp:3596)
-              selfv[i] = a.src64[jg].w * a.sp.intg / (a.sw ? a.sw[jg] : 1.0);
+              selfv[i] = a.src64[jg].w * se->intg / (a.sw ? a.sw[jg] : 1.0);
             }
           }
           part = shfl_sum(part, tpt);
@@ -303,7 +296,7 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
               const double4* ds = reinterpret_cast<const double4*>(ts);
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
               for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) fpair(x, y, z, ds[j], a.sp.del, fx, fy, fz);
+                if (j != selfj) fpair(x, y, z, ds[j], sdel, fx, fy, fz);
             }
           }
           fx = shfl_sum(fx, tpt);
@@ -335,39 +328,11 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
       a.out_y[t0 + i] += accd[kGroupMax + i];
       a.out_z[t0 + i] += accd[2 * kGroupMax + i];
     } else if (F32) {
-      a.out[t0 + i] += a.sp.sign * ((double)acch[i] + (double)acch[kGroupMax + i]) + selfv[i];
+      a.out[t0 + i] += se->near_sign * ((double)acch[i] + (double)acch[kGroupMax + i]) + selfv[i];
     } else {
-      a.out[t0 + i] += a.sp.sign * accd[i] + selfv[i];
+      a.out[t0 + i] += se->near_sign * accd[i] + selfv[i];
     }
   }
-}
-
-NearSpec make_spec(const bit_eval_params& p, int points) {
-  NearSpec s{};
-  const bool ref = p.mode == BIT_MODE_REFERENCE;
-  s.kappa = p.kappa;
-  s.intg = p.intg;
-  s.particles = !points;
-  switch (p.kernel) {
-    case BIT_KERNEL_COULOMB:
-      // src/tree3d.cpp:4744-4772: points use del, particles drop it (reference mode)
-      s.del = (points || !ref) ? p.del : 0.0;
-      s.eps_check = 1;
-      s.sign = 1;
-      break;
-    case BIT_KERNEL_SCREENED:
-      s.del = 0.0;
-      s.eps_check = points ? 1 : 0;            // :3557 / :3604-3619
-      s.sign = (points && ref) ? 1 : -1;       // :3558 adds, :3619 subtracts
-      s.self_term = (!points && ref) ? 1 : 0;  // :3575-3596
-      break;
-    default:
-      s.del = p.del;
-      s.eps_check = 1;
-      s.sign = 1;
-      break;
-  }
-  return s;
 }
 
 template <int KER, bool EPS, bool F32, bool FORCE>
@@ -384,10 +349,9 @@ void launch(const NearArgs& a, int ngroups, cudaStream_t s) {
   count_launch(), k_near<KER, EPS, F32, FORCE><<<ngroups, NT, bytes, s>>>(a);
 }
 
-NearArgs base_args(Tree* t, Lists* L, const double* tx, const double* ty, const double* tz,
-                   bool f32) {
+NearArgs base_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
+                   const double* tz) {
   NearArgs a{};
-  a.order = L->order.p;
   a.g_tstart = L->g_tstart.p;
   a.g_tcount = L->g_tcount.p;
   a.g_own = L->g_own.p;
@@ -400,47 +364,52 @@ NearArgs base_args(Tree* t, Lists* L, const double* tx, const double* ty, const 
   a.start = t->start.p;
   a.nummemb = t->nummemb.p;
   a.nodec = t->nodec.p;
-  a.src = f32 ? (const void*)t->src32.p : (const void*)t->src64.p;
+  a.src = P.f32 ? (const void*)t->src32.p : (const void*)t->src64.p;
   a.src64 = t->src64.p;
   a.sw = t->has_weights ? t->sw.p : nullptr;
+  a.sys = P.sys.p;
+  a.g_sys = L->g_sys.p;
   a.err = t->ctx->dev_err();
   return a;
 }
 
 }  // namespace
 
-void eval_near(Tree* t, Lists* L, const bit_eval_params& p, int points, const double* tx,
-               const double* ty, const double* tz, double* out) {
+// One launch per (kernel, eps check) class, each over its groups (P.near_ord + begin).
+void eval_near(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
+               const double* tz, double* out) {
   cudaStream_t s = t->ctx->stream;
-  const bool f32 = p.precision == BIT_PREC_MIXED;
-  NearArgs a = base_args(t, L, tx, ty, tz, f32);
-  a.sp = make_spec(p, points);
+  NearArgs a = base_args(t, L, P, tx, ty, tz);
   a.out = out;
-  const bool scr = p.kernel != BIT_KERNEL_COULOMB;
-  const bool eps = a.sp.eps_check;
-#define GO(K, E, F) launch<K, E, F, false>(a, L->ngroups, s)
-  if (f32) {
-    if (!scr) { if (eps) GO(BIT_KERNEL_COULOMB, true, true); else GO(BIT_KERNEL_COULOMB, false, true); }
-    else { if (eps) GO(BIT_KERNEL_SCREENED, true, true); else GO(BIT_KERNEL_SCREENED, false, true); }
-  } else {
-    if (!scr) { if (eps) GO(BIT_KERNEL_COULOMB, true, false); else GO(BIT_KERNEL_COULOMB, false, false); }
-    else { if (eps) GO(BIT_KERNEL_SCREENED, true, false); else GO(BIT_KERNEL_SCREENED, false, false); }
-  }
+  const bool f32 = P.f32;
+  for (const LaunchClass& k : P.near_classes) {
+    a.order = P.near_ord + k.begin;
+    const int ng = k.count;
+    const bool scr = k.kernel != BIT_KERNEL_COULOMB;
+    const bool eps = k.eps != 0;
+#define GO(K, E, F) launch<K, E, F, false>(a, ng, s)
+    if (f32) {
+      if (!scr) { if (eps) GO(BIT_KERNEL_COULOMB, true, true); else GO(BIT_KERNEL_COULOMB, false, true); }
+      else { if (eps) GO(BIT_KERNEL_SCREENED, true, true); else GO(BIT_KERNEL_SCREENED, false, true); }
+    } else {
+      if (!scr) { if (eps) GO(BIT_KERNEL_COULOMB, true, false); else GO(BIT_KERNEL_COULOMB, false, false); }
+      else { if (eps) GO(BIT_KERNEL_SCREENED, true, false); else GO(BIT_KERNEL_SCREENED, false, false); }
+    }
 #undef GO
-  BIT_CHECK_LAUNCH();
+    BIT_CHECK_LAUNCH();
+  }
 }
 
-void eval_near_force(Tree* t, Lists* L, double del, bit_precision prec, double* fx, double* fy,
-                     double* fz) {
+void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz) {
   cudaStream_t s = t->ctx->stream;
-  const bool f32 = prec == BIT_PREC_MIXED;
-  NearArgs a = base_args(t, L, t->sx.p, t->sy.p, t->sz.p, f32);
-  a.sp.del = del;
-  a.sp.particles = 1;
+  NearArgs a = base_args(t, L, P, t->sx.p, t->sy.p, t->sz.p);
   a.out = fx; a.out_y = fy; a.out_z = fz;
-  if (f32) launch<BIT_KERNEL_COULOMB, false, true, true>(a, L->ngroups, s);
-  else launch<BIT_KERNEL_COULOMB, false, false, true>(a, L->ngroups, s);
-  BIT_CHECK_LAUNCH();
+  for (const LaunchClass& k : P.near_classes) {
+    a.order = P.near_ord + k.begin;
+    if (P.f32) launch<BIT_KERNEL_COULOMB, false, true, true>(a, k.count, s);
+    else launch<BIT_KERNEL_COULOMB, false, false, true>(a, k.count, s);
+    BIT_CHECK_LAUNCH();
+  }
 }
 
 }  // namespace bit

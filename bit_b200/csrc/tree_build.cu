@@ -182,12 +182,15 @@ __device__ __forceinline__ int warp_sum(int v) {
   return v;
 }
 
-// Bounding box of all particles (the root, src/tree3d.cpp:1385-1403); flags NaNs.
-__global__ void k_root_bbox(int n, const double* x, const double* y, const double* z,
-                            SplitAcc* acc, int* err) {
+// Bounding box of each system's particles (its root, src/tree3d.cpp:1385-1403); flags
+// NaNs.  grid.y = system, grid.x = blocks striding over that system.
+__global__ void k_root_bbox(const int* sys_start, const int* sys_n, const double* x,
+                            const double* y, const double* z, SplitAcc* acc, int* err) {
+  const int sy = blockIdx.y;
+  const int i0 = sys_start[sy], i1 = i0 + sys_n[sy];
   unsigned long long mn[3] = {~0ULL, ~0ULL, ~0ULL}, mx[3] = {0, 0, 0};
   int bad = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += gridDim.x * blockDim.x) {
     double v[3] = {x[i], y[i], z[i]};
     for (int d = 0; d < 3; d++) {
       if (isnan(v[d])) bad = 1;
@@ -203,8 +206,8 @@ __global__ void k_root_bbox(int n, const double* x, const double* y, const doubl
   bad = __any_sync(0xffffffffu, bad);
   if ((threadIdx.x & 31) == 0) {
     for (int d = 0; d < 3; d++) {
-      atomicMin(&acc->mn[0][d], mn[d]);
-      atomicMax(&acc->mx[0][d], mx[d]);
+      atomicMin(&acc[sy].mn[0][d], mn[d]);
+      atomicMax(&acc[sy].mx[0][d], mx[d]);
     }
     if (bad) atomicOr(err, 1);
   }
@@ -215,24 +218,29 @@ __global__ void k_acc_reset(SplitAcc* acc, int n) {
   if (i < n) acc_reset(&acc[i]);
 }
 
-__global__ void k_root_init(int n, const SplitAcc* acc, int* nummemb, int* start, int* children,
-                            int* level, int* parent, double* fields) {
+__global__ void k_root_init(int nsys, const int* sys_start, const int* sys_n, const SplitAcc* acc,
+                            int* nummemb, int* start, int* children, int* level, int* parent,
+                            double* fields, int* node_sys) {
+  const int sy = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sy >= nsys) return;
   double f[13];
-  box_fields(f, okey_inv(acc->mn[0][0]), okey_inv(acc->mx[0][0]), okey_inv(acc->mn[0][1]),
-             okey_inv(acc->mx[0][1]), okey_inv(acc->mn[0][2]), okey_inv(acc->mx[0][2]));
-  for (int k = 0; k < 13; k++) fields[k] = f[k];
-  nummemb[0] = n; start[0] = 0; level[0] = 0; parent[0] = -1;
-  for (int c = 0; c < 8; c++) children[c] = -1;
+  const SplitAcc* A = &acc[sy];
+  box_fields(f, okey_inv(A->mn[0][0]), okey_inv(A->mx[0][0]), okey_inv(A->mn[0][1]),
+             okey_inv(A->mx[0][1]), okey_inv(A->mn[0][2]), okey_inv(A->mx[0][2]));
+  for (int k = 0; k < 13; k++) fields[13LL * sy + k] = f[k];
+  nummemb[sy] = sys_n[sy]; start[sy] = sys_start[sy]; level[sy] = 0; parent[sy] = -1;
+  node_sys[sy] = sy;
+  for (int c = 0; c < 8; c++) children[8LL * sy + c] = -1;
 }
 
 // Per level node: active flag and the number of member chunks it needs.
-__global__ void k_level_init(int a, int nlev, const int* nummemb, int maxmemb, SplitState* st,
-                             SplitAcc* acc, int* nchunk) {
+__global__ void k_level_init(int a, int nlev, const int* nummemb, const int* node_sys,
+                             const int* sys_maxmemb, SplitState* st, SplitAcc* acc, int* nchunk) {
   int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= nlev) return;
   SplitState* S = &st[li];
   int cnt = nummemb[a + li];
-  S->active = cnt > maxmemb;
+  S->active = cnt > sys_maxmemb[node_sys[a + li]];
   S->finished = 0; S->ndone = 0; S->has_cur = 0; S->has_prev = 0; S->nchild = 0;
   acc_reset(&acc[li]);
   nchunk[li] = S->active ? (cnt + CH - 1) / CH : 0;
@@ -281,8 +289,9 @@ __global__ void k_fill_chunks(int a, int nlev, const int* start, const int* numm
   for (int c = cbeg[li]; c < cbeg[li + 1]; c++) chunks[c] = make_int2(li, s + (c - cbeg[li]) * CH);
 }
 
-__global__ void k_split_decide(int a, int nlev, const double* fields, SplitState* st,
-                               SplitAcc* acc, int maxmemb, double lim, int* err) {
+__global__ void k_split_decide(int a, int nlev, const double* fields, const int* node_sys,
+                               const int* sys_maxmemb, SplitState* st, SplitAcc* acc, double lim,
+                               int* err) {
   int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= nlev) return;
   SplitState* S = &st[li];
@@ -308,7 +317,8 @@ __global__ void k_split_decide(int a, int nlev, const double* fields, SplitState
   }
   if (S->finished) return;
   Replay r;
-  r.S = S; r.pf = fields + 13 * (long long)(a + li); r.maxmemb = maxmemb; r.lim = lim;
+  r.S = S; r.pf = fields + 13 * (long long)(a + li); r.lim = lim;
+  r.maxmemb = sys_maxmemb[node_sys[a + li]];
   r.d = 0; r.need = false;
   int order[8];
   int nchild = split_program(r, order);
@@ -493,7 +503,7 @@ __global__ void k_child_counts(int nlev, const SplitState* st, int* nch) {
 
 __global__ void k_make_children(int a, int b, int nlev, const SplitState* st, const int* cscan,
                                 int* nummemb, int* start, int* children, int* level,
-                                int* parent, double* fields) {
+                                int* parent, double* fields, int* node_sys) {
   int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= nlev) return;
   const SplitState* S = &st[li];
@@ -507,6 +517,7 @@ __global__ void k_make_children(int a, int b, int nlev, const SplitState* st, co
     off += S->slot_n[s];
     level[node] = level[p] + 1;
     parent[node] = p;
+    node_sys[node] = node_sys[p];
     for (int k = 0; k < 13; k++) fields[13LL * node + k] = S->slot_f[s][k];
     for (int c = 0; c < 8; c++) children[8LL * node + c] = -1;
   }
@@ -555,15 +566,32 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
   Ctx* c = t->ctx;
   cudaStream_t s = c->stream;
   const int n = t->n;
+  const int nsys = t->nsys;
+  // systems: particle ranges and leaf sizes (one system unless the caller made a forest)
+  if ((int)t->h_sys_start.size() != nsys) {
+    t->h_sys_start.assign(1, 0);
+    t->h_sys_n.assign(1, n);
+    t->h_sys_maxmemb.assign(1, t->maxmemb);
+  }
+  t->sys_start.ensure(c, nsys);
+  t->sys_n.ensure(c, nsys);
+  t->sys_maxmemb.ensure(c, nsys);
+  BIT_CUDA(cudaMemcpyAsync(t->sys_start.p, t->h_sys_start.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, s));
+  BIT_CUDA(cudaMemcpyAsync(t->sys_n.p, t->h_sys_n.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, s));
+  BIT_CUDA(cudaMemcpyAsync(t->sys_maxmemb.p, t->h_sys_maxmemb.data(), nsys * sizeof(int), cudaMemcpyHostToDevice, s));
   t->perm.ensure(c, n);
   t->sx.ensure(c, n); t->sy.ensure(c, n); t->sz.ensure(c, n);
   DBuf<int> perm2; DBuf<double> sx2, sy2, sz2;
   perm2.ensure(c, n); sx2.ensure(c, n); sy2.ensure(c, n); sz2.ensure(c, n);
   DBuf<signed char> lab;
   lab.ensure(c, n);
-  int cap = std::max(64, 16 * (n / std::max(t->maxmemb, 1) + 1) + 64);
+  long long capl = 64;
+  for (int k = 0; k < nsys; k++)
+    capl += 16LL * (t->h_sys_n[k] / std::max(t->h_sys_maxmemb[k], 1) + 1) + 8;
+  int cap = (int)std::min<long long>(capl, 1LL << 30);
   t->nummemb.ensure(c, cap); t->start.ensure(c, cap); t->level.ensure(c, cap);
   t->parent.ensure(c, cap); t->children.ensure(c, 8LL * cap); t->fields.ensure(c, 13LL * cap);
+  t->node_sys.ensure(c, cap);
   DBuf<int> err;
   err.ensure(c, 4);
   BIT_CUDA(cudaMemsetAsync(err.p, 0, 4 * sizeof(int), s));
@@ -576,19 +604,23 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
   BIT_CUDA(cudaMemsetAsync(lab.p, -1, n, s));
 
   DBuf<SplitAcc> acc;
-  acc.ensure(c, 1);
-  count_launch(), k_acc_reset<<<1, 32, 0, s>>>(acc.p, 1);
-  count_launch(), k_root_bbox<<<std::min<unsigned>(grid_for(n, 256), 4 * c->num_sms), 256, 0, s>>>(
-      n, t->sx.p, t->sy.p, t->sz.p, acc.p, err.p);
-  count_launch(), k_root_init<<<1, 1, 0, s>>>(n, acc.p, t->nummemb.p, t->start.p, t->children.p, t->level.p,
-                             t->parent.p, t->fields.p);
+  acc.ensure(c, nsys);
+  count_launch(), k_acc_reset<<<grid_for(nsys, 128), 128, 0, s>>>(acc.p, nsys);
+  {
+    const unsigned per = std::max(1u, std::min<unsigned>(grid_for(n / nsys + 1, 256), 4 * c->num_sms / nsys + 1));
+    count_launch(), k_root_bbox<<<dim3(per, nsys), 256, 0, s>>>(t->sys_start.p, t->sys_n.p, t->sx.p,
+                                                                t->sy.p, t->sz.p, acc.p, err.p);
+  }
+  count_launch(), k_root_init<<<grid_for(nsys, 128), 128, 0, s>>>(
+      nsys, t->sys_start.p, t->sys_n.p, acc.p, t->nummemb.p, t->start.p, t->children.p,
+      t->level.p, t->parent.p, t->fields.p, t->node_sys.p);
   BIT_CHECK_LAUNCH();
 
   const double lim = 1.0 / std::sqrt(2.0);  // src/tree3d.cpp:1371
   DBuf<SplitState> st;
   DBuf<int> nchunk, cbeg, cc, coff, nch, cscan;
   DBuf<int2> chunks;
-  int a = 0, b = 1, depth = 1;
+  int a = 0, b = nsys, depth = 1;
   while (true) {
     const int nlev = b - a;
     st.ensure(c, nlev);
@@ -598,7 +630,8 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     nch.ensure(c, nlev);
     cscan.ensure(c, nlev + 1);
     const unsigned gl = grid_for(nlev, 128);
-    count_launch(), k_level_init<<<gl, 128, 0, s>>>(a, nlev, t->nummemb.p, t->maxmemb, st.p, acc.p, nchunk.p);
+    count_launch(), k_level_init<<<gl, 128, 0, s>>>(a, nlev, t->nummemb.p, t->node_sys.p,
+                                                    t->sys_maxmemb.p, st.p, acc.p, nchunk.p);
     count_launch(), k_scan_small<<<1, 1024, 0, s>>>(nchunk.p, cbeg.p, nlev);
     BIT_CUDA(cudaMemcpyAsync(hp, cbeg.p + nlev, sizeof(int), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
@@ -608,22 +641,23 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     cc.ensure(c, 8LL * nch_total);
     coff.ensure(c, 8LL * nch_total);
     count_launch(), k_fill_chunks<<<gl, 128, 0, s>>>(a, nlev, t->start.p, t->nummemb.p, cbeg.p, chunks.p);
-    count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, st.p, acc.p, t->maxmemb, lim, err.p);
+    count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, t->node_sys.p,
+                                                      t->sys_maxmemb.p, st.p, acc.p, lim, err.p);
     for (int step = 0; step < 7; step++) {
       count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
-                                            t->sy.p, t->sz.p, lab.p, st.p, acc.p);
-      count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, st.p, acc.p, t->maxmemb, lim,
-                                        err.p);
+                                                            t->sy.p, t->sz.p, lab.p, st.p, acc.p);
+      count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, t->node_sys.p,
+                                                        t->sys_maxmemb.p, st.p, acc.p, lim, err.p);
     }
     count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
-                                          t->sy.p, t->sz.p, lab.p, st.p, acc.p);
+                                                          t->sy.p, t->sz.p, lab.p, st.p, acc.p);
     count_launch(), k_scatter_count<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, cc.p);
     count_launch(), k_scatter_offsets<<<gl, 128, 0, s>>>(a, nlev, t->start.p, cbeg.p, cc.p, coff.p, st.p, err.p);
     count_launch(), k_scatter<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, coff.p,
-                                       t->perm.p, t->sx.p, t->sy.p, t->sz.p, perm2.p, sx2.p,
-                                       sy2.p, sz2.p);
+                                                       t->perm.p, t->sx.p, t->sy.p, t->sz.p, perm2.p, sx2.p,
+                                                       sy2.p, sz2.p);
     count_launch(), k_copy_back<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, perm2.p, sx2.p,
-                                         sy2.p, sz2.p, t->perm.p, t->sx.p, t->sy.p, t->sz.p);
+                                                         sy2.p, sz2.p, t->perm.p, t->sx.p, t->sy.p, t->sz.p);
     // the next level's members start unlabelled
     BIT_CUDA(cudaMemsetAsync(lab.p, -1, n, s));
     count_launch(), k_child_counts<<<gl, 128, 0, s>>>(nlev, st.p, nch.p);
@@ -645,17 +679,19 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
       t->nummemb.grow(c, ncap, b, s); t->start.grow(c, ncap, b, s);
       t->level.grow(c, ncap, b, s); t->parent.grow(c, ncap, b, s);
       t->children.grow(c, 8LL * ncap, 8LL * b, s); t->fields.grow(c, 13LL * ncap, 13LL * b, s);
+      t->node_sys.grow(c, ncap, b, s);
       cap = ncap;
     }
     count_launch(), k_make_children<<<gl, 128, 0, s>>>(a, b, nlev, st.p, cscan.p, t->nummemb.p, t->start.p,
-                                       t->children.p, t->level.p, t->parent.p, t->fields.p);
+                                                       t->children.p, t->level.p, t->parent.p, t->fields.p,
+                                                       t->node_sys.p);
     BIT_CHECK_LAUNCH();
     a = b;
     b += total;
     depth++;
   }
   {
-    // the root alone (n <= maxmemb) still has to report NaNs
+    // roots that are leaves (n <= maxmemb) still have to report NaNs
     BIT_CUDA(cudaMemcpyAsync(hp + 1, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
     if (*reinterpret_cast<int*>(hp + 1) & 1)
@@ -677,7 +713,7 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
                            cudaMemcpyHostToDevice, s));
   t->leaf_of.ensure(c, n);
   count_launch(), k_leaf_of<<<t->nleaves, 256, 0, s>>>(t->nleaves, t->leaves.p, t->start.p, t->nummemb.p,
-                                       t->leaf_of.p);
+                                                       t->leaf_of.p);
   t->iperm.ensure(c, n);
   count_launch(), k_iperm<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->iperm.p);
   BIT_CHECK_LAUNCH();
@@ -696,12 +732,13 @@ void tree_sync_host(Tree* t) {
   cudaStream_t s = t->ctx->stream;
   const int b = t->numtree;
   t->h_nummemb.resize(b); t->h_start.resize(b); t->h_children.resize(8LL * b);
-  t->h_level.resize(b); t->h_fields.resize(13LL * b);
+  t->h_level.resize(b); t->h_fields.resize(13LL * b); t->h_node_sys.resize(b);
   BIT_CUDA(cudaMemcpyAsync(t->h_nummemb.data(), t->nummemb.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaMemcpyAsync(t->h_start.data(), t->start.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaMemcpyAsync(t->h_children.data(), t->children.p, 8LL * b * sizeof(int), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaMemcpyAsync(t->h_level.data(), t->level.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaMemcpyAsync(t->h_fields.data(), t->fields.p, 13LL * b * sizeof(double), cudaMemcpyDeviceToHost, s));
+  BIT_CUDA(cudaMemcpyAsync(t->h_node_sys.data(), t->node_sys.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaStreamSynchronize(s));
 }
 

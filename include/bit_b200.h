@@ -161,6 +161,32 @@ bit_status bit_tree_target_lists(bit_tree* tree, const bit_eval_params* prm, int
                                  int* node, int* kind, int cap, int* n);
 
 /* ---------------------------------------------------------------------------------
+ * Forests: many independent systems in one tree, built, expanded and evaluated by the
+ * same launches (no reference counterpart: the reference handles one system per
+ * treemake / treepotential loop, src/tree3d.cpp:1345, 4679; this replaces a host loop of
+ * those calls over many systems).
+ * System s owns particles [o_s, o_s + n[s]) of x, y, z, q (o_s = n[0] + ... + n[s-1]).
+ * Its subtree is the tree treemake builds for those particles alone with maxmemb[s] (same
+ * nodes, children order and members), rooted at node s; its moments, MAC and kernel are
+ * its own, so every system's result equals a separate single-system evaluation.
+ * ------------------------------------------------------------------------------- */
+bit_status bit_forest_build(bit_ctx* ctx, int nsys, const int* n, const int* maxmemb,
+                            const double* x, const double* y, const double* z,
+                            bit_tree** tree);
+bit_status bit_forest_build_device(bit_ctx* ctx, int nsys, const int* n, const int* maxmemb,
+                                   const double* x, const double* y, const double* z,
+                                   bit_tree** tree);
+/* Moments of every system: nterms[s] (1..BIT_NTERMS_MAX) per system. */
+bit_status bit_forest_moments(bit_tree* tree, const int* nterms);
+/* Potential at every particle with params[s] for system s (one precision for all).
+ * pot: host array (bit_forest_eval) or device array (bit_forest_eval_device), original
+ * order. */
+bit_status bit_forest_eval(bit_tree* tree, const bit_eval_params* params, double* pot);
+bit_status bit_forest_eval_device(bit_tree* tree, const bit_eval_params* params, double* pot);
+/* Number of systems; first node of system s is its root, node s. */
+bit_status bit_forest_systems(const bit_tree* tree, int* nsys);
+
+/* ---------------------------------------------------------------------------------
  * GMRES with the treecode as its matvec (no reference counterpart: the reference's
  * solver::gmres, src/solver.h:157-260, takes a dense matrix).
  * Solves (diag*I + K) s = f, (K s)_i = sum_{j != i} G(x_i, x_j) w_j s_j, G from prm.
