@@ -121,6 +121,8 @@ SIGNATURES = [
     ("bit_forest_eval", C.c_int, [_vp, C.POINTER(EvalParams), _dp]),
     ("bit_forest_eval_device", C.c_int, [_vp, C.POINTER(EvalParams), _vp]),
     ("bit_forest_systems", C.c_int, [_vp, _ip]),
+    ("bit_gmres_dense_static", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip, C.c_char_p,
+                                         C.c_int]),
 ]
 
 _lib = None

@@ -16,6 +16,8 @@
 // of x is below 1e-5 on odd steps (:243-255), breakdown at h < 1e-14 (:220-225).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "common.cuh"
@@ -487,3 +489,163 @@ extern "C" bit_status bit_gmres_dense(bit_ctx* h, int n, const double* a, const 
   });
   return st != BIT_OK ? st : result;
 }
+
+// ---- bit_gmres_dense_static: the dense GMRES above with no allocation at call time ------
+// Device scratch is one file-scope array sized for n <= BIT_GMRES_STATIC_MAX; host scratch
+// (Hessenberg and the least-squares work arrays) is file-scope too.  Its address on each
+// device is looked up once (cudaGetSymbolAddress, with that device current).  Calls that
+// overlap in time (two host threads, or two streams of one device) share this scratch and
+// race; the first call on a device does the set-up and must come before any stream capture.
+namespace bit {
+namespace {
+
+constexpr int kStaticMax = BIT_GMRES_STATIC_MAX;
+constexpr size_t rup32(size_t v) { return (v + 31) / 32 * 32; }
+// segments, in doubles, each a multiple of 256 bytes
+constexpr size_t kSegA = rup32((size_t)kStaticMax * kStaticMax);
+constexpr size_t kSegQ = rup32((size_t)(kStaticMax + 1) * kStaticMax);
+constexpr size_t kSegV = rup32(kStaticMax);
+constexpr size_t kSegH = rup32(kStaticMax + 2);
+constexpr size_t kSegY = rup32(kStaticMax + 1);
+constexpr size_t kSegX = rup32(kStaticMax);
+constexpr size_t kSegE = 32;
+constexpr size_t kStaticDoubles = kSegA + kSegQ + kSegV + kSegH + kSegY + kSegX + kSegE;
+
+static __device__ __align__(256) double g_dense_static[kStaticDoubles];
+
+constexpr int kStaticDevices = 64;
+double* s_dense_static_ptr[kStaticDevices];  // device address of g_dense_static, per device
+
+constexpr size_t kLd = kStaticMax + 1;
+double s_H[(kStaticMax + 2) * kLd];
+double s_V2[(kStaticMax + 1) * kStaticMax];
+double s_Q2[(kStaticMax + 1) * kStaticMax];
+double s_R2[kStaticMax * kStaticMax];
+double s_yv[kStaticMax + 1];
+double s_hc[kStaticMax + 2];
+double s_q0[kStaticMax];
+
+void put_err(char* err, int len, const char* what, const char* detail) {
+  if (err && len > 0) std::snprintf(err, (size_t)len, "%s%s%s", what, detail ? ": " : "", detail ? detail : "");
+}
+
+}  // namespace
+}  // namespace bit
+
+#define BIT_STATIC_CK(call)                                                    \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      bit::put_err(err, errlen, #call, cudaGetErrorString(e_));                \
+      return BIT_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+extern "C" bit_status bit_gmres_dense_static(void* stream, int n, const double* a,
+                                             const double* b, double* x, int* iterations,
+                                             char* err, int errlen) {
+  using namespace bit;
+  if (err && errlen > 0) err[0] = '\0';
+  if (!a || !b || !x || n < 1) {
+    put_err(err, errlen, "a, b and x must be non-NULL and n >= 1", nullptr);
+    return BIT_ERR_INVALID_ARGUMENT;
+  }
+  if (n > kStaticMax) {
+    char d[96];
+    std::snprintf(d, sizeof d, "n = %d exceeds the static scratch limit %d", n, kStaticMax);
+    put_err(err, errlen, "bit_gmres_dense_static", d);
+    return BIT_ERR_CAPACITY;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int dev = 0;
+  BIT_STATIC_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticDevices) {
+    put_err(err, errlen, "bit_gmres_dense_static", "device ordinal out of range");
+    return BIT_ERR_INVALID_ARGUMENT;
+  }
+  if (!s_dense_static_ptr[dev]) {
+    void* p = nullptr;
+    BIT_STATIC_CK(cudaGetSymbolAddress(&p, g_dense_static));
+    s_dense_static_ptr[dev] = static_cast<double*>(p);
+  }
+  double* base = s_dense_static_ptr[dev];
+  double* A = base;
+  double* Q = A + kSegA;
+  double* v = Q + kSegQ;
+  double* hd = v + kSegV;
+  double* y = hd + kSegH;
+  double* xd = y + kSegY;
+  double* me = xd + kSegX;
+  // the reductions' outputs start from zero on every call
+  BIT_STATIC_CK(cudaMemsetAsync(hd, 0, kSegH * sizeof(double), s));
+  BIT_STATIC_CK(cudaMemsetAsync(me, 0, kSegE * sizeof(double), s));
+  BIT_STATIC_CK(cudaMemcpyAsync(A, a, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  BIT_STATIC_CK(cudaMemcpyAsync(xd, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  double bnorm = 0.0;
+  for (int i = 0; i < n; i++) bnorm += b[i] * b[i];
+  bnorm = std::sqrt(bnorm);
+  for (int i = 0; i < n; i++) s_q0[i] = b[i] / bnorm;
+  BIT_STATIC_CK(cudaMemcpyAsync(Q, s_q0, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  // the copies above read host scratch asynchronously: finish them before it is reused
+  BIT_STATIC_CK(cudaStreamSynchronize(s));
+  const int ld = n + 1;
+  std::memset(s_H, 0, (size_t)(n + 2) * ld * sizeof(double));
+  bit_status result = BIT_OK;
+  int go = 1, nn = 0;
+  while (go) {
+    const int n1 = nn + 1;
+    count_launch(), k_dense_gemv<<<grid_for(n, 8), 256, 0, s>>>(n, A, Q + (long long)nn * n, v);
+    count_launch(), k_dense_mgs<<<1, 1024, 0, s>>>(n, n1, Q, v, hd, Q + (long long)n1 * n);
+    BIT_STATIC_CK(cudaGetLastError());
+    BIT_STATIC_CK(cudaMemcpyAsync(s_hc, hd, (n1 + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_STATIC_CK(cudaStreamSynchronize(s));
+    for (int j = 0; j <= n1; j++) s_H[(size_t)j * ld + nn] = s_hc[j];
+    if (n1 < n && s_hc[n1] < 1e-14) {
+      go = 0;
+      result = BIT_ERR_BREAKDOWN;
+    }
+    // minimize(n1): Gram-Schmidt QR of the (n1+1) x n1 Hessenberg, back substitution
+    const int m = n1;
+    std::memset(s_V2, 0, (size_t)(m + 1) * m * sizeof(double));
+    std::memset(s_Q2, 0, (size_t)(m + 1) * m * sizeof(double));
+    std::memset(s_R2, 0, (size_t)m * m * sizeof(double));
+    for (int j = 0; j < m; j++)
+      for (int i = 0; i < j + 2; i++) s_V2[(size_t)i * m + j] = s_H[(size_t)i * ld + j];
+    for (int i = 0; i < m; i++) {
+      const int ind = i + 2;
+      double rr = 0.0;
+      for (int k = 0; k < ind; k++) rr += s_V2[(size_t)k * m + i] * s_V2[(size_t)k * m + i];
+      rr = std::sqrt(rr);
+      s_R2[(size_t)i * m + i] = rr;
+      for (int k = 0; k < ind; k++) s_Q2[(size_t)k * m + i] = s_V2[(size_t)k * m + i] / rr;
+      for (int j = i + 1; j < m; j++) {
+        double r = 0.0;
+        for (int k = 0; k < ind; k++) r += s_Q2[(size_t)k * m + i] * s_V2[(size_t)k * m + j];
+        s_R2[(size_t)i * m + j] = r;
+        for (int k = 0; k < ind; k++) s_V2[(size_t)k * m + j] -= r * s_Q2[(size_t)k * m + i];
+      }
+    }
+    for (int i = m - 1; i > -1; i--) {
+      double t = bnorm * s_Q2[i];
+      for (int j = i + 1; j < m; j++) t -= s_R2[(size_t)i * m + j] * s_yv[j];
+      s_yv[i] = t / s_R2[(size_t)i * m + i];
+    }
+    if (n1 == n) go = 0;
+    if (n1 % 2 || !go) {
+      BIT_STATIC_CK(cudaMemcpyAsync(y, s_yv, n1 * sizeof(double), cudaMemcpyHostToDevice, s));
+      count_launch(), k_dense_update<<<1, 1024, 0, s>>>(n, n1, Q, y, xd, me);
+      BIT_STATIC_CK(cudaGetLastError());
+      double maxerr = 0.0;
+      BIT_STATIC_CK(cudaMemcpyAsync(&maxerr, me, sizeof(double), cudaMemcpyDeviceToHost, s));
+      BIT_STATIC_CK(cudaStreamSynchronize(s));
+      if (maxerr < 1e-5 && nn > 1) go = 0;
+    }
+    nn++;
+  }
+  BIT_STATIC_CK(cudaMemcpyAsync(x, xd, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  BIT_STATIC_CK(cudaStreamSynchronize(s));
+  if (iterations) *iterations = nn;
+  if (result == BIT_ERR_BREAKDOWN) put_err(err, errlen, "GMRES breakdown (h < 1e-14)", nullptr);
+  return result;
+}
+#undef BIT_STATIC_CK

@@ -220,6 +220,22 @@ bit_status bit_bie_solve(bit_tree* tree, const bit_eval_params* prm, int nterms,
 bit_status bit_gmres_dense(bit_ctx* ctx, int n, const double* a, const double* b, double* x,
                            int* iterations);
 
+/* bit_gmres_dense without any allocation at call time, for callers that cannot allocate
+ * (no reference counterpart: it is the same solve as bit_gmres_dense / solver::gmres,
+ * src/solver.h:157-310, with the same kernels and results).
+ * Scratch is one file-scope device array (about 4.2 MB) sized for n <= BIT_GMRES_STATIC_MAX,
+ * plus file-scope host arrays; no cudaMalloc / cudaFree and no allocating library call is
+ * made.  n > BIT_GMRES_STATIC_MAX returns BIT_ERR_CAPACITY.  Runs on the calling thread's
+ * current device, on `stream` (a cudaStream_t; NULL = the default stream), with host
+ * arrays a (row-major n x n), b, x (initial values in, solution out).  A message for any
+ * error goes to err (errlen bytes, NUL-terminated; may be NULL).
+ * Calls that overlap in time share the scratch and race: serialise them.  The first call
+ * on a device looks up the scratch's address (cudaGetSymbolAddress) and must come before
+ * any stream capture. */
+#define BIT_GMRES_STATIC_MAX 512
+bit_status bit_gmres_dense_static(void* stream, int n, const double* a, const double* b,
+                                  double* x, int* iterations, char* err, int errlen);
+
 #ifdef __cplusplus
 }
 #endif
