@@ -58,7 +58,7 @@ class Stats(C.Structure):
                 ("far_entries", C.c_longlong), ("near_entries", C.c_longlong),
                 ("batches", C.c_longlong), ("numtree", C.c_int), ("nleaves", C.c_int),
                 ("depth", C.c_int), ("nterms", C.c_int), ("far_launches", C.c_int),
-                ("near_launches", C.c_int)]
+                ("near_launches", C.c_int), ("list_fallback", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -121,6 +121,10 @@ SIGNATURES = [
     ("bit_forest_eval", C.c_int, [_vp, C.POINTER(EvalParams), _dp]),
     ("bit_forest_eval_device", C.c_int, [_vp, C.POINTER(EvalParams), _vp]),
     ("bit_forest_systems", C.c_int, [_vp, _ip]),
+    ("bit_direct_potential", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, C.POINTER(EvalParams),
+                                       C.c_int, _ip, _dp]),
+    ("bit_direct_potential_device", C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp,
+                                              C.POINTER(EvalParams), C.c_int, _vp, _vp]),
     ("bit_gmres_dense_static", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip, C.c_char_p,
                                          C.c_int]),
 ]
@@ -223,6 +227,20 @@ class Context:
     def forest(self, x, y, z, sizes, maxmemb):
         """Independent systems in one tree: system s is the next sizes[s] particles."""
         return Forest(self, x, y, z, sizes, maxmemb)
+
+    def direct(self, x, y, z, q, prm, targets):
+        """FP64 direct sum at particle targets (bit_direct_potential)."""
+        x, y, z, q = map(_f64, (x, y, z, q))
+        tg = np.ascontiguousarray(targets, dtype=np.int32)
+        out = np.zeros(len(tg))
+        self.check(lib().bit_direct_potential(self.h, len(x), _d(x), _d(y), _d(z), _d(q),
+                                              C.byref(prm), len(tg), tg.ctypes.data_as(_ip),
+                                              _d(out)), "bit_direct_potential")
+        return out
+
+    def direct_device(self, n, xp, yp, zp, qp, prm, m, tgp, outp):
+        self.check(lib().bit_direct_potential_device(self.h, n, xp, yp, zp, qp, C.byref(prm), m,
+                                                     tgp, outp), "bit_direct_potential_device")
 
     def gmres_dense(self, A, b, x0=None):
         """solver::gmres (src/solver.h:157) on the device."""

@@ -163,6 +163,7 @@ void eval_particles_sorted(Tree* t, const std::vector<bit_eval_params>& prm) {
   t->stats.batches = t->plists.ngroups;
   t->stats.far_launches = (int)t->pplan.far_classes.size();
   t->stats.near_launches = (int)t->pplan.near_classes.size();
+  t->stats.list_fallback = t->plists.fallback ? 1 : 0;
 }
 
 uint64_t spread3(uint64_t v) {
@@ -658,6 +659,50 @@ bit_status bit_treecode_potential(bit_ctx* h, int n, const double* x, const doub
     h->c.last_error = keep;
   }
   return st;
+}
+
+bit_status bit_direct_potential(bit_ctx* h, int n, const double* x, const double* y,
+                                const double* z, const double* q, const bit_eval_params* prm,
+                                int m, const int* targets, double* pot) {
+  if (!h || !x || !y || !z || !q || !prm || !targets || !pot || n < 1 || m < 0)
+    return BIT_ERR_INVALID_ARGUMENT;
+  if (m == 0) return BIT_OK;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    check_params(prm);
+    for (int i = 0; i < m; i++)
+      if (targets[i] < 0 || targets[i] >= n) fail(BIT_ERR_INVALID_ARGUMENT, "target index out of range");
+    BIT_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    DBuf<double> dx, dy, dz, dq, out;
+    DBuf<int> dt;
+    dx.ensure(c, n); dy.ensure(c, n); dz.ensure(c, n); dq.ensure(c, n);
+    dt.ensure(c, m); out.ensure(c, m);
+    BIT_CUDA(cudaMemcpyAsync(dx.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dy.p, y, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dz.p, z, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dq.p, q, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(dt.p, targets, m * sizeof(int), cudaMemcpyHostToDevice, s));
+    direct_potential(c, n, dx.p, dy.p, dz.p, dq.p, *prm, m, dt.p, out.p);
+    BIT_CUDA(cudaMemcpyAsync(pot, out.p, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    check_dev_err(c);
+  });
+}
+
+bit_status bit_direct_potential_device(bit_ctx* h, int n, const double* x, const double* y,
+                                       const double* z, const double* q,
+                                       const bit_eval_params* prm, int m, const int* targets,
+                                       double* pot) {
+  if (!h || !x || !y || !z || !q || !prm || !targets || !pot || n < 1 || m < 0)
+    return BIT_ERR_INVALID_ARGUMENT;
+  if (m == 0) return BIT_OK;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    check_params(prm);
+    BIT_CUDA(cudaSetDevice(c->device));
+    direct_potential(c, n, x, y, z, q, *prm, m, targets, pot);
+  });
 }
 
 bit_status bit_tree_stats(const bit_tree* th, bit_stats* st) {

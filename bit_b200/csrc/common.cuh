@@ -138,6 +138,9 @@ struct Lists {
   DBuf<int> order;                          // groups by decreasing work
   std::vector<long long> h_work;            // estimated work of each group
   long long version = 0;                    // bumped by every build
+  int last_ngroups = 0;                     // groups and totals of the last build (sizing)
+  unsigned long long last_totals[4] = {0, 0, 0, 0};
+  bool fallback = false;                    // the last build used count, scan and fill
 };
 
 struct Ctx {
@@ -184,6 +187,7 @@ struct Tree {
   DBuf<int> nummemb, start, children, level, parent;
   DBuf<double> fields;   // 13 per node
   DBuf<double4> nodec;   // (xmid, ymid, zmid, sqradius)
+  DBuf<float4> nodeh;    // half extents of the box about the midpoint (rounded up)
   DBuf<int> leaves;
   // host mirror of the node structure
   std::vector<int> h_nummemb, h_start, h_children, h_level, h_perm;
@@ -232,6 +236,10 @@ void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const doub
 void eval_near(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
                const double* tz, double* out_sorted);
 void eval_far_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz);
+// FP64 direct sum at m particle targets tg (device pointers); out[i] for target i.
+void direct_potential(Ctx* c, int n, const double* x, const double* y, const double* z,
+                      const double* q, const bit_eval_params& p, int m, const int* tg,
+                      double* out);
 void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz);
 
 // Per-system parameters of a potential (force = 0) or field (force = 1) evaluation.

@@ -14,8 +14,9 @@
 // Single pass: each CTA stages its entries in shared memory, then reserves room in the
 // global lists with one atomic per list and copies them out (a group's entries stay
 // contiguous and in order; groups land in completion order, addressed by begin/count).
-// A group whose entries do not fit the staging area makes the whole build fall back to a
-// count pass, a prefix sum and a fill pass.
+// The lists are written in place, into arrays sized from an estimate.  A group whose
+// entries do not fit its staging area, or whose reservation runs past the arrays, makes
+// the whole build fall back to a count pass, a prefix sum and a fill pass.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -49,7 +50,8 @@ struct ListArgs {
   unsigned *far_mask, *near_mask;
   unsigned long long* totals;  // far entries, far words, near entries, near words
   unsigned long long* pairs;   // far pairs, near pairs
-  int* err;                    // 1: stack overflow, 2: staging overflow
+  int* err;                    // 1: stack overflow, 2: staging or arena overflow
+  unsigned long long cap[4];   // MODE_STAGE: room in the four output arrays
 };
 
 template <int MODE>
@@ -161,6 +163,12 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
     s_base[1] = atomicAdd(&a.totals[1], (unsigned long long)(nf * W));
     s_base[2] = atomicAdd(&a.totals[2], (unsigned long long)nn);
     s_base[3] = atomicAdd(&a.totals[3], (unsigned long long)(nn * W));
+    // the arrays were sized from an estimate: past their end, the build falls back
+    if (s_base[0] + nf > a.cap[0] || s_base[1] + nf * W > a.cap[1] ||
+        s_base[2] + nn > a.cap[2] || s_base[3] + nn * W > a.cap[3]) {
+      atomicOr(a.err, 2);
+      s_base[0] = ~0ull;
+    }
     a.far_off[g] = (long long)s_base[0];
     a.far_moff[g] = (long long)s_base[1];
     a.near_off[g] = (long long)s_base[2];
@@ -169,6 +177,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
     a.near_cnt[g] = (int)nn;
   }
   __syncthreads();
+  if (s_base[0] == ~0ull) return;
   for (int k = threadIdx.x; k < nf; k += LT) a.far_node[s_base[0] + k] = sf_node[k];
   for (int k = threadIdx.x; k < nf * W; k += LT) a.far_mask[s_base[1] + k] = sf_mask[k];
   for (int k = threadIdx.x; k < nn; k += LT) a.near_node[s_base[2] + k] = sn_node[k];
@@ -290,15 +299,28 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   a.totals = cnt.p;
   a.pairs = cnt.p + 4;
   a.err = reinterpret_cast<int*>(cnt.p + 6);
-  // worst case of the single pass: every group's staging area full
-  DBuf<int> snode_f, snode_n;
-  DBuf<unsigned> smask_f, smask_n;
-  snode_f.ensure(c, (size_t)ng * STAGE_FAR / 2);
-  smask_f.ensure(c, (size_t)ng * STAGE_FAR);
-  snode_n.ensure(c, (size_t)ng * STAGE_NEAR / 2);
-  smask_n.ensure(c, (size_t)ng * STAGE_NEAR);
-  a.far_node = snode_f.p; a.far_mask = smask_f.p;
-  a.near_node = snode_n.p; a.near_mask = smask_n.p;
+  // Single pass straight into the lists, sized from an estimate: the last build's totals
+  // scaled by the group count, else a per-group allowance.  A group that does not fit
+  // its staging area or the arrays makes the build fall back to count, scan and fill.
+  long long words = 0;
+  for (int g = 0; g < ng; g++) words += (tc[g] + 31) / 32;
+  unsigned long long cap[4];
+  if (L->last_ngroups > 0) {
+    const double f = 1.25 * (double)ng / L->last_ngroups;
+    for (int k = 0; k < 4; k++) cap[k] = (unsigned long long)(f * L->last_totals[k]) + 1024;
+  } else {
+    cap[0] = 192ull * ng + 1024;
+    cap[1] = 192ull * words + 1024;
+    cap[2] = 48ull * ng + 1024;
+    cap[3] = 48ull * words + 1024;
+  }
+  L->far_node.ensure(c, cap[0]);
+  L->far_mask.ensure(c, cap[1]);
+  L->near_node.ensure(c, cap[2]);
+  L->near_mask.ensure(c, cap[3]);
+  for (int k = 0; k < 4; k++) a.cap[k] = cap[k];
+  a.far_node = L->far_node.p; a.far_mask = L->far_mask.p;
+  a.near_node = L->near_node.p; a.near_mask = L->near_mask.p;
   set_stage_attr();
   count_launch(), k_lists<MODE_STAGE><<<ng, LT, STAGE_BYTES, s>>>(a);
   BIT_CHECK_LAUNCH();
@@ -310,8 +332,9 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   BIT_CUDA(cudaStreamSynchronize(s));
   int err = (int)(h[6] & 0xffffffffu);
   if (err & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded (tree deeper than supported)");
+  L->fallback = (err & 2) != 0;
   if (err & 2) {
-    // some group's lists exceed the staging area: count, scan, fill
+    // some group's lists exceed the staging area or the arrays: count, scan, fill
     BIT_CUDA(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s));
     count_launch(), k_lists<MODE_COUNT><<<ng, LT, 0, s>>>(a);
     count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->far_cnt.p, nullptr, L->far_off.p, ng, cnt.p + 0);
@@ -331,17 +354,9 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
     a.near_node = L->near_node.p; a.near_mask = L->near_mask.p;
     count_launch(), k_lists<MODE_FILL><<<ng, LT, 0, s>>>(a);
     BIT_CHECK_LAUNCH();
-  } else {
-    // exact-size copies of the staged lists
-    L->far_node.ensure(c, h[0]);
-    L->far_mask.ensure(c, h[1]);
-    L->near_node.ensure(c, h[2]);
-    L->near_mask.ensure(c, h[3]);
-    BIT_CUDA(cudaMemcpyAsync(L->far_node.p, snode_f.p, h[0] * sizeof(int), cudaMemcpyDeviceToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(L->far_mask.p, smask_f.p, h[1] * sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(L->near_node.p, snode_n.p, h[2] * sizeof(int), cudaMemcpyDeviceToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(L->near_mask.p, smask_n.p, h[3] * sizeof(unsigned), cudaMemcpyDeviceToDevice, s));
   }
+  L->last_ngroups = ng;
+  for (int k = 0; k < 4; k++) L->last_totals[k] = h[k];
   L->nfar = (long long)h[0];
   L->nnear = (long long)h[2];
   L->far_pairs = (long long)h[4];

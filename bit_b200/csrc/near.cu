@@ -12,7 +12,9 @@
 //
 // FP64 path: the reference's arithmetic.  Mixed path: sources in FP32 relative to their
 // leaf centre, the target's offset from that centre formed in FP64 and rounded once, MUFU
-// rsqrt / ex2, and per-target compensated (two-sum) accumulation.
+// rsqrt / ex2, and per-target compensated (two-sum) accumulation; pairs too close for FP32
+// coordinates are summed in FP64 (below).  The self pair is skipped by splitting each
+// lane's index range around it.
 #include <climits>
 
 #include "common.cuh"
@@ -35,6 +37,7 @@ struct NearArgs {
   const double4* nodec;
   const void* src;  // float4 (mixed) or double4 (FP64) in tree order
   const double4* src64;
+  const float4* nodeh;  // per node: half extents of the box, rounded up
   const double* sw;
   const SysEval* sys;  // per system: near_del, kappa, intg, near_sign, self_term, particles
   const int* g_sys;    // per group: system
@@ -75,17 +78,7 @@ struct Prec<false> {
   static constexpr int TILE = 512;
 };
 
-// One pair's contribution.  Mixed: target and source relative to the source leaf centre.
-template <int KER, bool EPS>
-__device__ __forceinline__ float pair(float xt, float yt, float zt, float4 s, float del,
-                                      float kl2) {
-  const float dx = s.x - xt, dy = s.y - yt, dz = s.z - zt;
-  const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
-  const float ri = rsqrt_approx(r2);
-  float v = KER == BIT_KERNEL_COULOMB ? s.w * ri : s.w * ex2_approx(r2 * ri * kl2) * ri;
-  if (EPS && !(r2 > (float)kEpsNear)) v = 0.f;
-  return v;
-}
+// One pair's contribution in FP64 (the reference's arithmetic).
 template <int KER, bool EPS>
 __device__ __forceinline__ double pair(double x, double y, double z, double4 s, double del,
                                        double kappa) {
@@ -98,14 +91,6 @@ __device__ __forceinline__ double pair(double x, double y, double z, double4 s, 
 }
 // Field of eval_grad_kernel_reg (src/tree3d.cpp:73-97), KERNEL_ORDER = 0:
 // q * (-(x_j - x) / (r * r^2)).
-__device__ __forceinline__ void fpair(float xt, float yt, float zt, float4 s, float del,
-                                      float& ax, float& ay, float& az) {
-  const float dx = xt - s.x, dy = yt - s.y, dz = zt - s.z;
-  const float rs = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
-  const float ri = rsqrt_approx(rs);
-  const float tq = s.w * ri * ri * ri;
-  ax = fmaf(dx, tq, ax); ay = fmaf(dy, tq, ay); az = fmaf(dz, tq, az);
-}
 __device__ __forceinline__ void fpair(double x, double y, double z, double4 s, double del,
                                       double& ax, double& ay, double& az) {
   const double dx = s.x - x, dy = s.y - y, dz = s.z - z;
@@ -119,6 +104,105 @@ template <class T>
 __device__ __forceinline__ T shfl_sum(T v, int tpt) {
   for (int o = tpt >> 1; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
+}
+
+// Close pairs in the mixed path.  FP32 leaf-centred coordinates carry an absolute error of
+// about 6e-8 of their magnitude, so a pair much closer than the leaf's size loses relative
+// accuracy in its FP32 difference (two particles 1e-4 apart in a leaf of size 0.1 give
+// ~1e-5).  Pairs closer than r_t = 1/32 of the source leaf's radius (r^2 below thr) are
+// left out of the FP32 sum and summed in FP64 from the FP64 sources instead, with the
+// reference's rules (including its r^2 <= 1e-14 skip, which only such pairs can meet:
+// thr >= 2e-14).  Every other pair keeps at most ~4e-6 relative error, far below 1e-6 of a
+// target's total.  Close pairs can only occur where a target lies within r_t of the source
+// leaf's box (its own leaf, or a neighbour's boundary), so a warp runs the checked loop on
+// those tiles and the plain loop, with no test at all, everywhere else.
+constexpr float kCloseFrac = 1.0f / 1024.0f;  // (1/32)^2
+constexpr float kThrMin = 2e-14f;             // above the 1e-14 skip of src/constants.h:35
+
+// Squared distance from a point (relative to a leaf's centre) to the leaf's box (half
+// extents h, rounded up); 0 inside.
+__device__ __forceinline__ float box_d2(float x, float y, float z, float4 h) {
+  const float dx = fmaxf(fabsf(x) - h.x, 0.f), dy = fmaxf(fabsf(y) - h.y, 0.f),
+              dz = fmaxf(fabsf(z) - h.z, 0.f);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// FP32 r^2 of a pair (identical wherever it is formed, so the FP32 and FP64 sums split the
+// pairs exactly).
+__device__ __forceinline__ float r2_32(float xt, float yt, float zt, float4 s, float del) {
+  const float dx = s.x - xt, dy = s.y - yt, dz = s.z - zt;
+  return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
+}
+
+// p += q * G(r); CHK: pairs with r^2 < thr are left out and flagged.
+template <int KER, bool CHK>
+__device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, float del,
+                                        float kl2, float thr, float& p, bool& close) {
+  float r2 = r2_32(xt, yt, zt, s, del);
+  float q = s.w;
+  if (CHK) {
+    const bool cl = r2 < thr;
+    close |= cl;
+    q = cl ? 0.f : q;
+    r2 = cl ? 1.f : r2;
+  }
+  const float ri = rsqrt_approx(r2);
+  if (KER == BIT_KERNEL_COULOMB) p = fmaf(q, ri, p);
+  else p = fmaf(q * ri, ex2_approx(r2 * ri * kl2), p);
+}
+
+// This lane's pairs j = jb, jb + tpt, ... < je, two accumulators.
+template <int KER, bool CHK>
+__device__ __forceinline__ void sweep_pot(const float4* fs, int j, int je, int tpt, float xt,
+                                          float yt, float zt, float del, float kl2, float thr,
+                                          float& p0, float& p1, bool& close) {
+  for (; j + tpt < je; j += 2 * tpt) {
+    acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
+    acc_pot<KER, CHK>(xt, yt, zt, fs[j + tpt], del, kl2, thr, p1, close);
+  }
+  if (j < je) acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
+}
+
+// FP64 sum of this lane's pairs with FP32 r^2 < thr (self skipped).
+template <int KER, bool EPS>
+__device__ __forceinline__ double close_pot(float xt, float yt, float zt, double x, double y,
+                                         double z, const float4* fs, const double4* s64,
+                                         int slice, int tpt, int ns, int selfj, float del,
+                                         float thr, double del64, double kappa) {
+  double acc = 0.0;
+  for (int j = slice; j < ns; j += tpt)
+    if (j != selfj && r2_32(xt, yt, zt, fs[j], del) < thr)
+      acc += pair<KER, EPS>(x, y, z, s64[j], del64, kappa);
+  return acc;
+}
+
+// Field of one pair, q (x - x_j) / r^3 (eval_grad_kernel_reg, src/tree3d.cpp:73-97,
+// KERNEL_ORDER = 0); CHK as acc_pot.
+template <bool CHK>
+__device__ __forceinline__ void acc_force(float xt, float yt, float zt, float4 s, float del,
+                                          float thr, float& ax, float& ay, float& az,
+                                          bool& close) {
+  const float dx = xt - s.x, dy = yt - s.y, dz = zt - s.z;
+  float rs = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
+  float q = s.w;
+  if (CHK) {
+    const bool cl = rs < thr;
+    close |= cl;
+    q = cl ? 0.f : q;
+    rs = cl ? 1.f : rs;
+  }
+  const float ri = rsqrt_approx(rs);
+  const float tq = q * ri * ri * ri;
+  ax = fmaf(dx, tq, ax); ay = fmaf(dy, tq, ay); az = fmaf(dz, tq, az);
+}
+
+__device__ __forceinline__ void close_force(float xt, float yt, float zt, double x, double y,
+                                         double z, const float4* fs, const double4* s64,
+                                         int slice, int tpt, int ns, int selfj, float del,
+                                         float thr, double del64, double& cx, double& cy,
+                                         double& cz) {
+  for (int j = slice; j < ns; j += tpt)
+    if (j != selfj && r2_32(xt, yt, zt, fs[j], del) < thr) fpair(x, y, z, s64[j], del64, cx, cy, cz);
 }
 
 // Shared-memory layout of one CTA.
@@ -140,7 +224,7 @@ struct Smem {
 // The whole near field of one group.  FORCE: the three field components instead of the
 // potential (Coulomb only).
 template <int KER, bool EPS, bool F32, bool FORCE>
-__global__ void __launch_bounds__(NT) k_near(NearArgs a) {
+__global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a) {
   using P = Prec<F32>;
   using S = typename P::S;
   using T = typename P::T;
@@ -242,30 +326,45 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
       const int selfbase = (node == own) ? (t0 - (j0 + toff)) : INT_MIN;
       const int units = cnt * tpt;
       const int lt = __ffs(tpt) - 1;
+      // close-pair checks are needed only where a target comes within r_t of this leaf's box
+      const float thr = fmaxf((float)c.w * kCloseFrac, kThrMin);  // r_t^2 = sqradius / 1024
+      const float4 hb = a.nodeh[node];
+      const double4* s64 = a.src64 + j0 + toff;
       for (int u0 = 0; u0 < units; u0 += NT) {
         const int u = u0 + tid;
         const bool valid = u < units;
         const int slot = u >> lt, slice = u & (tpt - 1);
         const int i = valid ? tl[slot] : 0;
         const int selfj = selfbase == INT_MIN ? -1 : i + selfbase;
+        // the target's own source in this lane's slice: sum around it
+        const bool self_in = selfj >= 0 && selfj < ns && ((selfj - slice) & (tpt - 1)) == 0;
+        const int je = self_in ? selfj : ns;
         if (!FORCE) {
           T part = 0;
-          if (valid) {
-            if constexpr (F32) {
-              const float4* fs = reinterpret_cast<const float4*>(ts);
-              const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
-                          zt = (float)(cz[t0 + i] - c.z);
+          if constexpr (F32) {
+            const float4* fs = reinterpret_cast<const float4*>(ts);
+            const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
+                        zt = (float)(cz[t0 + i] - c.z);
+            const bool chk = __any_sync(0xffffffffu, valid && box_d2(xt, yt, zt, hb) < thr);
+            if (valid) {
               float p0 = 0.f, p1 = 0.f;
-              int j = slice;
-              for (; j + tpt < ns; j += 2 * tpt) {
-                const float v0 = pair<KER, EPS>(xt, yt, zt, fs[j], del, kl2);
-                const float v1 = pair<KER, EPS>(xt, yt, zt, fs[j + tpt], del, kl2);
-                p0 += (j == selfj) ? 0.f : v0;
-                p1 += (j + tpt == selfj) ? 0.f : v1;
+              bool close = false;
+              if (!chk) {
+                sweep_pot<KER, false>(fs, slice, je, tpt, xt, yt, zt, del, kl2, thr, p0, p1, close);
+                if (self_in)
+                  sweep_pot<KER, false>(fs, selfj + tpt, ns, tpt, xt, yt, zt, del, kl2, thr, p0, p1, close);
+              } else {
+                sweep_pot<KER, true>(fs, slice, je, tpt, xt, yt, zt, del, kl2, thr, p0, p1, close);
+                if (self_in)
+                  sweep_pot<KER, true>(fs, selfj + tpt, ns, tpt, xt, yt, zt, del, kl2, thr, p0, p1, close);
               }
-              if (j < ns && j != selfj) p0 += pair<KER, EPS>(xt, yt, zt, fs[j], del, kl2);
               part = p0 + p1;
-            } else {
+              if (close)
+                part += (float)close_pot<KER, EPS>(xt, yt, zt, cx[t0 + i], cy[t0 + i], cz[t0 + i], fs,
+                                                   s64, slice, tpt, ns, selfj, del, thr, sdel, skappa);
+            }
+          } else {
+            if (valid) {
               const double4* ds = reinterpret_cast<const double4*>(ts);
               double p = 0.0;
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
@@ -273,10 +372,10 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
                 if (j != selfj) p += pair<KER, EPS>(x, y, z, ds[j], sdel, skappa);
               part = p;
             }
-            if (se->self_term && selfj >= 0 && selfj < ns && ((selfj - slice) & (tpt - 1)) == 0) {
-              const int jg = j0 + toff + selfj;  // added, not subtracted (src/tree3d.cpp:3596)
-              selfv[i] = a.src64[jg].w * se->intg / (a.sw ? a.sw[jg] : 1.0);
-            }
+          }
+          if (valid && se->self_term && self_in) {
+            const int jg = j0 + toff + selfj;  // added, not subtracted (src/tree3d.cpp:3596)
+            selfv[i] = a.src64[jg].w * se->intg / (a.sw ? a.sw[jg] : 1.0);
           }
           part = shfl_sum(part, tpt);
           if (valid && slice == 0) {
@@ -285,14 +384,35 @@ __global__ void __launch_bounds__(NT) k_near(NearArgs a) {
           }
         } else {
           T fx = 0, fy = 0, fz = 0;
-          if (valid) {
-            if constexpr (F32) {
-              const float4* fs = reinterpret_cast<const float4*>(ts);
-              const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
-                          zt = (float)(cz[t0 + i] - c.z);
-              for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) fpair(xt, yt, zt, fs[j], del, fx, fy, fz);
-            } else {
+          if constexpr (F32) {
+            const float4* fs = reinterpret_cast<const float4*>(ts);
+            const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
+                        zt = (float)(cz[t0 + i] - c.z);
+            const bool chk = __any_sync(0xffffffffu, valid && box_d2(xt, yt, zt, hb) < thr);
+            if (valid) {
+              bool close = false;
+              if (!chk) {
+                for (int j = slice; j < je; j += tpt)
+                  acc_force<false>(xt, yt, zt, fs[j], del, thr, fx, fy, fz, close);
+                if (self_in)
+                  for (int j = selfj + tpt; j < ns; j += tpt)
+                    acc_force<false>(xt, yt, zt, fs[j], del, thr, fx, fy, fz, close);
+              } else {
+                for (int j = slice; j < je; j += tpt)
+                  acc_force<true>(xt, yt, zt, fs[j], del, thr, fx, fy, fz, close);
+                if (self_in)
+                  for (int j = selfj + tpt; j < ns; j += tpt)
+                    acc_force<true>(xt, yt, zt, fs[j], del, thr, fx, fy, fz, close);
+              }
+              if (close) {
+                double qx = 0.0, qy = 0.0, qz = 0.0;
+                close_force(xt, yt, zt, cx[t0 + i], cy[t0 + i], cz[t0 + i], fs, s64, slice, tpt,
+                            ns, selfj, del, thr, sdel, qx, qy, qz);
+                fx += (float)qx; fy += (float)qy; fz += (float)qz;
+              }
+            }
+          } else {
+            if (valid) {
               const double4* ds = reinterpret_cast<const double4*>(ts);
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
               for (int j = slice; j < ns; j += tpt)
@@ -366,6 +486,7 @@ NearArgs base_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const
   a.nodec = t->nodec.p;
   a.src = P.f32 ? (const void*)t->src32.p : (const void*)t->src64.p;
   a.src64 = t->src64.p;
+  a.nodeh = t->nodeh.p;
   a.sw = t->has_weights ? t->sw.p : nullptr;
   a.sys = P.sys.p;
   a.g_sys = L->g_sys.p;

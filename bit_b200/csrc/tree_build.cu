@@ -524,11 +524,15 @@ __global__ void k_make_children(int a, int b, int nlev, const SplitState* st, co
   for (int c = 0; c < 8; c++) children[8LL * p + c] = c < S->nchild ? base + S->order[c] : -1;
 }
 
-__global__ void k_node_centres(int numtree, const double* fields, double4* nodec) {
+__global__ void k_node_centres(int numtree, const double* fields, double4* nodec, float4* nodeh) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < numtree) {
     const double* f = fields + 13LL * i;
     nodec[i] = make_double4(f[6], f[7], f[8], f[12]);
+    // half extents about the midpoint, rounded up to FP32 (a box the members are inside of)
+    const double hx = fmax(f[1] - f[6], f[6] - f[0]), hy = fmax(f[3] - f[7], f[7] - f[2]),
+                 hz = fmax(f[5] - f[8], f[8] - f[4]);
+    nodeh[i] = make_float4(__double2float_ru(hx), __double2float_ru(hy), __double2float_ru(hz), 0.f);
   }
 }
 
@@ -701,7 +705,8 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
   t->depth = depth;
   t->cap = cap;
   t->nodec.ensure(c, b);
-  count_launch(), k_node_centres<<<grid_for(b, 128), 128, 0, s>>>(b, t->fields.p, t->nodec.p);
+  t->nodeh.ensure(c, b);
+  count_launch(), k_node_centres<<<grid_for(b, 128), 128, 0, s>>>(b, t->fields.p, t->nodec.p, t->nodeh.p);
   tree_sync_host(t);
   // leaves in node order
   std::vector<int> leaves;

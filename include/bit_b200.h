@@ -87,6 +87,7 @@ typedef struct {
   long long far_entries, near_entries, batches;
   int numtree, nleaves, depth, nterms;
   int far_launches, near_launches;
+  int list_fallback; /* the last list build used the count / scan / fill passes */
 } bit_stats;
 
 const char* bit_status_string(bit_status s);
@@ -151,6 +152,22 @@ bit_status bit_treecode_potential(bit_ctx* ctx, int n, const double* x, const do
                                   const double* z, const double* q, const double* w,
                                   int nterms, int maxmemb, const bit_eval_params* prm,
                                   double* pot);
+
+/* FP64 direct sum at m particle targets (indices into the n sources; each target skips
+ * itself by index): shielded_pot_particle_ds (src/tree3d.cpp:1966-2016), -sum q e^{-kappa r}/r,
+ * for BIT_KERNEL_SCREENED; sum q / sqrt(r^2 + del) for BIT_KERNEL_COULOMB; and
+ * sum q e^{-kappa R}/R with R = sqrt(r^2 + del) for BIT_KERNEL_SCREENED_REG, the two
+ * regularised sums skipping r^2 + del <= 1e-14 (src/constants.h:35).  The accuracy
+ * reference of every treecode result.  pot[i] belongs to targets[i].  Host arrays; the
+ * _device variant takes device pointers (an out-of-range device target index is reported
+ * by the next synchronising call). */
+bit_status bit_direct_potential(bit_ctx* ctx, int n, const double* x, const double* y,
+                                const double* z, const double* q, const bit_eval_params* prm,
+                                int m, const int* targets, double* pot);
+bit_status bit_direct_potential_device(bit_ctx* ctx, int n, const double* x, const double* y,
+                                       const double* z, const double* q,
+                                       const bit_eval_params* prm, int m, const int* targets,
+                                       double* pot);
 
 bit_status bit_tree_stats(const bit_tree* tree, bit_stats* st);
 

@@ -160,3 +160,95 @@ def test_whole_pipeline_host_buffers(ctx, orc):
     T = orc.Tree(x, y, z, 500)
     T.compute_moments(q, 7)
     assert rel(pot, T.evaluate(orc.params(orc.COULOMB, orc.MODE_REFERENCE, del_=1e-4, acc=0.5))) < TOL64
+
+
+def test_acc_zero_is_the_direct_sum_through_the_fallback_lists(ctx, orc):
+    """acc = 0 accepts no cluster: every leaf is a near entry of every group, more than a
+    group's staging area holds, so the lists come from the count / scan / fill passes, and
+    the potential is the FP64 direct sum."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(20000, seed=7)
+    t = ctx.treemake(x, y, z, 8)
+    t.treemoments(q, 3)
+    got = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=1e-4, acc=0.0))
+    assert t.stats()["list_fallback"] == 1
+    assert t.stats()["far_pairs"] == 0
+    tg = workloads.sample_targets(20000, 400, seed=2)
+    ds = orc.direct(x, y, z, q, orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=1e-4), tg)
+    assert rel(got[tg], ds) < TOL64
+
+
+def test_lists_past_the_estimated_arena_fall_back_exactly(ctx, orc):
+    """Small leaves and a strict MAC give more near entries than the first build's
+    per-group allowance: the in-place pass runs out of room and the build falls back; the
+    result still matches the oracle, and the next build is sized from this one."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(20000, seed=8)
+    t, T = both(ctx, orc, x, y, z, q, 4, 32)
+    p = B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=1e-4, acc=0.1)
+    got = t.evaluate(p)
+    assert t.stats()["list_fallback"] == 1
+    ref = T.evaluate(orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=1e-4, acc=0.1))
+    assert rel(got, ref) < TOL64
+    # a different MAC rebuilds the lists, sized from the last totals: no fallback
+    got2 = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=1e-4, acc=0.11))
+    assert t.stats()["list_fallback"] == 0
+    ref2 = T.evaluate(orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=1e-4, acc=0.11))
+    assert rel(got2, ref2) < TOL64
+
+
+def planted_close_pairs(n, pairs, seed):
+    """Uniform particles plus `pairs` partners placed 1e-6..1e-4 from existing ones."""
+    rng = np.random.default_rng(seed)
+    p = rng.uniform(0.0, 1.0, (n, 3))
+    src = rng.choice(n, pairs, replace=False)
+    d = rng.standard_normal((pairs, 3))
+    d *= (10.0 ** rng.uniform(-6, -4, pairs) / np.linalg.norm(d, axis=1))[:, None]
+    p = np.concatenate([p, p[src] + d])
+    q = rng.uniform(-1.0, 1.0, len(p))
+    return p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), q
+
+
+@pytest.mark.parametrize("kern", ["screened", "coulomb"])
+def test_mixed_close_pairs_within_tolerance(ctx, kern):
+    """Near-coincident pairs: the FP32 difference of leaf-centred coordinates would lose
+    ~1e-5 relative accuracy; such pairs are summed in FP64, so the mixed path stays within
+    1e-6 of the FP64 path."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = planted_close_pairs(20000, 300, seed=9)
+    t = ctx.treemake(x, y, z, 256)
+    t.treemoments(q, 7)
+    kw = dict(kappa=2.5) if kern == "screened" else dict(del_=1e-14)
+    k = B.SCREENED if kern == "screened" else B.COULOMB
+    p64 = t.evaluate(B.params(k, B.CONSISTENT, B.FP64, acc=0.6, **kw))
+    p32 = t.evaluate(B.params(k, B.CONSISTENT, B.MIXED, acc=0.6, **kw))
+    assert workloads.rel_l2(p32, p64) < TOL_MIXED
+
+
+def test_mixed_force_close_pairs_within_tolerance(ctx):
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = planted_close_pairs(20000, 300, seed=10)
+    t = ctx.treemake(x, y, z, 256)
+    t.treemoments(q, 7)
+    f64 = np.stack(t.treeforce(0.5, 1e-14, B.FP64))
+    f32 = np.stack(t.treeforce(0.5, 1e-14, B.MIXED))
+    assert workloads.rel_l2(f32, f64) < TOL_MIXED
+
+
+def test_mixed_coincident_duplicates_follow_the_fp64_rules(ctx):
+    """Exact duplicates: the Coulomb sum skips r^2 + del <= 1e-14 in both precisions."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(5000, seed=11)
+    x = np.concatenate([x, x[:50]]); y = np.concatenate([y, y[:50]]); z = np.concatenate([z, z[:50]])
+    q = np.concatenate([q, q[:50]])
+    t = ctx.treemake(x, y, z, 64)
+    t.treemoments(q, 5)
+    p64 = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=0.0, acc=0.5))
+    p32 = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.MIXED, del_=0.0, acc=0.5))
+    assert np.all(np.isfinite(p64)) and np.all(np.isfinite(p32))
+    assert workloads.rel_l2(p32, p64) < TOL_MIXED
