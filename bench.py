@@ -251,11 +251,17 @@ def run_bit(args):
     line["roofline"] = {"bound": "fp32", "kernel": "k_near32<SCREENED>",
                         "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
                         "frac": achieved / peak["tflops"], "peak_source": peak["source"],
-                        "traffic": None,
+                        "traffic": profiled_traffic(),
+                        "traffic_unit": "bytes per launch (dram read+write, one ncu pass at full size, "
+                                        "profiles/launches_clustered2M_step.md)",
                         "algorithmic": f"{FLOPS_NEAR['screened']} flops x {pairs} near pairs per launch",
                         "mufu_bound_frac": (2 * pairs / t_near) / peak["mufu_ops"]}
     # accuracy of this step against the FP64 GPU path and the FP64 direct sum (sampled)
-    line["accuracy"] = accuracy(x, y, z, q, res_s, res_c, res64_s, res64_c, args)
+    line["accuracy"] = accuracy(ctx, x, y, z, q, res_s, res_c, res64_s, res64_c, args)
+    if args.bie:
+        line["bie"] = run_bie(ctx, args)
+    if args.batched:
+        line["batched"] = run_batched(ctx, args, dev)
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x, y, z, q, n, args)
     line["gpu_launches"] = launches[B.MIXED] * args.steps
@@ -264,6 +270,149 @@ def run_bit(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_bie(ctx, args):
+    """Boundary-integral GMRES solve: icosphere level 6 (81,920 centroids, weights = areas),
+    (I/2 + K) sigma = f, K the area-weighted screened kernel (kappa = 1) regularised with
+    delta = mean edge length, f = real spherical harmonics of degree <= 8 with seeded
+    N(0,1) coefficients; p = 6, theta = 0.5, N0 = 500, GMRES(50) to 1e-8.  Plain FP64
+    matvecs vs FP32 matvecs inside FP64 iterative refinement; device seconds per solve."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    cen, area, h = workloads.icosphere(args.bie_level)
+    f = workloads.sh_rhs(cen, lmax=8, seed=1)
+    cx, cy, cz = [np.ascontiguousarray(cen[:, a]) for a in range(3)]
+    p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=h * h, kappa=1.0, acc=0.5)
+    t = ctx.treemake(cx, cy, cz, 500)
+    out = {"workload": f"icosphere level {args.bie_level} ({len(cen)} nodes), screened kappa=1 "
+                       f"regularised with delta = mean edge ({h:.4g}), p=6, theta=0.5, N0=500, "
+                       "GMRES(50) to 1e-8", "n": int(len(cen))}
+    tg = workloads.sample_targets(len(cen), 2000, seed=4)
+    for name, prec in (("fp64", B.FP64), ("mixed", B.MIXED)):
+        t.bie_solve(p, 7, 0.5, area, f, restart=50, tol=1e-8, precision=prec)  # warm-up
+        secs, info, sol, st = [], None, None, None
+        for _ in range(args.bie_solves):
+            sol, info, st = t.bie_solve(p, 7, 0.5, area, f, restart=50, tol=1e-8, precision=prec)
+            secs.append(info["seconds"])
+        # residual of the solution against the direct-sum operator on sampled rows
+        Ks = ctx.direct(cx, cy, cz, area * sol, p, tg)
+        res = workloads.rel_l2(0.5 * sol[tg] + Ks, f[tg])
+        out[name] = {"solves_per_s": 1.0 / statistics.median(secs),
+                     "s_per_solve": statistics.median(secs), "status": int(st),
+                     "iterations": info["iterations"], "refinements": info["refinements"],
+                     "matvecs_fp64": info["matvecs_fp64"], "matvecs_fp32": info["matvecs_fp32"],
+                     "relres_treecode": info["relres"], "relres_direct_sum_2000_rows": res}
+    out["mixed_speedup"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    t.treeempty()
+    return out
+
+
+def run_batched(ctx, args, dev):
+    """Batched uneven systems in one pass: 2048 independent systems, N log-uniform in
+    [1e3, 1e5], each uniform in its own unit cube; half regularised Coulomb (delta = 0.01),
+    half screened (kappa ~ U[0.5, 4]); p from {4, 6, 8}; theta = 0.6; N0 per (p, kernel)
+    from the autotuner.  Mixed precision as one forest (build, moments, far and near
+    launches per class) vs a per-system loop of the plain FP64 path; error vs the FP64
+    direct sum on 1,000 sampled targets per system."""
+    import torch
+    import bit_b200 as B
+    from bit_b200 import autotune, workloads
+    systems = workloads.batched_systems(args.batched, seed=3)
+    sizes = np.array([len(s["x"]) for s in systems], dtype=np.int64)
+    med = int(np.median(sizes))
+    n0 = {}
+    for s in systems:
+        key = (s["nterms"], s["kernel"])
+        if key not in n0:
+            n0[key] = autotune.tune_n0(ctx, s["nterms"], s["kernel"], med, acc=0.6,
+                                       del_=1e-4 if s["kernel"] == B.COULOMB else 0.0,
+                                       kappa=2.0)[0]
+    mm = np.array([n0[(s["nterms"], s["kernel"])] for s in systems], dtype=np.int32)
+    nt = np.array([s["nterms"] for s in systems], dtype=np.int32)
+    total = int(sizes.sum())
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    X = torch.tensor(np.stack([np.concatenate([s[k] for s in systems]) for k in "xyzq"]),
+                     dtype=torch.float64, device=dev)
+    out32 = torch.empty(total, dtype=torch.float64, device=dev)
+    out64 = torch.empty(total, dtype=torch.float64, device=dev)
+
+    def prm(s, prec):
+        return B.params(s["kernel"], B.CONSISTENT, prec, del_=s["del_"], kappa=s["kappa"], acc=0.6)
+    p32 = [prm(s, B.MIXED) for s in systems]
+    p64 = [prm(s, B.FP64) for s in systems]
+    ptr = [X[k].data_ptr() for k in range(4)]
+
+    def forest_step():
+        F = ctx.forest_device(sizes, mm, ptr[0], ptr[1], ptr[2])
+        F.set_charges_device(ptr[3])
+        F.moments(nt)
+        F.evaluate_device(p32, out32.data_ptr())
+        st = F.stats()
+        F.treeempty()
+        return st
+
+    def loop_step(prec, out):
+        for i, s in enumerate(systems):
+            o = int(off[i]) * 8
+            t = ctx.treemake_device(int(sizes[i]), ptr[0] + o, ptr[1] + o, ptr[2] + o, int(mm[i]))
+            t.set_charges_device(ptr[3] + o)
+            t.moments(int(nt[i]))
+            t.evaluate_device(prm(s, prec), out.data_ptr() + o)
+            t.treeempty()
+
+    def timed(fn, reps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = None
+        for _ in range(reps):
+            r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e-3, r
+
+    forest_step()  # warm-up
+    t32, st = timed(forest_step, 2)
+    loop_step(B.FP64, out64)  # warm-up
+    t64, _ = timed(lambda: loop_step(B.FP64, out64), 1)
+    r32 = out32.cpu().numpy()
+    r64 = out64.cpu().numpy()
+    e32, e64 = [], []
+    for i, s in enumerate(systems):
+        tg = workloads.sample_targets(int(sizes[i]), 1000, seed=i)
+        ds = ctx.direct(s["x"], s["y"], s["z"], s["q"], p64[i], tg)
+        e32.append(workloads.rel_l2(r32[off[i]:off[i + 1]][tg], ds))
+        e64.append(workloads.rel_l2(r64[off[i]:off[i + 1]][tg], ds))
+    mix_vs_64 = [workloads.rel_l2(r32[off[i]:off[i + 1]], r64[off[i]:off[i + 1]])
+                 for i in range(len(systems))]
+    return {"workload": f"{len(systems)} systems, N log-uniform in [1e3, 1e5] (total {total}), "
+                        "half Coulomb delta=0.01, half screened kappa~U[0.5,4], p in {4,6,8}, "
+                        "theta=0.6, N0 autotuned per (p, kernel)",
+            "systems": len(systems), "particles": total,
+            "n0": {f"nterms{k[0]}_{'coulomb' if k[1] == 0 else 'screened'}": v
+                   for k, v in sorted(n0.items())},
+            "mixed_forest": {"evals_per_s": total / t32, "s_per_step": t32,
+                             "far_launches": st["far_launches"], "near_launches": st["near_launches"]},
+            "fp64_per_system_loop": {"evals_per_s": total / t64, "s_per_step": t64},
+            "speedup": t64 / t32,
+            "error_vs_direct_1000_per_system": {
+                "mixed_median": float(np.median(e32)), "mixed_max": float(np.max(e32)),
+                "fp64_median": float(np.median(e64)), "fp64_max": float(np.max(e64)),
+                "mixed_vs_fp64_max": float(np.max(mix_vs_64))}}
+
+
+def profiled_traffic(key="k_near_screened_f32"):
+    """DRAM bytes per launch of the dominant kernel, from the committed one-pass ncu launch
+    list of this workload (profiles/launches_clustered2M_step.md); None if absent."""
+    path = os.path.join(ROOT, "profiles", "launches_clustered2M_step.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch") and key in line:
+                return int(line.split("=")[1].strip())
+    except OSError:
+        pass
+    return None
 
 
 def fp32_peak_from_clock(clocks):
@@ -275,16 +424,25 @@ def fp32_peak_from_clock(clocks):
                       "MEASURED_PEAKS.json has no CUDA-core FP32 figure"}
 
 
-def accuracy(x, y, z, q, s32, c32, s64, c64, args):
+def accuracy(ctx, x, y, z, q, s32, c32, s64, c64, args):
+    """Relative L2 error against the FP64 direct sum on args.sample seeded targets.  The
+    direct sum runs on the GPU (bit_direct_potential, FP64); it is itself checked against
+    the CPU oracle's direct sum on the first args.oracle_sample of those targets."""
+    import bit_b200 as B
     from bit_b200 import workloads
     from oracle import orc
     tg = workloads.sample_targets(len(x), args.sample, seed=11)
+    ds_s = ctx.direct(x, y, z, q, B.params(B.SCREENED, B.CONSISTENT, B.FP64, kappa=KAPPA), tg)
+    ds_c = ctx.direct(x, y, z, q, B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=DEL), tg)
+    sub = tg[:args.oracle_sample]
     ps = orc.params(orc.SCREENED, orc.MODE_CONSISTENT, kappa=KAPPA, acc=ACC)
     pc = orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=DEL, acc=ACC)
-    ds_s = orc.direct(x, y, z, q, ps, tg)
-    ds_c = orc.direct(x, y, z, q, pc, tg)
+    pin_s = workloads.rel_l2(ds_s[:len(sub)], orc.direct(x, y, z, q, ps, sub))
+    pin_c = workloads.rel_l2(ds_c[:len(sub)], orc.direct(x, y, z, q, pc, sub))
     return {
         "direct_sum_targets": int(len(tg)),
+        "direct_sum": f"FP64 on the GPU; equals the CPU oracle's direct sum on {len(sub)} of "
+                      f"the targets to {max(pin_s, pin_c):.1e} relative",
         "screened": {"mixed_vs_direct": workloads.rel_l2(s32[tg], ds_s),
                      "fp64_vs_direct": workloads.rel_l2(s64[tg], ds_s),
                      "mixed_vs_fp64": workloads.rel_l2(s32, s64)},
@@ -341,7 +499,7 @@ def run_reference(args):
     x, y, z, q = workload(args.n, seed=1)
     times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_time(x, y, z, q, args.n, args.cpu_sample, threads)
+        r = cpu_reference_time(x, y, z, q, args.n, args.ref_sample, threads)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) not present"}))
             return
@@ -357,7 +515,7 @@ def run_reference(args):
                                    "screened kappa=1 + Coulomb delta=0.005", "n": args.n},
             "cpu_baseline": {"value": v, "unit": "evals/s", "cores": threads, "kind": "reference",
                              "sample": f"per step: full tree build + moments, evaluation of "
-                                       f"{args.cpu_sample} seeded targets scaled to all N"},
+                                       f"{args.ref_sample} seeded targets scaled to all N"},
             "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -369,9 +527,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bit", choices=["bit", "reference"])
     ap.add_argument("--n", type=int, default=2_000_000)
-    ap.add_argument("--sample", type=int, default=400, help="direct-sum targets for the error")
-    ap.add_argument("--cpu-sample", type=int, default=2000)
+    ap.add_argument("--sample", type=int, default=10_000, help="direct-sum targets for the error")
+    ap.add_argument("--oracle-sample", type=int, default=100,
+                    help="of those, targets also summed by the CPU oracle")
+    ap.add_argument("--cpu-sample", type=int, default=300_000,
+                    help="targets of the CPU baseline's evaluation sample (about 10 s on 16 cores)")
+    ap.add_argument("--ref-sample", type=int, default=100_000,
+                    help="targets per step of the --impl reference arm")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--bie-level", type=int, default=6, help="icosphere level of the GMRES solve")
+    ap.add_argument("--bie-solves", type=int, default=2)
+    ap.add_argument("--no-bie", dest="bie", action="store_false")
+    ap.add_argument("--batched", type=int, default=2048, help="systems of the batched run (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

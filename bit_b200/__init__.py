@@ -228,6 +228,9 @@ class Context:
         """Independent systems in one tree: system s is the next sizes[s] particles."""
         return Forest(self, x, y, z, sizes, maxmemb)
 
+    def forest_device(self, sizes, maxmemb, xptr, yptr, zptr):
+        return Forest(self, None, None, None, sizes, maxmemb, device=(xptr, yptr, zptr))
+
     def direct(self, x, y, z, q, prm, targets):
         """FP64 direct sum at particle targets (bit_direct_potential)."""
         x, y, z, q = map(_f64, (x, y, z, q))
@@ -390,20 +393,26 @@ class Forest(Tree):
     evaluated with its own parameters and expansion order, and its result equals a
     separate single-system evaluation."""
 
-    def __init__(self, ctx, x, y, z, sizes, maxmemb):
+    def __init__(self, ctx, x, y, z, sizes, maxmemb, device=None):
         self.ctx = ctx
         self.h = _vp()
-        self.x, self.y, self.z = map(_f64, (x, y, z))
         self.sizes = np.ascontiguousarray(sizes, dtype=np.int32)
         self.nsys = len(self.sizes)
         mm = np.broadcast_to(np.asarray(maxmemb, dtype=np.int32), (self.nsys,))
         self.maxmembs = np.ascontiguousarray(mm)
         self.n = int(self.sizes.sum())
-        if self.n != len(self.x):
-            raise ValueError("sizes must add up to the number of particles")
-        st = lib().bit_forest_build(ctx.h, self.nsys, self.sizes.ctypes.data_as(_ip),
-                                    self.maxmembs.ctypes.data_as(_ip), _d(self.x), _d(self.y),
-                                    _d(self.z), C.byref(self.h))
+        if device is None:
+            self.x, self.y, self.z = map(_f64, (x, y, z))
+            if self.n != len(self.x):
+                raise ValueError("sizes must add up to the number of particles")
+            st = lib().bit_forest_build(ctx.h, self.nsys, self.sizes.ctypes.data_as(_ip),
+                                        self.maxmembs.ctypes.data_as(_ip), _d(self.x),
+                                        _d(self.y), _d(self.z), C.byref(self.h))
+        else:
+            xp, yp, zp = device
+            st = lib().bit_forest_build_device(ctx.h, self.nsys, self.sizes.ctypes.data_as(_ip),
+                                               self.maxmembs.ctypes.data_as(_ip), xp, yp, zp,
+                                               C.byref(self.h))
         ctx.check(st, "bit_forest_build")
         ctx._trees.add(self)
         self.maxmemb = int(self.maxmembs.min())
@@ -424,20 +433,28 @@ class Forest(Tree):
     def export_moments(self):
         raise NotImplementedError("forest moments differ in size per system; use export()")
 
-    def evaluate(self, prm, points=None):
-        """prm: one EvalParams for all systems, or a sequence of one per system."""
-        if points is not None:
-            raise ValueError("external points need a single-system tree")
-        arr = (EvalParams * self.nsys)()
+    def _params(self, prm):
         if isinstance(prm, EvalParams):
             prm = [prm] * self.nsys
         if len(prm) != self.nsys:
             raise ValueError("one parameter set per system expected")
+        arr = (EvalParams * self.nsys)()
         for i, p in enumerate(prm):
             arr[i] = p
+        return arr
+
+    def evaluate(self, prm, points=None):
+        """prm: one EvalParams for all systems, or a sequence of one per system."""
+        if points is not None:
+            raise ValueError("external points need a single-system tree")
+        arr = self._params(prm)
         out = np.zeros(self.n)
         self.ctx.check(lib().bit_forest_eval(self.h, arr, _d(out)), "bit_forest_eval")
         return out
+
+    def evaluate_device(self, prm, outptr):
+        arr = prm if isinstance(prm, C.Array) else self._params(prm)
+        self.ctx.check(lib().bit_forest_eval_device(self.h, arr, outptr), "bit_forest_eval_device")
 
     def system(self, s, a):
         """System s's slice of a per-particle array."""
