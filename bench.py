@@ -41,11 +41,6 @@ FLOPS_NEAR = {"screened": 14, "coulomb": 11}     # per near pair (rsqrt, exp cou
 METRIC = "treecode evals/s (clustered N=2M, p=8, theta=0.7, N0=1000, screened+Coulomb)"
 
 
-def rank_info():
-    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
-            int(os.environ.get("LOCAL_RANK", 0)))
-
-
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -109,15 +104,12 @@ def run_bit(args):
     import bit_b200 as B
     from bit_b200 import workloads
 
-    rank, world, local = rank_info()
+    from bit_b200 import replicas
+    rank, world, local = replicas.rank_info()
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dist = replicas.init("nccl")
     n = args.n
-    x, y, z, q = workload(n, seed=1 + rank)
+    x, y, z, q = workload(n, seed=replicas.system_seed(rank))
     dev = torch.device("cuda", local)
     X = torch.tensor(np.stack([x, y, z, q]), dtype=torch.float64, device=dev)
     out_s = torch.empty(n, dtype=torch.float64, device=dev)
@@ -146,8 +138,7 @@ def run_bit(args):
         for _ in range(warmup):
             step(prec)
         torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
+        replicas.barrier(dist)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -158,12 +149,7 @@ def run_bit(args):
         e1.record(stream)
         torch.cuda.synchronize()
         launches[prec] = (B.kernel_launches() - l0) // steps
-        ms = e0.elapsed_time(e1) / steps
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return replicas.max_over_ranks(e0.elapsed_time(e1) / steps, dist, dev)
 
     # mixed precision (the product path): timed with clocks sampled
     with ClockSampler(local) as clk:
@@ -190,23 +176,16 @@ def run_bit(args):
     for _ in range(max(1, args.warmup // 2)):
         e2e_step()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     t0 = time.perf_counter()
     e2e_steps = max(1, args.steps // 2)
     for _ in range(e2e_steps):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-    if dist:
-        tt = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = replicas.max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, dist, dev)
 
     if rank != 0:
-        if dist:
-            dist.barrier()
-            dist.destroy_process_group()
+        replicas.finish(dist)
         return
 
     evals = 2 * n * world
@@ -267,9 +246,7 @@ def run_bit(args):
     line["gpu_launches"] = launches[B.MIXED] * args.steps
     line["gpu_launches_per_step"] = launches[B.MIXED]
     print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(dist)
 
 
 def run_bie(ctx, args):
@@ -492,7 +469,8 @@ def cpu_baseline(x, y, z, q, n, args):
 
 
 def run_reference(args):
-    rank, world, _ = rank_info()
+    from bit_b200 import replicas
+    rank, world, _ = replicas.rank_info()
     if rank != 0:
         return
     threads = os.cpu_count() or 1
