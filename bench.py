@@ -241,6 +241,8 @@ def run_bit(args):
         line["bie"] = run_bie(ctx, args)
     if args.batched:
         line["batched"] = run_batched(ctx, args, dev)
+    if args.serve_requests:
+        line["serving"] = run_serving(ctx, args)
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x, y, z, q, n, args)
     line["gpu_launches"] = launches[B.MIXED] * args.steps
@@ -377,6 +379,119 @@ def run_batched(ctx, args, dev):
                 "mixed_median": float(np.median(e32)), "mixed_max": float(np.max(e32)),
                 "fp64_median": float(np.median(e64)), "fp64_max": float(np.max(e64)),
                 "mixed_vs_fp64_max": float(np.max(mix_vs_64))}}
+
+
+def serving_requests(count, seed, ctx):
+    """The request stream: 70% evaluate requests (N lognormal, median 20,000, clipped to
+    [1e3, 1e6], Gaussian blobs; kernel and parameters as in the batched run) and 30%
+    GMRES solves on icospheres of level 4..7 (system as in the boundary-integral solve)."""
+    import bit_b200 as B
+    from bit_b200 import autotune, workloads
+    rng = np.random.default_rng(seed)
+    spheres = {}
+    reqs = []
+    for i in range(count):
+        if rng.uniform() < 0.7:
+            n = int(np.clip(round(20000 * np.exp(rng.normal(0.0, 1.0))), 1000, 1_000_000))
+            x, y, z, q = workloads.clustered_blobs(n, seed=seed * 100000 + i)
+            coul = rng.uniform() < 0.5
+            nterms = int(rng.choice([4, 6, 8])) + 1
+            kappa = 0.0 if coul else float(rng.uniform(0.5, 4.0))
+            kern = B.COULOMB if coul else B.SCREENED
+            n0 = autotune.tune_n0(ctx, nterms, kern, 20000, acc=0.6, del_=1e-4 if coul else 0.0,
+                                  kappa=2.0, dist="clustered")[0]
+            reqs.append(dict(kind="eval", n=n, data=(x, y, z, q), nterms=nterms, n0=n0,
+                             kernel=kern, del_=1e-4 if coul else 0.0, kappa=kappa))
+        else:
+            level = int(rng.integers(4, 8))
+            if level not in spheres:
+                spheres[level] = workloads.icosphere(level)
+            cen, area, h = spheres[level]
+            f = workloads.sh_rhs(cen, lmax=8, seed=seed * 100000 + i)
+            cx, cy, cz = [np.ascontiguousarray(cen[:, a]) for a in range(3)]
+            reqs.append(dict(kind="solve", n=len(cen), data=(cx, cy, cz, area, f), nterms=7,
+                             n0=500, del_=h * h, level=level))
+    return reqs
+
+
+def serve(reqs, arrivals, prec, slots, budget):
+    """Submit request i at arrivals[i] seconds (open loop) and collect every result."""
+    import threading
+    import bit_b200 as B
+    srv = B.Server(slots=slots, hbm_budget=budget)
+    ids = [None] * len(reqs)
+
+    def producer():
+        t0 = time.perf_counter()
+        for i, r in enumerate(reqs):
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            if r["kind"] == "eval":
+                p = B.params(r["kernel"], B.CONSISTENT, prec, del_=r["del_"], kappa=r["kappa"], acc=0.6)
+                ids[i] = srv.submit_eval(*r["data"], r["nterms"], r["n0"], p)
+            else:
+                p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=r["del_"], kappa=1.0, acc=0.5)
+                x, y, z, w, f = r["data"]
+                ids[i] = srv.submit_solve(x, y, z, w, f, r["nterms"], r["n0"], p, 0.5, restart=50,
+                                          tol=1e-8, precision=prec)
+    th = threading.Thread(target=producer)
+    th.start()
+    th.join()
+    out, infos = [], []
+    for i in range(len(reqs)):
+        res, info, st = srv.wait(ids[i])
+        out.append(res)
+        info["status"] = st
+        infos.append(info)
+    stats = srv.stats()
+    srv.close()
+    lat = np.array([i["t_done"] - i["t_submit"] for i in infos])
+    span = max(i["t_done"] for i in infos) - min(i["t_submit"] for i in infos)
+    return out, {"requests_per_s": len(reqs) / span, "p50_latency_s": float(np.percentile(lat, 50)),
+                 "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
+                 "max_running": stats["max_running"], "slots": slots,
+                 "failed": int(sum(1 for i in infos if i["status"] not in (0,)))}
+
+
+def run_serving(ctx, args):
+    """Serving stream: open-loop Poisson arrivals of the request mix, admitted by a 150 GB
+    HBM budget into a continuous-batching server (mixed precision, several slots), next to
+    the plain FP64 GPU path serving one request at a time on the same arrivals."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    reqs = serving_requests(args.serve_requests, seed=5, ctx=ctx)
+    budget = 150 * 10 ** 9
+    # arrival rate: 1.5x what one mixed slot serves back to back (calibrated on 12 requests)
+    cal, _ = serve(reqs[:12], [0.0] * 12, B.MIXED, 1, budget)
+    _, cal_stats = serve(reqs[:12], [0.0] * 12, B.MIXED, 1, budget)
+    service = 1.0 / cal_stats["requests_per_s"]
+    rate = 1.5 / service
+    rng = np.random.default_rng(6)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+    res32, mixed = serve(reqs, arrivals, B.MIXED, args.serve_slots, budget)
+    res64, plain = serve(reqs, arrivals, B.FP64, 1, budget)
+    # accuracy: mixed vs plain FP64 per request; evaluate requests also vs the direct sum
+    diff = [workloads.rel_l2(a, b) for a, b in zip(res32, res64)]
+    derr = []
+    for i, r in enumerate(reqs):
+        if r["kind"] != "eval":
+            continue
+        x, y, z, q = r["data"]
+        tg = workloads.sample_targets(r["n"], 200, seed=i)
+        p = B.params(r["kernel"], B.CONSISTENT, B.FP64, del_=r["del_"], kappa=r["kappa"])
+        derr.append(workloads.rel_l2(res32[i][tg], ctx.direct(x, y, z, q, p, tg)))
+    kinds = [r["kind"] for r in reqs]
+    return {"workload": f"{len(reqs)} requests, Poisson arrivals at {rate:.1f}/s "
+                        f"({kinds.count('eval')} evaluate: N lognormal median 2e4 in [1e3, 1e6], "
+                        f"blobs, p in {{4,6,8}}, theta 0.6; {kinds.count('solve')} solves: "
+                        "icosphere level 4..7, p=6, theta=0.5, GMRES(50) to 1e-8), 150 GB budget",
+            "mixed_continuous_batching": mixed, "fp64_one_at_a_time": plain,
+            "throughput_ratio": mixed["requests_per_s"] / plain["requests_per_s"],
+            "p99_ratio": plain["p99_latency_s"] / mixed["p99_latency_s"],
+            "mixed_vs_fp64_max": float(max(diff)),
+            "eval_error_vs_direct_200_targets": {"median": float(np.median(derr)),
+                                                 "max": float(np.max(derr))}}
 
 
 def profiled_traffic(key="k_near_screened_f32"):
@@ -517,6 +632,9 @@ def main():
     ap.add_argument("--bie-solves", type=int, default=2)
     ap.add_argument("--no-bie", dest="bie", action="store_false")
     ap.add_argument("--batched", type=int, default=2048, help="systems of the batched run (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=120,
+                    help="requests of the serving stream (0: skip)")
+    ap.add_argument("--serve-slots", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -78,6 +78,32 @@ class GmresInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("device", C.c_int), ("slots", C.c_int), ("hbm_budget", C.c_size_t)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("slot", C.c_int), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_done", C.c_double),
+                ("bytes_reserved", C.c_size_t), ("peak_bytes", C.c_size_t),
+                ("gmres", GmresInfo)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "gmres"}
+        d["gmres"] = self.gmres.as_dict()
+        return d
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("queued", C.c_longlong), ("running", C.c_int), ("max_running", C.c_int),
+                ("slots", C.c_int), ("budget", C.c_size_t), ("reserved", C.c_size_t),
+                ("max_reserved", C.c_size_t), ("now", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _vp = C.c_void_p
@@ -125,6 +151,17 @@ SIGNATURES = [
                                        C.c_int, _ip, _dp]),
     ("bit_direct_potential_device", C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp,
                                               C.POINTER(EvalParams), C.c_int, _vp, _vp]),
+    ("bit_server_create", C.c_int, [C.POINTER(_vp), C.POINTER(ServerOpts)]),
+    ("bit_server_destroy", C.c_int, [_vp]),
+    ("bit_server_submit_eval", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, C.c_int, C.c_int,
+                                         C.POINTER(EvalParams), C.POINTER(C.c_longlong)]),
+    ("bit_server_submit_solve", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int,
+                                          C.c_int, C.POINTER(EvalParams), C.c_double,
+                                          C.POINTER(GmresOpts), C.POINTER(C.c_longlong)]),
+    ("bit_server_wait", C.c_int, [_vp, C.c_longlong, _dp, C.POINTER(RequestInfo)]),
+    ("bit_server_poll", C.c_int, [_vp, C.c_longlong, _ip]),
+    ("bit_server_stats", C.c_int, [_vp, C.POINTER(ServerInfo)]),
+    ("bit_server_last_error", C.c_char_p, [_vp]),
     ("bit_gmres_dense_static", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip, C.c_char_p,
                                          C.c_int]),
 ]
@@ -459,3 +496,70 @@ class Forest(Tree):
     def system(self, s, a):
         """System s's slice of a per-particle array."""
         return a[self.offsets[s]:self.offsets[s + 1]]
+
+
+class Server:
+    """Request loop with continuous batching (bit_server_*): evaluate and solve requests
+    of any size, admitted as slots and HBM budget free up, overlapping on the device."""
+
+    def __init__(self, device=0, slots=4, hbm_budget=0):
+        self.h = _vp()
+        self.sizes = {}
+        opts = ServerOpts(device, slots, hbm_budget)
+        st = lib().bit_server_create(C.byref(self.h), C.byref(opts))
+        if st:
+            raise BitError(st, "bit_server_create")
+
+    def _check(self, st, what):
+        if st:
+            msg = lib().bit_server_last_error(self.h)
+            raise BitError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def submit_eval(self, x, y, z, q, nterms, maxmemb, prm):
+        x, y, z, q = map(_f64, (x, y, z, q))
+        rid = C.c_longlong()
+        self._check(lib().bit_server_submit_eval(self.h, len(x), _d(x), _d(y), _d(z), _d(q),
+                                                 nterms, maxmemb, C.byref(prm), C.byref(rid)),
+                    "bit_server_submit_eval")
+        self.sizes[rid.value] = len(x)
+        return rid.value
+
+    def submit_solve(self, x, y, z, w, f, nterms, maxmemb, prm, diag, restart=50, tol=1e-8,
+                     maxit=1000, precision=FP64, inner_tol=0.0, max_refinements=0):
+        x, y, z, w, f = map(_f64, (x, y, z, w, f))
+        rid = C.c_longlong()
+        opts = GmresOpts(restart, maxit, tol, precision, inner_tol, max_refinements)
+        self._check(lib().bit_server_submit_solve(self.h, len(x), _d(x), _d(y), _d(z), _d(w),
+                                                  _d(f), nterms, maxmemb, C.byref(prm), diag,
+                                                  C.byref(opts), C.byref(rid)),
+                    "bit_server_submit_solve")
+        self.sizes[rid.value] = len(x)
+        return rid.value
+
+    def wait(self, rid):
+        """(result, info dict, status) of a request; blocks until it is done."""
+        out = np.zeros(self.sizes.pop(rid))
+        info = RequestInfo()
+        st = lib().bit_server_wait(self.h, rid, _d(out), C.byref(info))
+        return out, info.as_dict(), st
+
+    def done(self, rid):
+        d = C.c_int()
+        self._check(lib().bit_server_poll(self.h, rid, C.byref(d)), "bit_server_poll")
+        return bool(d.value)
+
+    def stats(self):
+        si = ServerInfo()
+        self._check(lib().bit_server_stats(self.h, C.byref(si)), "bit_server_stats")
+        return si.as_dict()
+
+    def close(self):
+        if self.h:
+            lib().bit_server_destroy(self.h)
+            self.h = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

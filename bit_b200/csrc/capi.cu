@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <set>
 #include <numeric>
 #include <vector>
 
@@ -26,6 +28,19 @@ static void release_cache(Ctx* c) {
   for (auto& kv : c->cache) cudaFree(kv.second);
   c->cache.clear();
   c->cached = 0;
+}
+
+void ctx_trim(Ctx* c, size_t keep) {
+  if (c->in_use + c->cached <= keep) return;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  // largest blocks first
+  while (!c->cache.empty() && c->in_use + c->cached > keep) {
+    auto it = std::prev(c->cache.end());
+    cudaFree(it->second);
+    c->cached -= it->first;
+    c->cache.erase(it);
+  }
 }
 
 void* dev_alloc(Ctx* c, size_t bytes) {
@@ -797,10 +812,22 @@ bit_status bit_tree_target_lists(bit_tree* th, const bit_eval_params* prm, int p
 }  // extern "C"
 
 namespace bit {
-long long& launch_counter() {
-  static long long n = 0;
+std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> n{0};
   return n;
+}
+
+void ensure_smem_attr(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  BIT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(kernel, dev);
+  if (done.count(key)) return;
+  BIT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.insert(key);
 }
 }  // namespace bit
 
-extern "C" long long bit_kernel_launches(void) { return bit::launch_counter(); }
+extern "C" long long bit_kernel_launches(void) { return bit::launch_counter().load(); }

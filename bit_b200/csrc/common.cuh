@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <map>
 #include <string>
 #include <vector>
@@ -39,15 +40,22 @@ struct Error {
 
 inline void fail(bit_status c, const std::string& m) { throw Error{c, m}; }
 
-// Kernels launched by this library in this process (every launch site counts itself).
-long long& launch_counter();
-inline void count_launch() { ++launch_counter(); }
+// Kernels launched by this library in this process (every launch site counts itself;
+// several host threads may launch at once).
+std::atomic<long long>& launch_counter();
+inline void count_launch() { launch_counter().fetch_add(1, std::memory_order_relaxed); }
+
+// Set a kernel's dynamic shared-memory limit once per (kernel, current device); safe to
+// call from several host threads.
+void ensure_smem_attr(const void* kernel, int bytes);
 
 // ---- device memory with budget accounting ------------------------------------------
 struct Ctx;
 struct Tree;
 void* dev_alloc(Ctx* c, size_t bytes);
 void dev_free(Ctx* c, void* p);
+// Free cached (unused) blocks until live + cached bytes are at most `keep`.
+void ctx_trim(Ctx* c, size_t keep);
 
 template <class T>
 struct DBuf {

@@ -9,9 +9,6 @@
 // shared-memory row; rows are summed in warp order at the end, so the result does not
 // depend on timing.  The target-centre offset is formed in FP64; the mixed path rounds it
 // once to FP32 and runs recurrence and dot product in FP32, accumulating with two-sum.
-#include <set>
-#include <utility>
-
 #include "common.cuh"
 
 namespace bit {
@@ -234,14 +231,7 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
 
 template <class K>
 void set_smem(K kernel, size_t bytes) {
-  // once per (kernel, device)
-  static std::set<std::pair<const void*, int>> done;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
-  if (done.count(key)) return;
-  BIT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-  done.insert(key);
+  ensure_smem_attr(reinterpret_cast<const void*>(kernel), (int)bytes);
 }
 
 template <int NT, int KER, class T>

@@ -222,13 +222,7 @@ __global__ void k_scan_cnt(const int* in, const int* tcount, long long* out, int
 }
 
 void set_stage_attr() {
-  static std::vector<int> done;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (std::find(done.begin(), done.end(), dev) != done.end()) return;
-  BIT_CUDA(cudaFuncSetAttribute(k_lists<MODE_STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)STAGE_BYTES));
-  done.push_back(dev);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_STAGE>), (int)STAGE_BYTES);
 }
 
 }  // namespace

@@ -458,14 +458,7 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
 template <int KER, bool EPS, bool F32, bool FORCE>
 void launch(const NearArgs& a, int ngroups, cudaStream_t s) {
   constexpr size_t bytes = Smem<F32, FORCE>::total;
-  static int done[64] = {0};  // once per kernel and device
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !done[dev]) {
-    BIT_CUDA(cudaFuncSetAttribute(k_near<KER, EPS, F32, FORCE>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    done[dev] = 1;
-  }
+  ensure_smem_attr(reinterpret_cast<const void*>(k_near<KER, EPS, F32, FORCE>), (int)bytes);
   count_launch(), k_near<KER, EPS, F32, FORCE><<<ngroups, NT, bytes, s>>>(a);
 }
 

@@ -226,6 +226,62 @@ typedef struct {
   double seconds;  /* device time of the solve                      */
 } bit_gmres_info;
 
+/* ---------------------------------------------------------------------------------
+ * Serving (no reference counterpart: the reference has no request layer).
+ * A server owns `slots` contexts on one device, each with its own stream, and a FIFO of
+ * evaluate and solve requests.  A request starts when a slot is free and its estimated
+ * device memory fits in what running requests leave of the HBM budget (the head of the
+ * queue is never overtaken); requests in different slots overlap on the device.  Inputs
+ * are copied at submission; results are identical to the single-request calls
+ * (bit_treecode_potential, bit_bie_solve) whatever else runs.  The functions are safe to
+ * call from several host threads.
+ * ------------------------------------------------------------------------------- */
+typedef struct bit_server bit_server;
+
+typedef struct {
+  int device;
+  int slots;          /* requests on the device at once (1..64)                  */
+  size_t hbm_budget;  /* bytes the running requests may hold (0: 90% of free)     */
+} bit_server_opts;
+
+typedef struct {
+  bit_status status;
+  int slot;
+  double t_submit, t_start, t_done;  /* seconds on the server's clock          */
+  size_t bytes_reserved;             /* admission estimate                      */
+  size_t peak_bytes;                 /* device memory the request's slot peaked at */
+  bit_gmres_info gmres;              /* solve requests                          */
+} bit_request_info;
+
+typedef struct {
+  long long submitted, completed, queued;
+  int running, max_running, slots;
+  size_t budget, reserved, max_reserved;
+  double now;  /* seconds since the server was created */
+} bit_server_info;
+
+bit_status bit_server_create(bit_server** server, const bit_server_opts* opts);
+/* Finishes every submitted request, then releases the device. */
+bit_status bit_server_destroy(bit_server* server);
+/* Potential at every particle (treemake + treemoments + treepotential /
+ * shielded_treepot for all p); returns the request id.  BIT_ERR_BUDGET if the request
+ * alone exceeds the budget. */
+bit_status bit_server_submit_eval(bit_server* server, int n, const double* x, const double* y,
+                                  const double* z, const double* q, int nterms, int maxmemb,
+                                  const bit_eval_params* prm, long long* id);
+/* (diag*I + K) s = f with weights w, as bit_bie_solve. */
+bit_status bit_server_submit_solve(bit_server* server, int n, const double* x, const double* y,
+                                   const double* z, const double* w, const double* f,
+                                   int nterms, int maxmemb, const bit_eval_params* prm,
+                                   double diag, const bit_gmres_opts* opts, long long* id);
+/* Block until the request is done; out gets its n results (original order).  Returns the
+ * request's status.  Each id can be waited for once. */
+bit_status bit_server_wait(bit_server* server, long long id, double* out,
+                           bit_request_info* info);
+bit_status bit_server_poll(bit_server* server, long long id, int* done);
+bit_status bit_server_stats(bit_server* server, bit_server_info* info);
+const char* bit_server_last_error(const bit_server* server);
+
 bit_status bit_bie_solve(bit_tree* tree, const bit_eval_params* prm, int nterms, double diag,
                          const double* w, const double* f, double* s,
                          const bit_gmres_opts* opts, bit_gmres_info* info);
