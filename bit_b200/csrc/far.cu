@@ -110,7 +110,7 @@ constexpr int NWP = 8;  // warps per CTA, potential
 constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
 
 template <int NT, int KER, class T>
-__global__ void __launch_bounds__(32 * NWP) k_far(FarArgs a) {
+__global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArgs a) {
   constexpr int TT = num_terms(NT);
   constexpr int TP = FarField<NT>::kPadded;
   constexpr int NW = NWP;

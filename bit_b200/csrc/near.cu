@@ -2,9 +2,9 @@
 // (src/tree3d.cpp:4737-4774, 3539-3623, 923-967), one CTA per target group.
 //
 // For each near entry (source leaf, bitmask over the group's targets) the CTA packs the
-// targets that need the leaf into a dense list, and when fewer than half the threads
-// would be busy it splits the leaf's sources across 2..32 threads per target (partial
-// sums combined by warp shuffles).  Source tiles are staged in shared memory by TMA bulk
+// targets that need the leaf into a dense list and splits the leaf's sources across 1..32
+// threads per target, whichever keeps the most threads busy (partial sums combined by
+// warp shuffles).  Source tiles are staged in shared memory by TMA bulk
 // copies (cp.async.bulk with an mbarrier), double buffered so the next tile streams in
 // while the current one is consumed; every thread then reads each source from shared
 // memory, broadcast across the targets.  Accumulation per target is in shared memory in a
@@ -205,6 +205,32 @@ __device__ __forceinline__ void close_force(float xt, float yt, float zt, double
     if (j != selfj && r2_32(xt, yt, zt, fs[j], del) < thr) fpair(x, y, z, s64[j], del64, cx, cy, cz);
 }
 
+// Threads per target for an entry with cnt targets.  For pairs with costly arithmetic
+// (MUFU exp, FP64): the power of two (1..32) that keeps the most of the CTA's threads busy
+// over the rounds of NT units (a larger split must win by 4% to be taken, since it adds a
+// shuffle reduction and shortens each thread's run).  For the cheap FP32 Coulomb pair the
+// per-unit overhead weighs more: split only until half the threads are busy.
+template <bool CHEAP>
+__device__ __forceinline__ int split_for(int cnt) {
+  if (CHEAP) {
+    int tpt = 1;
+    while (tpt < 32 && cnt * tpt * 2 <= NT) tpt <<= 1;
+    return tpt;
+  }
+  int best = 1;
+  float bu = 0.f;
+  for (int tp = 1; tp <= 32; tp <<= 1) {
+    const int units = cnt * tp;
+    const int rounds = (units + NT - 1) / NT;
+    const float util = (float)units / (float)(rounds * NT);
+    if (util > bu + 0.04f) {
+      bu = util;
+      best = tp;
+    }
+  }
+  return best;
+}
+
 // Shared-memory layout of one CTA.
 template <bool F32, bool FORCE>
 struct Smem {
@@ -312,8 +338,7 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
       __syncthreads();
       if (toff == 0) {
         cnt = s_cnt;
-        tpt = 1;
-        while (tpt < 32 && cnt * tpt * 2 <= NT) tpt <<= 1;
+        tpt = split_for<F32 && KER == BIT_KERNEL_COULOMB && !FORCE>(cnt);
       }
       if (!mbar_wait(&bar[buf], (k >> 1) & 1)) {
         if (tid == 0) atomicOr(a.err, 2);
