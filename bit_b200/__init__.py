@@ -104,6 +104,21 @@ class ServerInfo(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PicOpts(C.Structure):
+    _fields_ = [("steps", C.c_int), ("nterms", C.c_int), ("maxmemb", C.c_int), ("dt", C.c_double),
+                ("del_", C.c_double), ("acc", C.c_double), ("charge_constant", C.c_double),
+                ("invmass", C.c_double), ("precision", C.c_int)]
+
+
+class Panel(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("x0", "x1", "y0", "y1", "z0", "z1", "str", "xnrm",
+                                          "ynrm", "znrm", "refpot", "midx", "midy", "midz")] + \
+               [("type", C.c_int), ("orientation", C.c_int), ("area", C.c_double)]
+
+    FIELDS = ("x0", "x1", "y0", "y1", "z0", "z1", "str", "xnrm", "ynrm", "znrm", "refpot",
+              "midx", "midy", "midz", "type", "orientation", "area")
+
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _vp = C.c_void_p
@@ -162,6 +177,14 @@ SIGNATURES = [
     ("bit_server_poll", C.c_int, [_vp, C.c_longlong, _ip]),
     ("bit_server_stats", C.c_int, [_vp, C.POINTER(ServerInfo)]),
     ("bit_server_last_error", C.c_char_p, [_vp]),
+    ("bit_pic_steps", C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                C.POINTER(PicOpts), _vp, _vp, _vp]),
+    ("bit_panels_box", C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                 C.POINTER(Panel), _ip]),
+    ("bit_panel_matrix", C.c_int, [_vp, C.c_int, C.POINTER(Panel), C.c_double, _dp]),
+    ("bit_panel_solve", C.c_int, [_vp, C.c_int, C.POINTER(Panel), C.c_int, _dp, _dp, _dp, _dp,
+                                  C.c_double, C.c_int, C.c_double, C.c_int,
+                                  C.POINTER(GmresOpts), C.POINTER(GmresInfo)]),
     ("bit_gmres_dense_static", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip, C.c_char_p,
                                          C.c_int]),
 ]
@@ -190,6 +213,22 @@ def _d(a):
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def panels_box(xpanels, ypanels, zpanels, dlength, dheight, ddepth):
+    """setboundaries: a ctypes array of Panel (and .as_array(): (numpan, 17) floats)."""
+    n = C.c_int()
+    st = lib().bit_panels_box(xpanels, ypanels, zpanels, dlength, dheight, ddepth, None,
+                              C.byref(n))
+    if st:
+        raise BitError(st, "bit_panels_box")
+    arr = (Panel * n.value)()
+    lib().bit_panels_box(xpanels, ypanels, zpanels, dlength, dheight, ddepth, arr, C.byref(n))
+    return arr
+
+
+def panels_as_array(pan):
+    return np.array([[getattr(p, k) for k in Panel.FIELDS] for p in pan], dtype=np.float64)
 
 
 def kernel_launches():
@@ -281,6 +320,29 @@ class Context:
     def direct_device(self, n, xp, yp, zp, qp, prm, m, tgp, outp):
         self.check(lib().bit_direct_potential_device(self.h, n, xp, yp, zp, qp, C.byref(prm), m,
                                                      tgp, outp), "bit_direct_potential_device")
+
+    def pic_steps_device(self, n, ptrs, qptr, opts, fptrs=(None, None, None)):
+        """bit_pic_steps on device arrays: ptrs = (x, y, z, u, v, w) updated in place."""
+        self.check(lib().bit_pic_steps(self.h, n, *ptrs, qptr, C.byref(opts), *fptrs),
+                   "bit_pic_steps")
+
+    def panel_matrix(self, pan, del_):
+        n = len(pan)
+        A = np.zeros(n * n)
+        self.check(lib().bit_panel_matrix(self.h, n, pan, del_, _d(A)), "bit_panel_matrix")
+        return A.reshape(n, n)
+
+    def panel_solve(self, pan, x, y, z, q, del_, nterms, acc, maxmemb, restart=50, tol=1e-10,
+                    maxit=1000):
+        """Sets pan[i].str; returns (sigma, info, status)."""
+        x, y, z, q = map(_f64, (x, y, z, q))
+        opts = GmresOpts(restart, maxit, tol, FP64, 0.0, 0)
+        info = GmresInfo()
+        st = lib().bit_panel_solve(self.h, len(pan), pan, len(x), _d(x), _d(y), _d(z), _d(q),
+                                   del_, nterms, acc, maxmemb, C.byref(opts), C.byref(info))
+        if st not in (0, 7):
+            self.check(st, "bit_panel_solve")
+        return np.array([p.str for p in pan]), info.as_dict(), st
 
     def gmres_dense(self, A, b, x0=None):
         """solver::gmres (src/solver.h:157) on the device."""

@@ -659,6 +659,82 @@ bit_status bit_eval_force(bit_tree* th, double del, double acc, bit_precision pr
   });
 }
 
+namespace bit {
+namespace {
+// After the field of step k (tree order): the reference's force scaling and explicit
+// update, particle by particle in original order, without contraction so the arithmetic
+// is the reference's (src/tree3d.cpp:2330-2332, 4846-4848, 4884-4886):
+//   F = f * charge_constant * q;  u += dt * F * invmass;  x += dt * u
+__global__ void k_pic_update(int n, const int* perm, const double* fxs, const double* fys,
+                             const double* fzs, const double* q, double cc, double invmass,
+                             double dt, double* x, double* y, double* z, double* u, double* v,
+                             double* w, double* fx_out, double* fy_out, double* fz_out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int j = perm[e];
+  const double qj = q[j];
+  const double Fx = dmul(dmul(fxs[e], cc), qj), Fy = dmul(dmul(fys[e], cc), qj),
+               Fz = dmul(dmul(fzs[e], cc), qj);
+  if (fx_out) { fx_out[j] = Fx; fy_out[j] = Fy; fz_out[j] = Fz; }
+  const double uj = dadd(u[j], dmul(dmul(dt, Fx), invmass));
+  const double vj = dadd(v[j], dmul(dmul(dt, Fy), invmass));
+  const double wj = dadd(w[j], dmul(dmul(dt, Fz), invmass));
+  u[j] = uj; v[j] = vj; w[j] = wj;
+  x[j] = dadd(x[j], dmul(dt, uj));
+  y[j] = dadd(y[j], dmul(dt, vj));
+  z[j] = dadd(z[j], dmul(dt, wj));
+}
+}  // namespace
+}  // namespace bit
+
+bit_status bit_pic_steps(bit_ctx* h, int n, double* x, double* y, double* z, double* u,
+                         double* v, double* w, const double* q, const bit_pic_opts* o,
+                         double* fx, double* fy, double* fz) {
+  if (!h || !x || !y || !z || !u || !v || !w || !q || !o || n < 1) return BIT_ERR_INVALID_ARGUMENT;
+  if ((fx || fy || fz) && !(fx && fy && fz)) return BIT_ERR_INVALID_ARGUMENT;
+  Ctx* c = &h->c;
+  if (o->steps < 0 || o->maxmemb < 1 || o->nterms < 1 || o->nterms > kNtermsMax) {
+    c->last_error = "steps >= 0, maxmemb >= 1 and 1 <= nterms <= BIT_NTERMS_MAX required";
+    return BIT_ERR_INVALID_ARGUMENT;
+  }
+  for (int k = 0; k < o->steps; k++) {
+    bit_tree* th = nullptr;
+    bit_status st = bit_tree_build_device(h, n, x, y, z, o->maxmemb, &th);
+    if (st == BIT_OK) st = bit_tree_set_charges_device(th, q, nullptr);
+    if (st == BIT_OK) st = bit_tree_moments(th, o->nterms);
+    if (st == BIT_OK) {
+      Tree* t = &th->t;
+      st = guard(c, [&] {
+        bit_eval_params p{};
+        p.kernel = BIT_KERNEL_COULOMB;
+        p.del = o->del;
+        p.acc = o->acc;
+        p.precision = o->precision;
+        prepare_particles(t, {p}, 1);
+        t->fx_sorted.ensure(c, n); t->fy_sorted.ensure(c, n); t->fz_sorted.ensure(c, n);
+        eval_far_force(t, &t->plists, t->pplan, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
+        eval_near_force(t, &t->plists, t->pplan, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p);
+        const bool last = k == o->steps - 1;
+        count_launch(), k_pic_update<<<grid_for(n, 256), 256, 0, c->stream>>>(
+            n, t->perm.p, t->fx_sorted.p, t->fy_sorted.p, t->fz_sorted.p, q, o->charge_constant,
+            o->invmass, o->dt, x, y, z, u, v, w, last ? fx : nullptr, last ? fy : nullptr,
+            last ? fz : nullptr);
+        BIT_CHECK_LAUNCH();
+      });
+    }
+    if (th) {
+      std::string keep = c->last_error;
+      bit_tree_destroy(th);
+      c->last_error = keep;
+    }
+    if (st != BIT_OK) return st;
+  }
+  return guard(c, [&] {
+    BIT_CUDA(cudaStreamSynchronize(c->stream));
+    check_dev_err(c);
+  });
+}
+
 bit_status bit_treecode_potential(bit_ctx* h, int n, const double* x, const double* y,
                                   const double* z, const double* q, const double* w, int nterms,
                                   int maxmemb, const bit_eval_params* prm, double* pot) {

@@ -252,6 +252,26 @@ void freespace_particles_tree(int npart, PARTICLE* part, int nterms, double acc,
   treeempty(numtree, tree);
 }
 
+// vel_update / loc_update (src/tree3d.cpp:4842-4888): host loops over the caller's
+// particle array, as in the reference (bit_pic_steps is the device-resident loop).
+int vel_update(int npart, PARTICLE* part, double dt) {
+  for (int i = 0; i < npart; i++) {
+    part[i].u += dt * part[i].xforce * invmass;
+    part[i].v += dt * part[i].yforce * invmass;
+    part[i].w += dt * part[i].zforce * invmass;
+  }
+  return 0;
+}
+
+int loc_update(int npart, PARTICLE* part, double dt) {
+  for (int i = 0; i < npart; i++) {
+    part[i].x += dt * part[i].u;
+    part[i].y += dt * part[i].v;
+    part[i].z += dt * part[i].w;
+  }
+  return 0;
+}
+
 // solver::gmres (src/solver.h:157-260) on the device
 int solver::gmres(double** a, double* b, double* x, int num) {
   std::lock_guard<std::mutex> lk(mu);

@@ -146,6 +146,22 @@ bit_status bit_eval_points(bit_tree* tree, const bit_eval_params* prm, int m,
 bit_status bit_eval_force(bit_tree* tree, double del, double acc, bit_precision prec,
                           double* fx, double* fy, double* fz);
 
+/* Time stepping of the reference's particle loop, device-resident: every step rebuilds
+ * the tree from the current positions and runs freespace_particles_tree
+ * (src/tree3d.cpp:2268-2335: treemake, treemoments, treeforce, F = field * charge_constant
+ * * q), then vel_update (:4842-4850, u += dt F invmass) and loc_update (:4880-4888,
+ * x += dt u).  x..w are device arrays in original order, updated in place; fx, fy, fz
+ * (device, may all be NULL) receive F of the last step. */
+typedef struct {
+  int steps, nterms, maxmemb;
+  double dt, del, acc;
+  double charge_constant, invmass; /* src/constants.h:22 / :30 and :19 / :29 */
+  bit_precision precision;
+} bit_pic_opts;
+bit_status bit_pic_steps(bit_ctx* ctx, int n, double* x, double* y, double* z, double* u,
+                         double* v, double* w, const double* q, const bit_pic_opts* opts,
+                         double* fx, double* fy, double* fz);
+
 /* Whole pipeline through host buffers, the analogue of treemake + treemoments + a loop of
  * treepotential / shielded_treepot over all particles (tests/treecode_mp.cpp:57-95). */
 bit_status bit_treecode_potential(bit_ctx* ctx, int n, const double* x, const double* y,
@@ -225,6 +241,38 @@ typedef struct {
   double relres;   /* final true relative residual in FP64          */
   double seconds;  /* device time of the solve                      */
 } bit_gmres_info;
+
+/* ---------------------------------------------------------------------------------
+ * Boundary panels (PANEL, src/tree3d.h:77-95) and the panel solve.
+ * ------------------------------------------------------------------------------- */
+typedef struct {
+  double x0, x1, y0, y1, z0, z1;
+  double str;                /* panel strength sigma (set by bit_panel_solve) */
+  double xnrm, ynrm, znrm;
+  double refpot;             /* Dirichlet value                                */
+  double midx, midy, midz;   /* quadrature point                               */
+  int type;                  /* 0: Dirichlet                                   */
+  int orientation;           /* 1: xy, 2: xz, 3: yz                            */
+  double area;
+} bit_panel;
+
+/* setboundaries (src/tree3d.cpp:3764-3934): the faces of a dlength x dheight x ddepth box
+ * centred at the origin, in the reference's panel order.  *numpan gets
+ * 2 (xp yp + zp yp + xp zp); pan (that many entries) may be NULL to ask for the count. */
+bit_status bit_panels_box(int xpanels, int ypanels, int zpanels, double dlength,
+                          double dheight, double ddepth, bit_panel* pan, int* numpan);
+/* panelconstantsreal (src/tree3d.cpp:4054-4078) on the device, bit-exact:
+ * A[i*n + j] = -1 / sqrt(|mid_i - mid_j|^2 + del) / 2 * inv2pi * area_j. */
+bit_status bit_panel_matrix(bit_ctx* ctx, int n, const bit_panel* pan, double del, double* A);
+/* The panel solve the reference left commented out (panel_solve_tree,
+ * src/tree3d.cpp:4351-4438) on the treecode: b_i = refpot_i + 0.5 sum_j q_j / r_ij over the
+ * np particles (FP64 direct sum), then A sigma = b for A as in bit_panel_matrix, solved as
+ * (I/sqrt(del) + K) (area sigma) = -4 pi b with the regularised Coulomb treecode K over
+ * the panel midpoints (nterms, acc, maxmemb) and GMRES(m) (opts).  Sets pan[i].str. */
+bit_status bit_panel_solve(bit_ctx* ctx, int npan, bit_panel* pan, int np, const double* x,
+                           const double* y, const double* z, const double* q, double del,
+                           int nterms, double acc, int maxmemb, const bit_gmres_opts* opts,
+                           bit_gmres_info* info);
 
 /* ---------------------------------------------------------------------------------
  * Serving (no reference counterpart: the reference has no request layer).

@@ -34,6 +34,7 @@ const double inv2pi = 0.5 / pi;
 const double perm = 8.85418781762e-12;
 const double elec = 1.60217733e-19;
 const double charge_constant = inv2pi / perm;
+const double invmass = 1.0 / 9.1093897e-31; /* src/constants.h:19 */
 const double eps = 1e-14;
 
 /* src/tree3d.h:33-47 */
@@ -78,6 +79,9 @@ double treeforce(int ind, int p, int nterms, double x, double y, double z, doubl
                  double* xfor, double* yfor, double* zfor, TREE* tree, PARTICLE* part);
 void freespace_particles_tree(int npart, PARTICLE* part, int nterms, double acc, TREE* tree,
                               int numtree, int maxmemb);
+/* src/tree3d.cpp:4842-4850 and :4880-4888: explicit velocity and position updates */
+int vel_update(int npart, PARTICLE* part, double dt);
+int loc_update(int npart, PARTICLE* part, double dt);
 
 /* src/solver.h:31-315: dense GMRES, on the device */
 class solver {

@@ -60,6 +60,9 @@ def lib(del_=0.01):
         L.ref_eval_grad_kernel.argtypes = [C.c_double] * 4 + [C.c_int, _dp]
         L.ref_gmres_dense.restype = C.c_int
         L.ref_gmres_dense.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.ref_setboundaries.restype = C.c_int
+        L.ref_setboundaries.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp]
+        L.ref_panelconstantsreal.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp]
         _libs[del_] = L
     return _libs[del_]
 
@@ -189,3 +192,18 @@ def gmres_dense(A, b, x0=None):
     x = np.ones(len(b)) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
     lib(0.01).ref_gmres_dense(len(b), _d(A), _d(b), _d(x))
     return x
+
+
+def setboundaries(xp, yp, zp, dl, dh, dd, del_=0.01):
+    """The reference's box panels: (numpan, 17) array, columns as in ref_setboundaries."""
+    n = 2 * (xp * yp + zp * yp + xp * zp)
+    out = np.zeros(17 * n)
+    lib(del_).ref_setboundaries(xp, yp, zp, dl, dh, dd, _d(out))
+    return out.reshape(n, 17)
+
+
+def panelconstantsreal(xp, yp, zp, dl, dh, dd, del_=0.01):
+    n = 2 * (xp * yp + zp * yp + xp * zp)
+    A = np.zeros(n * n)
+    lib(del_).ref_panelconstantsreal(xp, yp, zp, dl, dh, dd, _d(A))
+    return A.reshape(n, n)

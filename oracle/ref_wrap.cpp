@@ -286,4 +286,32 @@ int ref_gmres_dense(int n, const double* A, const double* b, double* x) {
   return s.gmres(rows.data(), bb.data(), x, n);
 }
 
+// setboundaries (src/tree3d.cpp:3764-3934): the box's boundary panels, 17 doubles each
+// (x0 x1 y0 y1 z0 z1 str xnrm ynrm znrm refpot midx midy midz type orientation area).
+// Returns the panel count.
+int ref_setboundaries(int xp, int yp, int zp, double dl, double dh, double dd, double* out) {
+  const int numpan = 2 * (xp * yp + zp * yp + xp * zp);
+  std::vector<PANEL> pan(numpan);
+  setboundaries(xp, yp, zp, dl, dh, dd, pan.data());
+  for (int i = 0; i < numpan; i++) {
+    const PANEL& q = pan[i];
+    const double v[17] = {q.x0, q.x1, q.y0, q.y1, q.z0, q.z1, q.str, q.xnrm, q.ynrm, q.znrm,
+                          q.refpot, q.midx, q.midy, q.midz, (double)q.type,
+                          (double)q.orientation, q.area};
+    for (int k = 0; k < 17; k++) out[17L * i + k] = v[k];
+  }
+  return numpan;
+}
+
+// panelconstantsreal (src/tree3d.cpp:4054-4078) on panels from ref_setboundaries; A is
+// row-major numpan x numpan.
+void ref_panelconstantsreal(int xp, int yp, int zp, double dl, double dh, double dd, double* A) {
+  const int numpan = 2 * (xp * yp + zp * yp + xp * zp);
+  std::vector<PANEL> pan(numpan);
+  setboundaries(xp, yp, zp, dl, dh, dd, pan.data());
+  std::vector<double*> rows(numpan);
+  for (int i = 0; i < numpan; i++) rows[i] = A + (long)i * numpan;
+  panelconstantsreal(numpan, pan.data(), rows.data());
+}
+
 }  // extern "C"

@@ -3,7 +3,8 @@
     make -C oracle ref && python tests/golden/make_golden.py
 
 Runs the reference's own treemake / treemoments / treepotential / shielded_treepot /
-treeforce (ongbw/bit src/tree3d.cpp, built by oracle/Makefile from the reference sources)
+treeforce / setboundaries / panelconstantsreal (ongbw/bit src/tree3d.cpp, built by
+oracle/Makefile from the reference sources)
 on seeded inputs and stores inputs and outputs as .npz.  The Coulomb potential runs with
 moment arrays padded to (nterms+1)^3 (oracle/ref_wrap.cpp) so its degree-nterms reads stay
 in bounds.  Only the reference's outputs are stored; nothing of the reference source is.
@@ -51,9 +52,20 @@ def case(name, x, y, z, q, w, nterms, maxmemb, del_, acc, kappa):
     print(name, "numtree", rec["nummemb"].shape[0])
 
 
+def panel_case(name, xp, yp, zp, dl, dh, dd, del_):
+    """setboundaries + panelconstantsreal of the reference build with DEL = del_."""
+    panels = ref.setboundaries(xp, yp, zp, dl, dh, dd, del_=del_)
+    A = ref.panelconstantsreal(xp, yp, zp, dl, dh, dd, del_=del_)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), xp=xp, yp=yp, zp=zp, dl=dl, dh=dh,
+                        dd=dd, del_=del_, panels=panels, A=A)
+    print(name, panels.shape, A.shape)
+
+
 def main():
     # the reference tests' own fixture (tests/treecode.cpp:41), smaller N
     x, y, z, q, w = ref.boxparticles(2000)
+    # 20 z-panels over depth 12 put one ring of panels in 4 < z < 5 (refpot 0)
+    panel_case("panels_box", 3, 2, 20, 2.0, 3.0, 12.0, 1e-4)
     case("box2000", x, y, z, q, w, nterms=5, maxmemb=100, del_=0.01, acc=0.5, kappa=1.0)
     # uniform cube, regularised Coulomb delta = 0.01 (DEL = 1e-4)
     x, y, z, q = workloads.uniform_cube(3000, seed=3)
