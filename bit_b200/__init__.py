@@ -185,6 +185,8 @@ SIGNATURES = [
     ("bit_panel_solve", C.c_int, [_vp, C.c_int, C.POINTER(Panel), C.c_int, _dp, _dp, _dp, _dp,
                                   C.c_double, C.c_int, C.c_double, C.c_int,
                                   C.POINTER(GmresOpts), C.POINTER(GmresInfo)]),
+    ("bit_write_potential", C.c_int, [C.c_char_p, C.c_int, _dp, _dp, _dp, _dp]),
+    ("bit_write_potential_device", C.c_int, [_vp, C.c_char_p, C.c_int, _vp, _vp, _vp, _vp]),
     ("bit_gmres_dense_static", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _ip, C.c_char_p,
                                          C.c_int]),
 ]
@@ -229,6 +231,14 @@ def panels_box(xpanels, ypanels, zpanels, dlength, dheight, ddepth):
 
 def panels_as_array(pan):
     return np.array([[getattr(p, k) for k in Panel.FIELDS] for p in pan], dtype=np.float64)
+
+
+def write_potential(path, x, y, z, pot):
+    """output_potential: 'i\tx\ty\tz\tpot' per particle, 14 significant digits."""
+    x, y, z, pot = map(_f64, (x, y, z, pot))
+    st = lib().bit_write_potential(path.encode(), len(x), _d(x), _d(y), _d(z), _d(pot))
+    if st:
+        raise BitError(st, f"bit_write_potential {path}")
 
 
 def kernel_launches():
@@ -343,6 +353,10 @@ class Context:
         if st not in (0, 7):
             self.check(st, "bit_panel_solve")
         return np.array([p.str for p in pan]), info.as_dict(), st
+
+    def write_potential_device(self, path, n, xp, yp, zp, potp):
+        self.check(lib().bit_write_potential_device(self.h, path.encode(), n, xp, yp, zp, potp),
+                   "bit_write_potential_device")
 
     def gmres_dense(self, A, b, x0=None):
         """solver::gmres (src/solver.h:157) on the device."""

@@ -274,6 +274,15 @@ bit_status bit_panel_solve(bit_ctx* ctx, int npan, bit_panel* pan, int np, const
                            int nterms, double acc, int maxmemb, const bit_gmres_opts* opts,
                            bit_gmres_info* info);
 
+/* output_potential (src/tree3d.cpp:4918-4937): one line per particle,
+ * "i\tx\ty\tz\tpot", 14 significant digits.  Host arrays. */
+bit_status bit_write_potential(const char* path, int n, const double* x, const double* y,
+                               const double* z, const double* pot);
+/* The same from device arrays, streamed to the file in chunks (device-to-host copies of the
+ * next chunk overlap the formatting of the current one). */
+bit_status bit_write_potential_device(bit_ctx* ctx, const char* path, int n, const double* x,
+                                      const double* y, const double* z, const double* pot);
+
 /* ---------------------------------------------------------------------------------
  * Serving (no reference counterpart: the reference has no request layer).
  * A server owns `slots` contexts on one device, each with its own stream, and a FIFO of

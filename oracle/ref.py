@@ -60,6 +60,7 @@ def lib(del_=0.01):
         L.ref_eval_grad_kernel.argtypes = [C.c_double] * 4 + [C.c_int, _dp]
         L.ref_gmres_dense.restype = C.c_int
         L.ref_gmres_dense.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.ref_output_potential.argtypes = [C.c_int] + [_dp] * 4 + [C.c_char_p]
         L.ref_setboundaries.restype = C.c_int
         L.ref_setboundaries.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp]
         L.ref_panelconstantsreal.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp]
@@ -207,3 +208,8 @@ def panelconstantsreal(xp, yp, zp, dl, dh, dd, del_=0.01):
     A = np.zeros(n * n)
     lib(del_).ref_panelconstantsreal(xp, yp, zp, dl, dh, dd, _d(A))
     return A.reshape(n, n)
+
+
+def output_potential(x, y, z, pot, filename, del_=0.01):
+    x, y, z, pot = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, pot)]
+    lib(del_).ref_output_potential(len(x), _d(x), _d(y), _d(z), _d(pot), filename.encode())

@@ -314,4 +314,13 @@ void ref_panelconstantsreal(int xp, int yp, int zp, double dl, double dh, double
   panelconstantsreal(numpan, pan.data(), rows.data());
 }
 
+// output_potential (src/tree3d.cpp:4918-4937) on caller arrays.
+void ref_output_potential(int n, const double* x, const double* y, const double* z,
+                          const double* pot, const char* filename) {
+  std::vector<PARTICLE> p(n);
+  for (int i = 0; i < n; i++) { p[i].x = x[i]; p[i].y = y[i]; p[i].z = z[i]; }
+  std::vector<double> pv(pot, pot + n);
+  output_potential(n, p.data(), pv.data(), std::string(filename));
+}
+
 }  // extern "C"

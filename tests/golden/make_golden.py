@@ -3,7 +3,7 @@
     make -C oracle ref && python tests/golden/make_golden.py
 
 Runs the reference's own treemake / treemoments / treepotential / shielded_treepot /
-treeforce / setboundaries / panelconstantsreal (ongbw/bit src/tree3d.cpp, built by
+treeforce / setboundaries / panelconstantsreal / output_potential (ongbw/bit src/tree3d.cpp, built by
 oracle/Makefile from the reference sources)
 on seeded inputs and stores inputs and outputs as .npz.  The Coulomb potential runs with
 moment arrays padded to (nterms+1)^3 (oracle/ref_wrap.cpp) so its degree-nterms reads stay
@@ -61,11 +61,23 @@ def panel_case(name, xp, yp, zp, dl, dh, dd, del_):
     print(name, panels.shape, A.shape)
 
 
+def output_case(name, n, seed):
+    """output_potential of the reference on seeded values (incl. signed zeros, tiny, huge)."""
+    rng = np.random.default_rng(seed)
+    x, y, z = (rng.uniform(-1, 1, n) for _ in range(3))
+    pot = rng.standard_normal(n) * 10.0 ** rng.integers(-20, 20, n)
+    pot[:4] = [0.0, -0.0, 1.0, -1234567.891011121314]
+    ref.output_potential(x, y, z, pot, os.path.join(HERE, name + ".txt"))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), x=x, y=y, z=z, pot=pot)
+    print(name, n)
+
+
 def main():
     # the reference tests' own fixture (tests/treecode.cpp:41), smaller N
     x, y, z, q, w = ref.boxparticles(2000)
     # 20 z-panels over depth 12 put one ring of panels in 4 < z < 5 (refpot 0)
     panel_case("panels_box", 3, 2, 20, 2.0, 3.0, 12.0, 1e-4)
+    output_case("output_potential", 300, 41)
     case("box2000", x, y, z, q, w, nterms=5, maxmemb=100, del_=0.01, acc=0.5, kappa=1.0)
     # uniform cube, regularised Coulomb delta = 0.01 (DEL = 1e-4)
     x, y, z, q = workloads.uniform_cube(3000, seed=3)

@@ -43,3 +43,17 @@ def test_direct_rejects_bad_target(ctx):
     x = np.zeros(4)
     with pytest.raises(B.BitError):
         ctx.direct(x, x, x, x, B.params(), [0, 4])
+
+
+def test_streamed_writer_from_device_matches_host_writer(tmp_path, ctx):
+    """bit_write_potential_device (chunked, overlapped copies) writes the same bytes."""
+    import torch
+    import bit_b200 as B
+    rng = np.random.default_rng(5)
+    n = 150_000  # more than two streamed chunks
+    x, y, z, pot = (rng.standard_normal(n) for _ in range(4))
+    B.write_potential(str(tmp_path / "host.txt"), x, y, z, pot)
+    d = [torch.tensor(a, dtype=torch.float64, device="cuda") for a in (x, y, z, pot)]
+    torch.cuda.synchronize()
+    ctx.write_potential_device(str(tmp_path / "dev.txt"), n, *[a.data_ptr() for a in d])
+    assert (tmp_path / "dev.txt").read_bytes() == (tmp_path / "host.txt").read_bytes()
