@@ -221,20 +221,30 @@ def run_bit(args):
     phases["fp64"] = {name: {"t_far": s["t_far"], "t_near": s["t_near"]}
                       for name, s in (("screened", st64_s), ("coulomb", st64_c))}
     line["phases"] = phases
-    # dominant kernel roofline: the screened near field
-    pairs = st_s["near_pairs"] - n
-    flops = FLOPS_NEAR["screened"] * pairs
-    t_near = st_s["t_near"]
-    achieved = flops / t_near / 1e12
+    # roofline of the dominant kernel, the screened far field (k_far, FP32 FMA pipe), and of
+    # the screened near field (FP32 + MUFU) beside it
     peak = fp32_peak_from_clock(clocks)
-    line["roofline"] = {"bound": "fp32", "kernel": "k_near32<SCREENED>",
-                        "achieved": achieved, "peak": peak["tflops"], "unit": "TFLOP/s",
-                        "frac": achieved / peak["tflops"], "peak_source": peak["source"],
-                        "traffic": profiled_traffic(),
+    fpp = far_flops_per_pair(NTERMS)
+    far_flops = fpp["screened"] * st_s["far_pairs"]
+    far_ach = far_flops / st_s["t_far"] / 1e12
+    line["roofline"] = {"bound": "fp32", "kernel": "k_far<nterms 9, SCREENED, float>",
+                        "achieved": far_ach, "peak": peak["tflops"], "unit": "TFLOP/s",
+                        "frac": far_ach / peak["tflops"], "peak_source": peak["source"],
+                        "traffic": profiled_traffic("k_far_screened_f32"),
                         "traffic_unit": "bytes per launch (dram read+write, one ncu pass at full size, "
                                         "profiles/launches_clustered2M_step.md)",
-                        "algorithmic": f"{FLOPS_NEAR['screened']} flops x {pairs} near pairs per launch",
-                        "mufu_bound_frac": (2 * pairs / t_near) / peak["mufu_ops"]}
+                        "algorithmic": f"{fpp['screened']} flops (the reference's screened recurrence "
+                                       f"to degree 8 and the moment dot product) x {st_s['far_pairs']} "
+                                       "(target, cluster) pairs per launch"}
+    pairs = st_s["near_pairs"] - n
+    t_near = st_s["t_near"]
+    near_ach = FLOPS_NEAR["screened"] * pairs / t_near / 1e12
+    line["roofline_near"] = {"bound": "fp32+mufu", "kernel": "k_near<SCREENED, F32>",
+                             "achieved": near_ach, "peak": peak["tflops"], "unit": "TFLOP/s",
+                             "frac": near_ach / peak["tflops"],
+                             "mufu_frac": (2 * pairs / t_near) / peak["mufu_ops"],
+                             "traffic": profiled_traffic("k_near_screened_f32"),
+                             "algorithmic": f"{FLOPS_NEAR['screened']} flops x {pairs} near pairs per launch"}
     # accuracy of this step against the FP64 GPU path and the FP64 direct sum (sampled)
     line["accuracy"] = accuracy(ctx, x, y, z, q, res_s, res_c, res64_s, res64_c, args)
     if args.bie:
@@ -492,6 +502,17 @@ def run_serving(ctx, args):
             "mixed_vs_fp64_max": float(max(diff)),
             "eval_error_vs_direct_200_targets": {"median": float(np.median(derr)),
                                                  "max": float(np.max(derr))}}
+
+
+def far_flops_per_pair(nterms):
+    """Flops per (target, cluster) pair of the generated far-field recurrences, counted from
+    the generator (bit_b200/csrc/gen_farfield.py)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "gen_farfield", os.path.join(ROOT, "bit_b200", "csrc", "gen_farfield.py"))
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    return g.flops_per_pair(nterms)
 
 
 def profiled_traffic(key="k_near_screened_f32"):

@@ -267,6 +267,30 @@ def gen_force(nt):
     return L
 
 
+def count_flops(lines):
+    """Floating-point operations of generated lines: every binary + - * /, 2 per fma_t,
+    1 per sqrt_t / rsqrt_t / exp_t (literals and the moment loads are not arithmetic)."""
+    import re
+    n = 0
+    for ln in lines:
+        if "=" not in ln or "ld4(" in ln:
+            continue
+        e = re.sub(r"T\([^()]*\)", "C", ln.split("=", 1)[1])
+        n += 2 * e.count("fma_t(") + e.count("sqrt_t(") + e.count("exp_t(")
+        e = re.sub(r"[a-z_]+\(", "(", e)
+        n += e.count("*") + e.count("/") + e.count("+")
+        # binary minus: preceded by an operand (name, number, closing parenthesis)
+        n += len(re.findall(r"[\w)]\s*-", e))
+    return n
+
+
+def flops_per_pair(nt):
+    """Flops of one (target, cluster) far-field evaluation: the reference's recurrence to
+    degree nterms-1 plus the moment dot product, as generated."""
+    return {"coulomb": count_flops(gen_coulomb(nt)), "screened": count_flops(gen_screened(nt)),
+            "force": count_flops(gen_force(nt))}
+
+
 def main(out):
     parts = ["// GENERATED by gen_farfield.py -- do not edit.",
              "#pragma once",

@@ -2,7 +2,8 @@
 //
 // bit_bie_solve: restarted GMRES(m) for (diag*I + K) s = f where K is the treecode with
 // charges w*s (no reference counterpart: the reference's solver::gmres takes a dense
-// matrix, src/solver.h:157-260).  Vectors live in tree order on the device; each matvec
+// matrix, src/solver.h:157-260); every matvec after the first of each precision replays a
+// CUDA graph.  Vectors live in tree order on the device; each matvec
 // rewrites the charges, recomputes the moments (FP64) and runs the far and near kernels
 // over the interaction lists built once for the tree.  Arnoldi is classical Gram-Schmidt
 // applied twice (FP64 dot products and updates on the device); the (m+1) x m Hessenberg
@@ -144,8 +145,24 @@ struct BieOp {
   double diag;
   DBuf<double> w_s;
   int mv64 = 0, mv32 = 0;
+  // One CUDA graph per precision holds a whole matvec (charges, moments, far and near
+  // launches, axpby) on fixed buffers; a matvec then copies x in, replays the graph and
+  // copies y out.  It is captured on the second matvec of a precision, after the first
+  // (eager) one has made every allocation and plan.  Capture failures fall back to eager
+  // launches.
+  DBuf<double> gin, gout;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  long long glaunches[2] = {0, 0};  // kernels in each graph
+  int eager[2] = {0, 0};
+  bool graphs = true;
+
+  ~BieOp() {
+    for (auto& g : gexec)
+      if (g) cudaGraphExecDestroy(g);
+  }
+
   // y = diag*x + K(w*x), everything in tree order
-  void apply(const double* x, double* y, bit_precision prec) {
+  void apply_eager(const double* x, double* y, bit_precision prec) {
     Ctx* c = t->ctx;
     cudaStream_t s = c->stream;
     const int n = t->n;
@@ -158,7 +175,67 @@ struct BieOp {
     eval_near(t, &t->plists, t->pplan, t->sx.p, t->sy.p, t->sz.p, y);
     count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, diag, x, 1.0, y);
     BIT_CHECK_LAUNCH();
+  }
+
+  bool capture(int pi, bit_precision prec) {
+    Ctx* c = t->ctx;
+    cudaStream_t s = c->stream;
+    gin.ensure(c, t->n);
+    gout.ensure(c, t->n);
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    bool ok = true;
+    try {
+      apply_eager(gin.p, gout.p, prec);
+    } catch (const Error&) {
+      ok = false;
+    }
+    const cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (!ok || e != cudaSuccess || !g) {
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      return false;
+    }
+    size_t nodes = 0;
+    cudaGraphGetNodes(g, nullptr, &nodes);
+    std::vector<cudaGraphNode_t> nv(nodes);
+    if (nodes) cudaGraphGetNodes(g, nv.data(), &nodes);
+    long long kernels = 0;
+    for (auto& nd : nv) {
+      cudaGraphNodeType ty;
+      if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) kernels++;
+    }
+    launch_counter().fetch_sub(kernels);  // counted while capturing, but nothing ran
+    const cudaError_t ie = cudaGraphInstantiate(&gexec[pi], g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      gexec[pi] = nullptr;
+      return false;
+    }
+    glaunches[pi] = kernels;
+    return true;
+  }
+
+  void apply(const double* x, double* y, bit_precision prec) {
+    const int pi = prec == BIT_PREC_MIXED ? 1 : 0;
     (prec == BIT_PREC_FP64 ? mv64 : mv32)++;
+    if (graphs && !gexec[pi] && eager[pi] >= 1 && !capture(pi, prec)) graphs = false;
+    if (!graphs || !gexec[pi]) {
+      eager[pi]++;
+      apply_eager(x, y, prec);
+      return;
+    }
+    Ctx* c = t->ctx;
+    cudaStream_t s = c->stream;
+    const size_t bytes = (size_t)t->n * sizeof(double);
+    BIT_CUDA(cudaMemcpyAsync(gin.p, x, bytes, cudaMemcpyDeviceToDevice, s));
+    BIT_CUDA(cudaGraphLaunch(gexec[pi], s));
+    BIT_CUDA(cudaMemcpyAsync(y, gout.p, bytes, cudaMemcpyDeviceToDevice, s));
+    launch_counter().fetch_add(glaunches[pi]);
   }
 };
 
