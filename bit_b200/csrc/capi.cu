@@ -274,6 +274,12 @@ bit_status bit_ctx_destroy(bit_ctx* h) {
 
 const char* bit_ctx_last_error(const bit_ctx* h) { return h ? h->c.last_error.c_str() : "null context"; }
 
+bit_status bit_ctx_set_group_size(bit_ctx* h, int targets) {
+  if (!h || (targets != 0 && (targets < 32 || targets > kGroupMax))) return BIT_ERR_INVALID_ARGUMENT;
+  h->c.group_targets = targets;
+  return BIT_OK;
+}
+
 bit_status bit_ctx_synchronize(bit_ctx* h) {
   if (!h) return BIT_ERR_INVALID_ARGUMENT;
   return guard(&h->c, [&] { BIT_CUDA(cudaStreamSynchronize(h->c.stream)); });

@@ -121,11 +121,12 @@ struct EvalPlan {
 struct ListKey {
   double acc = -1, add_del = 0, sub_del = 0;
   int points = 0;  // 0: particle targets, 1: external points
+  int group = 0;  // particle targets packed per group (0: one leaf per group)
   long long gen = -1;  // tree generation it was built for
   std::vector<double> sysmac;  // forests: (acc, add, sub) of every system
   bool operator==(const ListKey& o) const {
     return acc == o.acc && add_del == o.add_del && sub_del == o.sub_del &&
-           points == o.points && gen == o.gen && sysmac == o.sysmac;
+           points == o.points && group == o.group && gen == o.gen && sysmac == o.sysmac;
   }
 };
 
@@ -135,7 +136,7 @@ struct Lists {
   int ngroups = 0;
   long long nfar = 0, nnear = 0;            // entries
   long long far_pairs = 0, near_pairs = 0;  // interactions
-  DBuf<int> g_tstart, g_tcount, g_own;      // group: first target, count, own leaf (or -1)
+  DBuf<int> g_tstart, g_tcount;             // group: first target, count
   DBuf<int> g_sys;                          // group: system (its root node)
   std::vector<int> h_g_sys;
   DBuf<long long> far_off, near_off;        // first entry of each group
@@ -158,6 +159,7 @@ struct Ctx {
   size_t budget = 0, in_use = 0, peak = 0;
   std::string last_error;
   int num_sms = 148;
+  int group_targets = 0;  // leaves packed into groups of up to this many targets (0: off)
   // small device scratch for flags / counters
   DBuf<long long> scratch_ll;
   long long* h_pinned = nullptr;  // pinned host staging for small read-backs (64 entries)

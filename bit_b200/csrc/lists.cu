@@ -1,8 +1,8 @@
 // Interaction lists: the MAC traversal of treepotential / shielded_treepot / treeforce
 // (src/tree3d.cpp:4679-4778, 3448-3627, 851-971) for a whole group of targets at once.
 //
-// A group is up to 1024 consecutive targets (a leaf, or a chunk of one; for external
-// points, 256 consecutive points in Morton order).  One CTA walks the tree for the group,
+// A group is up to 1024 consecutive targets (a run of consecutive small leaves, a leaf, or
+// a chunk of one; for external points, 256 consecutive points in Morton order).  One CTA walks the tree for the group,
 // one thread per target, one 32-bit mask word per warp.  At a node every active target
 // evaluates the reference's acceptance test in FP64 without contraction
 // (sqradius < acc * ((dx*dx + dy*dy + dz*dz + add) - sub)); the node becomes a far entry
@@ -227,45 +227,82 @@ void set_stage_attr() {
 
 }  // namespace
 
-// Groups for particle targets: each leaf, in chunks of at most kGroupMax members.
-static void particle_groups(Tree* t, std::vector<int>& ts, std::vector<int>& tc,
-                            std::vector<int>& own, std::vector<int>& sys) {
-  for (int i = 0; i < t->numtree; i++) {
-    if (t->h_children[8LL * i] != -1) continue;
-    int st = t->h_start[i], en = st + t->h_nummemb[i];
-    for (int e = st; e < en; e += kGroupMax) {
-      ts.push_back(e);
-      tc.push_back(std::min(kGroupMax, en - e));
-      own.push_back(i);
-      sys.push_back(t->h_node_sys[i]);
+// Groups for particle targets.  G = 0: each leaf, in chunks of at most kGroupMax targets.
+// G > 0: runs of consecutive leaves (in tree order, which keeps them spatially close:
+// siblings and cousins) of one system, up to G targets together; a leaf larger than G is
+// cut into chunks of G.  Packed small leaves share one traversal, one set of entries and
+// the near field's source tiles, but each near entry then covers fewer targets; which is
+// faster depends on the workload (bit_b200.autotune measures it).
+static void particle_groups(Tree* t, int G, std::vector<int>& ts, std::vector<int>& tc,
+                            std::vector<int>& sys) {
+  if (G <= 0) {
+    for (int i = 0; i < t->numtree; i++) {
+      if (t->h_children[8LL * i] != -1) continue;
+      const int st = t->h_start[i], en = st + t->h_nummemb[i];
+      for (int e = st; e < en; e += kGroupMax) {
+        ts.push_back(e);
+        tc.push_back(std::min(kGroupMax, en - e));
+        sys.push_back(t->h_node_sys[i]);
+      }
     }
+    return;
   }
+  std::vector<int> leaves;
+  for (int i = 0; i < t->numtree; i++)
+    if (t->h_children[8LL * i] == -1) leaves.push_back(i);
+  std::sort(leaves.begin(), leaves.end(),
+            [&](int a, int b) { return t->h_start[a] < t->h_start[b]; });
+  int cur0 = -1, curn = 0, cursys = -1;
+  auto flush = [&] {
+    if (curn > 0) {
+      ts.push_back(cur0);
+      tc.push_back(curn);
+      sys.push_back(cursys);
+    }
+    curn = 0;
+  };
+  for (int i : leaves) {
+    const int st = t->h_start[i], cnt = t->h_nummemb[i], sy = t->h_node_sys[i];
+    if (cnt > G) {
+      flush();
+      for (int e = st; e < st + cnt; e += G) {
+        ts.push_back(e);
+        tc.push_back(std::min(G, st + cnt - e));
+        sys.push_back(sy);
+      }
+      continue;
+    }
+    if (curn > 0 && (sy != cursys || curn + cnt > G || cur0 + curn != st)) flush();
+    if (curn == 0) {
+      cur0 = st;
+      cursys = sy;
+    }
+    curn += cnt;
+  }
+  flush();
 }
 
 void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const double* tx,
                  const double* ty, const double* tz, const SysEval* d_sys) {
   Ctx* c = t->ctx;
   cudaStream_t s = c->stream;
-  std::vector<int> ts, tc, own, gsys;
+  std::vector<int> ts, tc, gsys;
   if (key.points) {
     if (t->nsys != 1) fail(BIT_ERR_INVALID_ARGUMENT, "external points need a single-system tree");
     for (int e = 0; e < ntargets; e += kPointGroup) {
       ts.push_back(e);
       tc.push_back(std::min(kPointGroup, ntargets - e));
-      own.push_back(-1);
       gsys.push_back(0);
     }
   } else {
-    particle_groups(t, ts, tc, own, gsys);
+    particle_groups(t, key.group, ts, tc, gsys);
   }
   const int ng = (int)ts.size();
   L->ngroups = ng;
   L->g_tstart.ensure(c, ng);
   L->g_tcount.ensure(c, ng);
-  L->g_own.ensure(c, ng);
   BIT_CUDA(cudaMemcpyAsync(L->g_tstart.p, ts.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   BIT_CUDA(cudaMemcpyAsync(L->g_tcount.p, tc.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
-  BIT_CUDA(cudaMemcpyAsync(L->g_own.p, own.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   L->g_sys.ensure(c, ng);
   BIT_CUDA(cudaMemcpyAsync(L->g_sys.p, gsys.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));
   L->h_g_sys = gsys;

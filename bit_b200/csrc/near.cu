@@ -27,7 +27,7 @@ namespace {
 constexpr int NT = 256;  // threads per CTA
 
 struct NearArgs {
-  const int *order, *g_tstart, *g_tcount, *g_own;
+  const int *order, *g_tstart, *g_tcount;
   const double *tx, *ty, *tz;
   const long long *off, *moff;
   const int* cnt;
@@ -274,7 +274,6 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const SysEval* se = a.sys + a.g_sys[g];
   const double sdel = se->near_del, skappa = se->kappa;
-  const int own = se->particles ? a.g_own[g] : -1;
   const int W = (tc + 31) >> 5;
   const long long e0 = a.off[g], e1 = e0 + a.cnt[g];
   const long long m0 = a.moff[g];
@@ -348,8 +347,10 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
       }
       const S* ts = tiles + buf * TILE;
       const double4 c = a.nodec[node];
-      // tile index of target i's own source is i + selfbase (particle targets, own leaf)
-      const int selfbase = (node == own) ? (t0 - (j0 + toff)) : INT_MIN;
+      // Particle targets: target i's own source sits at its sorted position t0 + i, i.e.
+      // at tile index i + selfbase, which is inside this tile only if the target is one
+      // of the tile's sources.
+      const int selfbase = se->particles ? (t0 - (j0 + toff)) : INT_MIN;
       const int units = cnt * tpt;
       const int lt = __ffs(tpt) - 1;
       // close-pair checks are needed only where a target comes within r_t of this leaf's box
@@ -493,7 +494,6 @@ NearArgs base_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const
   NearArgs a{};
   a.g_tstart = L->g_tstart.p;
   a.g_tcount = L->g_tcount.p;
-  a.g_own = L->g_own.p;
   a.tx = tx; a.ty = ty; a.tz = tz;
   a.off = L->near_off.p;
   a.cnt = L->near_cnt.p;

@@ -100,6 +100,7 @@ void plan_sys(Tree* t, EvalPlan* P, const std::vector<bit_eval_params>& prm, int
 ListKey plan_key(const Tree* t, const EvalPlan& P, int points) {
   ListKey k;
   k.points = points;
+  k.group = t->ctx->group_targets;
   k.gen = t->gen;
   const SysEval& s0 = P.h_sys[0];
   k.acc = s0.acc;

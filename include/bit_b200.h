@@ -99,6 +99,11 @@ bit_status bit_ctx_create(bit_ctx** ctx, const bit_ctx_opts* opts);
 bit_status bit_ctx_destroy(bit_ctx* ctx);
 const char* bit_ctx_last_error(const bit_ctx* ctx);
 bit_status bit_ctx_synchronize(bit_ctx* ctx);
+/* Leaf packing, a tuning knob (bit_b200.autotune): 0 (default) evaluates each leaf as its
+ * own group of targets; 32..1024 evaluates runs of consecutive small leaves together, up
+ * to that many targets (one traversal, shared source tiles).  Results do not depend on it
+ * beyond FP32 summation order. */
+bit_status bit_ctx_set_group_size(bit_ctx* ctx, int targets);
 bit_status bit_ctx_stream(const bit_ctx* ctx, void** stream);
 /* Bytes currently allocated by the context and its trees. */
 bit_status bit_ctx_memory(const bit_ctx* ctx, size_t* in_use, size_t* peak);

@@ -135,3 +135,53 @@ def test_forest_rejects_bad_input(ctx):
     F.moments([4, 5])
     with pytest.raises(B.BitError):  # mixed precisions in one call
         F.evaluate([B.params(precision=B.FP64), B.params(precision=B.MIXED)])
+
+
+@pytest.mark.parametrize("group", [256, 1024])
+def test_packed_leaf_groups_match_oracle(orc, group):
+    """Packing consecutive small leaves into one group changes only the grouping of work:
+    FP64 stays within 1e-12 of the oracle, every target keeps its own interaction lists,
+    and a forest still gives each system its single-system result."""
+    import bit_b200 as B
+    ctx = B.Context()
+    try:
+        ctx.set_group_size(group)
+        xs, ys, zs, qs = make_systems(SIZES, 5)
+        F = ctx.forest(np.concatenate(xs), np.concatenate(ys), np.concatenate(zs), SIZES, MAXMEMB)
+        F.set_charges(np.concatenate(qs))
+        F.moments(NTERMS)
+        prm = [system_params(B, s, B.FP64) for s in range(len(SIZES))]
+        got = F.evaluate(prm)
+        for s in range(len(SIZES)):
+            T = orc.Tree(xs[s], ys[s], zs[s], MAXMEMB[s])
+            T.compute_moments(qs[s], NTERMS[s])
+            ref = T.evaluate(oracle_params(orc, prm[s]))
+            scale = max(np.linalg.norm(ref), 1e-300)
+            assert np.linalg.norm(F.system(s, got) - ref) / scale < 1e-12, s
+        # per-target lists of a packed single-system tree equal the reference traversal
+        x, y, z, q = xs[0], ys[0], zs[0], qs[0]
+        t = ctx.treemake(x, y, z, 50)
+        t.treemoments(q, 5)
+        p = B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=1e-4, acc=0.5)
+        t.evaluate(p)
+        T = orc.Tree(x, y, z, 50)
+        T.compute_moments(q, 5)
+        po = orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=1e-4, acc=0.5)
+        for i in (0, 17, 1234, len(x) - 1):
+            node, kind = t.target_lists(p, i)
+            rn, rk = T.target_lists(po, i)
+            np.testing.assert_array_equal(node, rn)
+            np.testing.assert_array_equal(kind, rk)
+        mixed = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.MIXED, del_=1e-4, acc=0.5))
+        ref = T.evaluate(po)
+        assert np.linalg.norm(mixed - ref) / np.linalg.norm(ref) < 1e-6
+    finally:
+        ctx.close()
+
+
+def test_group_size_is_validated(ctx):
+    import bit_b200 as B
+    with pytest.raises(B.BitError):
+        ctx.set_group_size(5000)
+    with pytest.raises(B.BitError):
+        ctx.set_group_size(10)
