@@ -3,9 +3,10 @@
 // about the node's box midpoint, in FP64 for every node.
 //
 // Members of every node are contiguous in tree order, so a node is a run of chunks.  One
-// block per (node, chunk): members' powers are staged in shared memory and each thread
-// owns one (i, j, k) term; per-chunk partial sums are then added per node in chunk order,
-// so the result is deterministic (no floating-point atomics).
+// block per (node, chunk): each warp keeps one group of terms in registers while its lanes
+// run over the chunk's members (powers in registers, no shared-memory traffic per term);
+// lanes are combined by shuffles and chunks per node in chunk order, so the result is
+// deterministic (no floating-point atomics).
 #include <algorithm>
 #include <vector>
 
@@ -16,51 +17,101 @@ namespace bit {
 namespace {
 
 constexpr int MCH = 1024;  // members per chunk
-constexpr int SUB = 128;   // members staged in shared memory at a time
-constexpr int MTB = 256;   // threads per block (>= num_terms(10) = 220)
+constexpr int MTB = 256;   // threads per block: 8 warps = 4 term groups x 2 member halves
 
-// chunks: (node, first member, last member, chunk id); partials at part[id * TMAX + term]
+// The terms are split into MG groups of consecutive packed indices, cut at (i, j)
+// boundaries (a run of k for one (i, j) stays in one group) and balanced by count.
+constexpr int MG = 4;
+template <int NT>
+struct MomPlan {
+  // packed index of (i, j, 0)
+  static constexpr int start(int i, int j) {
+    int s = 0;
+    for (int a = 0; a < i; a++) s += (NT - a) * (NT - a + 1) / 2;
+    for (int b = 0; b < j; b++) s += NT - i - b;
+    return s;
+  }
+  // first packed index of group g (bound(MG) == T)
+  static constexpr int bound(int g) {
+    const int T = num_terms(NT);
+    if (g <= 0) return 0;
+    if (g >= MG) return T;
+    for (int i = 0; i < NT; i++)
+      for (int j = 0; j < NT - i; j++)
+        if (start(i, j) * MG >= g * T) return start(i, j);
+    return T;
+  }
+};
+
+// One warp: the terms of group G for the chunk's members e0 + half*32 + lane + 64 r, with
+// powers and accumulators in registers; the 32 lanes are summed by shuffles (fixed order).
+template <int NT, int G>
+__device__ __forceinline__ void moments_group(const double4* __restrict__ src, int e0, int e1,
+                                              double4 c, int lane, int half, double* s_part) {
+  constexpr int T0 = MomPlan<NT>::bound(G), T1 = MomPlan<NT>::bound(G + 1);
+  constexpr int NG = T1 - T0;
+  constexpr int TMAX = num_terms(kNtermsMax);
+  if constexpr (NG > 0) {
+    double acc[NG];
+#pragma unroll
+    for (int t = 0; t < NG; t++) acc[t] = 0.0;
+    for (int e = e0 + half * 32 + lane; e < e1; e += 64) {
+      const double4 s = src[e];
+      const double dx = s.x - c.x, dy = s.y - c.y, dz = s.z - c.z;
+      double py[NT], pz[NT];
+      py[0] = 1.0;
+      pz[0] = 1.0;
+#pragma unroll
+      for (int k = 1; k < NT; k++) {
+        py[k] = py[k - 1] * dy;
+        pz[k] = pz[k - 1] * dz;
+      }
+      double px = s.w;  // q dx^i
+#pragma unroll
+      for (int i = 0; i < NT; i++) {
+#pragma unroll
+        for (int j = 0; j < NT - i; j++) {
+          const int st = MomPlan<NT>::start(i, j);
+          if (st >= T0 && st < T1) {
+            const double xy = px * py[j];
+#pragma unroll
+            for (int k = 0; k < NT - i - j; k++) acc[st - T0 + k] = fma(xy, pz[k], acc[st - T0 + k]);
+          }
+        }
+        px *= dx;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < NG; t++) {
+      double v = acc[t];
+#pragma unroll
+      for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) s_part[half * TMAX + T0 + t] = v;
+    }
+  }
+}
+
+// chunks: (node, first member, last member, chunk id); partials at part[id * TMAX + term].
+// 8 warps: warp w takes term group w % 4 for the members of half w / 4.
 template <int NT>
 __global__ void __launch_bounds__(MTB) k_moments_partial(const int4* chunks, const double4* fld,
                                                          const double4* src, double* part) {
   constexpr int T = num_terms(NT);
   constexpr int TMAX = num_terms(kNtermsMax);
-  __shared__ double P[SUB][3 * NT];
+  __shared__ double s_part[2 * TMAX];
   const int4 ck = chunks[blockIdx.x];
   const double4 c = fld[ck.x];
-  int ti = 0, tj = 0, tk = 0;
-  {
-    int idx = 0;
-    for (int i = 0; i < NT; i++)
-      for (int j = 0; j < NT - i; j++)
-        for (int k = 0; k < NT - i - j; k++) {
-          if (idx == (int)threadIdx.x) { ti = i; tj = j; tk = k; }
-          idx++;
-        }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = w & (MG - 1), half = w / MG;
+  switch (g) {
+    case 0: moments_group<NT, 0>(src, ck.y, ck.z, c, lane, half, s_part); break;
+    case 1: moments_group<NT, 1>(src, ck.y, ck.z, c, lane, half, s_part); break;
+    case 2: moments_group<NT, 2>(src, ck.y, ck.z, c, lane, half, s_part); break;
+    default: moments_group<NT, 3>(src, ck.y, ck.z, c, lane, half, s_part); break;
   }
-  double acc = 0.0;
-  for (int e0 = ck.y; e0 < ck.z; e0 += SUB) {
-    const int cnt = min(SUB, ck.z - e0);
-    if ((int)threadIdx.x < cnt) {
-      double4 s = src[e0 + threadIdx.x];
-      double dx = s.x - c.x, dy = s.y - c.y, dz = s.z - c.z;
-      double px = s.w, py = 1.0, pz = 1.0;
-#pragma unroll
-      for (int i = 0; i < NT; i++) {
-        P[threadIdx.x][i] = px;
-        P[threadIdx.x][NT + i] = py;
-        P[threadIdx.x][2 * NT + i] = pz;
-        px *= dx; py *= dy; pz *= dz;
-      }
-    }
-    __syncthreads();
-    if ((int)threadIdx.x < T) {
-      for (int e = 0; e < cnt; e++)
-        acc = fma(P[e][ti] * P[e][NT + tj], P[e][2 * NT + tk], acc);
-    }
-    __syncthreads();
-  }
-  if ((int)threadIdx.x < T) part[(long long)ck.w * TMAX + threadIdx.x] = acc;
+  __syncthreads();
+  for (int t = threadIdx.x; t < T; t += MTB)
+    part[(long long)ck.w * TMAX + t] = s_part[t] + s_part[TMAX + t];
 }
 
 // Per node: the sum of its chunks' partials, in chunk order.
