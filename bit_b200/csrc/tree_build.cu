@@ -380,23 +380,43 @@ __global__ void __launch_bounds__(TB) k_split_pass(const int2* chunks, int a, co
     }
   }
   if (!hc) return;
-  __shared__ int s_cnt[2];
-  if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0;
-  __syncthreads();
+  // warp, then CTA reductions; one set of global atomics per CTA (min / max / sum are
+  // order-independent, so the result is exact whatever the order)
+  constexpr int NW = TB / 32;
+  __shared__ int s_c[NW][2];
+  __shared__ unsigned long long s_m[NW][2][3], s_M[NW][2][3];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int h = 0; h < 2; h++) {
-    int c = warp_sum(cnt[h]);
+    const int c = warp_sum(cnt[h]);
     unsigned long long m[3], M[3];
     for (int d = 0; d < 3; d++) { m[d] = warp_min(mn[h][d]); M[d] = warp_max(mx[h][d]); }
-    if ((threadIdx.x & 31) == 0 && c > 0) {
-      atomicAdd(&s_cnt[h], c);
-      for (int d = 0; d < 3; d++) {
-        atomicMin(&acc[ck.x].mn[h][d], m[d]);
-        atomicMax(&acc[ck.x].mx[h][d], M[d]);
-      }
+    if (lane == 0) {
+      s_c[w][h] = c;
+      for (int d = 0; d < 3; d++) { s_m[w][h][d] = m[d]; s_M[w][h][d] = M[d]; }
     }
   }
   __syncthreads();
-  if (threadIdx.x < 2 && s_cnt[threadIdx.x]) atomicAdd(&acc[ck.x].cnt[threadIdx.x], s_cnt[threadIdx.x]);
+  if (threadIdx.x < 2 * 7) {  // thread (h, v): v = 0..5 min/max of one axis, v = 6 count
+    const int h = threadIdx.x / 7, v = threadIdx.x % 7;
+    int c = 0;
+    for (int q = 0; q < NW; q++) c += s_c[q][h];
+    if (c > 0) {
+      if (v == 6) {
+        atomicAdd(&acc[ck.x].cnt[h], c);
+      } else {
+        const int d = v >> 1;
+        if (v & 1) {
+          unsigned long long M = 0;
+          for (int q = 0; q < NW; q++) M = s_M[q][h][d] > M ? s_M[q][h][d] : M;
+          atomicMax(&acc[ck.x].mx[h][d], M);
+        } else {
+          unsigned long long m = ~0ULL;
+          for (int q = 0; q < NW; q++) m = s_m[q][h][d] < m ? s_m[q][h][d] : m;
+          atomicMin(&acc[ck.x].mn[h][d], m);
+        }
+      }
+    }
+  }
 }
 
 __global__ void k_scatter_count(const int2* chunks, int a, const int* start, const int* nummemb,
