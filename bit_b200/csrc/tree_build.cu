@@ -442,23 +442,49 @@ __global__ void k_scatter_count(const int2* chunks, int a, const int* start, con
   if (threadIdx.x < 8) cc[blockIdx.x * 8 + threadIdx.x] = s[threadIdx.x];
 }
 
-// Per node: destination offset of each chunk's members of each child slot.
-__global__ void k_scatter_offsets(int a, int nlev, const int* start, const int* cbeg,
-                                  const int* cc, int* coff, const SplitState* st, int* err) {
-  int li = blockIdx.x * blockDim.x + threadIdx.x;
-  if (li >= nlev) return;
+// Per node (one block): destination offset of each chunk's members of each child slot,
+// an exclusive scan over the node's chunks of the per-slot counts, 8 slots at once.
+__global__ void __launch_bounds__(TB) k_scatter_offsets(int a, const int* start, const int* cbeg,
+                                                        const int* cc, int* coff,
+                                                        const SplitState* st, int* err) {
+  const int li = blockIdx.x;
   const SplitState* S = &st[li];
   if (!S->active) return;
-  int base[8], run[8];
-  int s0 = start[a + li], acc = 0;
-  for (int v = 0; v < 8; v++) { base[v] = acc; acc += S->slot_n[v]; run[v] = 0; }
-  for (int c = cbeg[li]; c < cbeg[li + 1]; c++)
+  constexpr int NW = TB / 32;
+  __shared__ int s_base[8], s_carry[8], s_warp[NW][8];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  if (tid == 0) {
+    int acc = 0;
+    for (int v = 0; v < 8; v++) { s_base[v] = start[a + li] + acc; acc += S->slot_n[v]; s_carry[v] = 0; }
+  }
+  __syncthreads();
+  const int c0 = cbeg[li], c1 = cbeg[li + 1];
+  for (int cb = c0; cb < c1; cb += TB) {
+    const int c = cb + tid;
+    int val[8], inc[8];
     for (int v = 0; v < 8; v++) {
-      coff[c * 8 + v] = s0 + base[v] + run[v];
-      run[v] += cc[c * 8 + v];
+      val[v] = c < c1 ? cc[c * 8 + v] : 0;
+      inc[v] = val[v];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, inc[v], o);
+        if (lane >= o) inc[v] += t;
+      }
     }
-  for (int v = 0; v < 8; v++)
-    if (run[v] != S->slot_n[v]) atomicOr(err, 8);
+    if (lane == 31)
+      for (int v = 0; v < 8; v++) s_warp[w][v] = inc[v];
+    __syncthreads();
+    if (c < c1)
+      for (int v = 0; v < 8; v++) {
+        int before = s_carry[v];
+        for (int q = 0; q < w; q++) before += s_warp[q][v];
+        coff[c * 8 + v] = s_base[v] + before + inc[v] - val[v];
+      }
+    __syncthreads();
+    if (tid < 8)
+      for (int q = 0; q < NW; q++) s_carry[tid] += s_warp[q][tid];
+    __syncthreads();
+  }
+  if (tid < 8 && s_carry[tid] != S->slot_n[tid]) atomicOr(err, 8);
 }
 
 // Stable scatter of each chunk's members to their child's range (order kept).
@@ -676,7 +702,7 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
                                                           t->sy.p, t->sz.p, lab.p, st.p, acc.p);
     count_launch(), k_scatter_count<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, cc.p);
-    count_launch(), k_scatter_offsets<<<gl, 128, 0, s>>>(a, nlev, t->start.p, cbeg.p, cc.p, coff.p, st.p, err.p);
+    count_launch(), k_scatter_offsets<<<nlev, TB, 0, s>>>(a, t->start.p, cbeg.p, cc.p, coff.p, st.p, err.p);
     count_launch(), k_scatter<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, coff.p,
                                                        t->perm.p, t->sx.p, t->sy.p, t->sz.p, perm2.p, sx2.p,
                                                        sy2.p, sz2.p);
