@@ -31,7 +31,8 @@ constexpr int LT = 1024;          // threads of the list builder (one per target
 constexpr int LSTK = 256;         // traversal stack entries per group
 constexpr int STAGE_FAR = 20480;  // staging words (node + mask words per entry), far list
 constexpr int STAGE_NEAR = 6144;  // staging words, near list
-constexpr size_t STAGE_BYTES = (STAGE_FAR + STAGE_NEAR) * sizeof(unsigned);
+constexpr size_t STACK_BYTES = 32 * LSTK * sizeof(int);  // per-warp node stacks
+constexpr size_t STAGE_BYTES = STACK_BYTES + (STAGE_FAR + STAGE_NEAR) * sizeof(unsigned);
 
 enum { MODE_COUNT = 0, MODE_FILL = 1, MODE_STAGE = 2 };
 
@@ -56,11 +57,14 @@ struct ListArgs {
 
 template <int MODE>
 __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
-  __shared__ int s_node[LSTK];
-  __shared__ unsigned s_mask[LSTK][32];
-  __shared__ unsigned s_am[32], s_rm[32];
+  __shared__ unsigned s_mask[LSTK][32];  // each warp's mask word of every stack entry
+  __shared__ unsigned s_am[2][32], s_rm[2][32];  // accept / reject words, by parity
   __shared__ unsigned long long s_base[4];
-  extern __shared__ unsigned stage[];
+  extern __shared__ unsigned dyn[];
+  // dynamic shared memory: each warp's own copy of the node stack, then (MODE_STAGE) the
+  // staging area of the lists
+  int (*s_node)[LSTK] = reinterpret_cast<int (*)[LSTK]>(dyn);
+  unsigned* stage = dyn + 32 * LSTK;
   const int g = blockIdx.x;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
@@ -76,8 +80,8 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   unsigned* sn_mask = stage + STAGE_FAR + ncap;
   double x = 0, y = 0, z = 0;
   if (i < tc) { x = a.tx[t0 + i]; y = a.ty[t0 + i]; z = a.tz[t0 + i]; }
-  if (threadIdx.x == 0) s_node[0] = root;
   if (lane == 0) {
+    s_node[w][0] = root;
     int live = tc - 32 * w;
     s_mask[0][w] = live >= 32 ? 0xffffffffu : (live > 0 ? (1u << live) - 1u : 0u);
   }
@@ -87,11 +91,15 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   const long long fmo = MODE == MODE_FILL ? a.far_moff[g] : 0, nmo = MODE == MODE_FILL ? a.near_moff[g] : 0;
   bool overflow = false, full = false;
   __syncthreads();
-  // Two barriers per visited node: (1) after every warp has read the popped entry and
-  // published its accept / reject words, (2) after the pushes.
+  // One barrier per visited node, after every warp has published its accept / reject
+  // words.  Every warp pushes the same children onto its own stack (all threads see the
+  // same children and the same CTA-wide decision), so no warp waits for another's push;
+  // the words alternate between two buffers, so a fast warp never overwrites words a
+  // slow one is still reading (it cannot get two barriers ahead of it).
+  int par = 0;
   while (sp > 0) {
     sp--;
-    const int node = s_node[sp];
+    const int node = s_node[w][sp];
     const unsigned word = s_mask[sp][w];
     bool ok = false;
     if ((word >> lane) & 1u) {
@@ -102,10 +110,11 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
     }
     const unsigned am = __ballot_sync(0xffffffffu, ok) & word;
     const unsigned rm = word & ~am;
-    if (lane == 0) { s_am[w] = am; s_rm[w] = rm; }
+    if (lane == 0) { s_am[par][w] = am; s_rm[par][w] = rm; }
     __syncthreads();
-    const bool anyA = __ballot_sync(0xffffffffu, s_am[lane] != 0u) != 0u;
-    const bool anyR = __ballot_sync(0xffffffffu, s_rm[lane] != 0u) != 0u;
+    const bool anyA = __ballot_sync(0xffffffffu, s_am[par][lane] != 0u) != 0u;
+    const bool anyR = __ballot_sync(0xffffffffu, s_rm[par][lane] != 0u) != 0u;
+    par ^= 1;
     if (anyA) {
       if (MODE == MODE_FILL) {
         if (threadIdx.x == 0) a.far_node[fo + nf] = node;
@@ -138,14 +147,16 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
         int q = sp;
         for (int k = 7; k >= 0; k--) {
           if (ch[k] == -1) continue;
-          if (threadIdx.x == 0) s_node[q] = ch[k];
-          if (lane == 0) s_mask[q][w] = rm;
+          if (lane == 0) {
+            s_node[w][q] = ch[k];
+            s_mask[q][w] = rm;
+          }
           q++;
         }
         sp += cnt;
       }
     }
-    __syncthreads();
+    __syncwarp();  // this warp's pushes, before its next pop
   }
   if (threadIdx.x == 0 && (overflow || full)) atomicOr(a.err, overflow ? 1 : 2);
   if (MODE != MODE_FILL && lane == 0 && (fpairs || npairs)) {
@@ -223,6 +234,9 @@ __global__ void k_scan_cnt(const int* in, const int* tcount, long long* out, int
 
 void set_stage_attr() {
   ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_STAGE>), (int)STAGE_BYTES);
+  // static + dynamic shared memory of the count / fill passes is above the 48 KB default
+  ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_COUNT>), (int)STACK_BYTES);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_FILL>), (int)STACK_BYTES);
 }
 
 }  // namespace
@@ -367,7 +381,7 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   if (err & 2) {
     // some group's lists exceed the staging area or the arrays: count, scan, fill
     BIT_CUDA(cudaMemsetAsync(cnt.p, 0, 8 * sizeof(unsigned long long), s));
-    count_launch(), k_lists<MODE_COUNT><<<ng, LT, 0, s>>>(a);
+    count_launch(), k_lists<MODE_COUNT><<<ng, LT, STACK_BYTES, s>>>(a);
     count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->far_cnt.p, nullptr, L->far_off.p, ng, cnt.p + 0);
     count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->far_cnt.p, L->g_tcount.p, L->far_moff.p, ng, cnt.p + 1);
     count_launch(), k_scan_cnt<<<1, 1024, 0, s>>>(L->near_cnt.p, nullptr, L->near_off.p, ng, cnt.p + 2);
@@ -383,7 +397,7 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
     L->near_mask.ensure(c, h[3]);
     a.far_node = L->far_node.p; a.far_mask = L->far_mask.p;
     a.near_node = L->near_node.p; a.near_mask = L->near_mask.p;
-    count_launch(), k_lists<MODE_FILL><<<ng, LT, 0, s>>>(a);
+    count_launch(), k_lists<MODE_FILL><<<ng, LT, STACK_BYTES, s>>>(a);
     BIT_CHECK_LAUNCH();
   }
   L->last_ngroups = ng;
