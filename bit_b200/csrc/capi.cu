@@ -267,6 +267,11 @@ bit_status bit_ctx_destroy(bit_ctx* h) {
   c.scratch_ll.release();
   release_cache(&c);
   if (c.h_pinned) cudaFreeHost(c.h_pinned);
+  for (int i = 0; i < 2; i++) {
+    if (c.stage_ev[i]) cudaEventSynchronize(c.stage_ev[i]);
+    if (c.stage[i]) cudaFreeHost(c.stage[i]);
+    if (c.stage_ev[i]) cudaEventDestroy(c.stage_ev[i]);
+  }
   if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
   delete h;
   return BIT_OK;
@@ -337,9 +342,9 @@ static bit_status build_common(bit_ctx* h, int nsys, const int* ns, const int* m
     if (host) {
       DBuf<double> dx, dy, dz;
       dx.ensure(c, n); dy.ensure(c, n); dz.ensure(c, n);
-      BIT_CUDA(cudaMemcpyAsync(dx.p, x, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-      BIT_CUDA(cudaMemcpyAsync(dy.p, y, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-      BIT_CUDA(cudaMemcpyAsync(dz.p, z, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      copy_h2d(c, dx.p, x, n * sizeof(double));
+      copy_h2d(c, dy.p, y, n * sizeof(double));
+      copy_h2d(c, dz.p, z, n * sizeof(double));
       tree_build(t, dx.p, dy.p, dz.p);
     } else {
       tree_build(t, x, y, z);
@@ -419,7 +424,7 @@ static bit_status forest_eval(bit_tree* th, const bit_eval_params* prm, double* 
     BIT_CHECK_LAUNCH();
     ev_rec(t, EV_ALL + 1);
     if (host) {
-      BIT_CUDA(cudaMemcpyAsync(pot, out.p, t->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      copy_d2h(c, pot, out.p, t->n * sizeof(double));
       BIT_CUDA(cudaStreamSynchronize(c->stream));
       check_dev_err(c);
     }
@@ -465,10 +470,10 @@ static bit_status set_charges(bit_tree* th, const double* q, const double* w, bo
     if (host) {
       DBuf<double> dq, dw;
       dq.ensure(c, t->n);
-      BIT_CUDA(cudaMemcpyAsync(dq.p, q, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      copy_h2d(c, dq.p, q, t->n * sizeof(double));
       if (w) {
         dw.ensure(c, t->n);
-        BIT_CUDA(cudaMemcpyAsync(dw.p, w, t->n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        copy_h2d(c, dw.p, w, t->n * sizeof(double));
       }
       tree_set_charges(t, dq.p, w ? dw.p : nullptr);
       BIT_CUDA(cudaStreamSynchronize(c->stream));
@@ -558,7 +563,7 @@ bit_status bit_eval_particles(bit_tree* th, const bit_eval_params* prm, double* 
     count_launch(), k_scatter_out<<<grid_for(t->n, 256), 256, 0, c->stream>>>(t->n, t->perm.p, t->pot_sorted.p, out.p);
     BIT_CHECK_LAUNCH();
     ev_rec(t, EV_ALL + 1);
-    BIT_CUDA(cudaMemcpyAsync(pot, out.p, t->n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    copy_d2h(c, pot, out.p, t->n * sizeof(double));
     BIT_CUDA(cudaStreamSynchronize(c->stream));
     check_dev_err(c);
   });
@@ -606,10 +611,10 @@ bit_status bit_eval_points(bit_tree* th, const bit_eval_params* prm, int m, cons
     DBuf<int> dord;
     dx.ensure(c, m); dy.ensure(c, m); dz.ensure(c, m); out.ensure(c, m); dord.ensure(c, m);
     cudaStream_t s = c->stream;
-    BIT_CUDA(cudaMemcpyAsync(dx.p, sx.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dy.p, sy.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dz.p, sz.data(), m * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dord.p, ord.data(), m * sizeof(int), cudaMemcpyHostToDevice, s));
+    copy_h2d(c, dx.p, sx.data(), m * sizeof(double));
+    copy_h2d(c, dy.p, sy.data(), m * sizeof(double));
+    copy_h2d(c, dz.p, sz.data(), m * sizeof(double));
+    copy_h2d(c, dord.p, ord.data(), m * sizeof(int));
     Lists L;
     EvalPlan P;
     plan_sys(t, &P, {*prm}, 1, 0);
@@ -621,7 +626,7 @@ bit_status bit_eval_points(bit_tree* th, const bit_eval_params* prm, int m, cons
     res.ensure(c, m);
     count_launch(), k_scatter_out<<<grid_for(m, 256), 256, 0, s>>>(m, dord.p, out.p, res.p);
     BIT_CHECK_LAUNCH();
-    BIT_CUDA(cudaMemcpyAsync(pot, res.p, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    copy_d2h(c, pot, res.p, m * sizeof(double));
     BIT_CUDA(cudaStreamSynchronize(s));
     check_dev_err(c);
   });
@@ -657,9 +662,9 @@ bit_status bit_eval_force(bit_tree* th, double del, double acc, bit_precision pr
     count_launch(), k_scatter_out<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->fy_sorted.p, o.p + n);
     count_launch(), k_scatter_out<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, t->fz_sorted.p, o.p + 2LL * n);
     BIT_CHECK_LAUNCH();
-    BIT_CUDA(cudaMemcpyAsync(fx, o.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    BIT_CUDA(cudaMemcpyAsync(fy, o.p + n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    BIT_CUDA(cudaMemcpyAsync(fz, o.p + 2LL * n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    copy_d2h(c, fx, o.p, n * sizeof(double));
+    copy_d2h(c, fy, o.p + n, n * sizeof(double));
+    copy_d2h(c, fz, o.p + 2LL * n, n * sizeof(double));
     BIT_CUDA(cudaStreamSynchronize(s));
     check_dev_err(c);
   });
@@ -775,13 +780,13 @@ bit_status bit_direct_potential(bit_ctx* h, int n, const double* x, const double
     DBuf<int> dt;
     dx.ensure(c, n); dy.ensure(c, n); dz.ensure(c, n); dq.ensure(c, n);
     dt.ensure(c, m); out.ensure(c, m);
-    BIT_CUDA(cudaMemcpyAsync(dx.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dy.p, y, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dz.p, z, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dq.p, q, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    BIT_CUDA(cudaMemcpyAsync(dt.p, targets, m * sizeof(int), cudaMemcpyHostToDevice, s));
+    copy_h2d(c, dx.p, x, n * sizeof(double));
+    copy_h2d(c, dy.p, y, n * sizeof(double));
+    copy_h2d(c, dz.p, z, n * sizeof(double));
+    copy_h2d(c, dq.p, q, n * sizeof(double));
+    copy_h2d(c, dt.p, targets, m * sizeof(int));
     direct_potential(c, n, dx.p, dy.p, dz.p, dq.p, *prm, m, dt.p, out.p);
-    BIT_CUDA(cudaMemcpyAsync(pot, out.p, m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    copy_d2h(c, pot, out.p, m * sizeof(double));
     BIT_CUDA(cudaStreamSynchronize(s));
     check_dev_err(c);
   });

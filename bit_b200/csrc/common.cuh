@@ -54,6 +54,12 @@ struct Ctx;
 struct Tree;
 void* dev_alloc(Ctx* c, size_t bytes);
 void dev_free(Ctx* c, void* p);
+// Copies between caller (pageable) host arrays and device memory on the context stream;
+// large ones are staged through pinned chunks.  copy_h2d returns once the host array may be
+// reused (the device copy completes in stream order); copy_d2h returns with the data in
+// place.
+void copy_h2d(Ctx* c, void* dst, const void* src, size_t bytes);
+void copy_d2h(Ctx* c, void* dst, const void* src, size_t bytes);
 // Free cached (unused) blocks until live + cached bytes are at most `keep`.
 void ctx_trim(Ctx* c, size_t keep);
 
@@ -169,6 +175,8 @@ struct Ctx {
   std::vector<Tree*> trees;                       // trees built by this context
   long long launches = 0;                         // kernels launched by this context
   int* err_flag = nullptr;                        // device word kernels raise errors in
+  void* stage[2] = {nullptr, nullptr};            // pinned staging chunks for host copies
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   int* dev_err() {
     if (!err_flag) {
       err_flag = static_cast<int*>(dev_alloc(this, 64));

@@ -422,9 +422,9 @@ extern "C" bit_status bit_bie_solve(bit_tree* th, const bit_eval_params* prm, in
     A.nterms = nterms;
     A.diag = diag;
     A.w_s.ensure(c, n);
-    BIT_CUDA(cudaMemcpyAsync(tmp.p, w, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    copy_h2d(c, tmp.p, w, n * sizeof(double));
     count_launch(), k_gather<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, tmp.p, A.w_s.p);
-    BIT_CUDA(cudaMemcpyAsync(tmp.p, f, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    copy_h2d(c, tmp.p, f, n * sizeof(double));
     count_launch(), k_gather<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, tmp.p, b.p);
     BIT_CUDA(cudaMemsetAsync(x.p, 0, n * sizeof(double), s));
     if (!t->has_charges) {
@@ -464,7 +464,7 @@ extern "C" bit_status bit_bie_solve(bit_tree* th, const bit_eval_params* prm, in
       }
     }
     count_launch(), k_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, t->perm.p, x.p, tmp.p);
-    BIT_CUDA(cudaMemcpyAsync(sol, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    copy_d2h(c, sol, tmp.p, n * sizeof(double));
     BIT_CUDA(cudaEventRecord(e1, s));
     BIT_CUDA(cudaStreamSynchronize(s));
     float ms = 0;
@@ -500,7 +500,7 @@ extern "C" bit_status bit_gmres_dense(bit_ctx* h, int n, const double* a, const 
     y.ensure(c, n + 1);
     xd.ensure(c, n);
     me.ensure(c, 1);
-    BIT_CUDA(cudaMemcpyAsync(A.p, a, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    copy_h2d(c, A.p, a, (size_t)n * n * sizeof(double));
     BIT_CUDA(cudaMemcpyAsync(xd.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
     double bnorm = 0.0;
     for (int i = 0; i < n; i++) bnorm += b[i] * b[i];
