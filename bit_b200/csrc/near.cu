@@ -151,16 +151,20 @@ __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, 
   else p = fmaf(q * ri, ex2_approx(r2 * ri * kl2), p);
 }
 
-// This lane's pairs j = jb, jb + tpt, ... < je, two accumulators.
+// This lane's pairs j = jb, jb + tpt, ... < je, four independent accumulators.
 template <int KER, bool CHK>
 __device__ __forceinline__ void sweep_pot(const float4* fs, int j, int je, int tpt, float xt,
                                           float yt, float zt, float del, float kl2, float thr,
                                           float& p0, float& p1, bool& close) {
-  for (; j + tpt < je; j += 2 * tpt) {
+  float p2 = 0.f, p3 = 0.f;
+  for (; j + 3 * tpt < je; j += 4 * tpt) {
     acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
     acc_pot<KER, CHK>(xt, yt, zt, fs[j + tpt], del, kl2, thr, p1, close);
+    acc_pot<KER, CHK>(xt, yt, zt, fs[j + 2 * tpt], del, kl2, thr, p2, close);
+    acc_pot<KER, CHK>(xt, yt, zt, fs[j + 3 * tpt], del, kl2, thr, p3, close);
   }
-  if (j < je) acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
+  for (; j < je; j += tpt) acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
+  p1 += p2 + p3;
 }
 
 // FP64 sum of this lane's pairs with FP32 r^2 < thr (self skipped).
