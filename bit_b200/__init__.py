@@ -58,7 +58,8 @@ class Stats(C.Structure):
                 ("far_entries", C.c_longlong), ("near_entries", C.c_longlong),
                 ("batches", C.c_longlong), ("numtree", C.c_int), ("nleaves", C.c_int),
                 ("depth", C.c_int), ("nterms", C.c_int), ("far_launches", C.c_int),
-                ("near_launches", C.c_int), ("list_fallback", C.c_int)]
+                ("near_launches", C.c_int), ("list_fallback", C.c_int),
+                ("lists_shared", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -179,6 +179,7 @@ void eval_particles_sorted(Tree* t, const std::vector<bit_eval_params>& prm) {
   t->stats.far_launches = (int)t->pplan.far_classes.size();
   t->stats.near_launches = (int)t->pplan.near_classes.size();
   t->stats.list_fallback = t->plists.fallback ? 1 : 0;
+  t->stats.lists_shared = t->plists.shared ? 1 : 0;
 }
 
 uint64_t spread3(uint64_t v) {
@@ -816,7 +817,7 @@ bit_status bit_tree_stats(const bit_tree* th, bit_stats* st) {
     bit_stats s = t->stats;
     s.t_build = ev_sec(t, EV_BUILD);
     s.t_moments = ev_sec(t, EV_MOM);
-    s.t_lists = ev_sec(t, EV_LIST);
+    s.t_lists = t->lists_built ? ev_sec(t, EV_LIST) : 0.0;  // 0: the lists were reused
     s.t_far = ev_sec(t, EV_FAR);
     s.t_near = ev_sec(t, EV_NEAR);
     s.t_total = ev_sec(t, EV_ALL);

@@ -134,6 +134,9 @@ struct ListKey {
     return acc == o.acc && add_del == o.add_del && sub_del == o.sub_del &&
            points == o.points && group == o.group && gen == o.gen && sysmac == o.sysmac;
   }
+  bool same_mac(const ListKey& o) const {
+    return acc == o.acc && add_del == o.add_del && sub_del == o.sub_del && sysmac == o.sysmac;
+  }
 };
 
 struct Lists {
@@ -156,6 +159,12 @@ struct Lists {
   int last_ngroups = 0;                     // groups and totals of the last build (sizing)
   unsigned long long last_totals[4] = {0, 0, 0, 0};
   bool fallback = false;                    // the last build used count, scan and fill
+  // The lists also serve alt_key when alt_valid: the build checked that MAC at every
+  // (target, node) it visited and no decision differed, so that MAC's own traversal
+  // would have visited the same nodes and emitted the same entries.
+  ListKey alt_key;
+  bool alt_valid = false;
+  bool shared = false;  // the last evaluation used them through alt_key
 };
 
 struct Ctx {
@@ -166,6 +175,7 @@ struct Ctx {
   std::string last_error;
   int num_sms = 148;
   int group_targets = 0;  // leaves packed into groups of up to this many targets (0: off)
+  ListKey mac_hint;       // MAC of the last particle-target evaluation (acc < 0: none)
   // small device scratch for flags / counters
   DBuf<long long> scratch_ll;
   long long* h_pinned = nullptr;  // pinned host staging for small read-backs (64 entries)
@@ -214,6 +224,7 @@ struct Tree {
   bool has_charges = false, has_weights = false;
   int nterms = 0;
   bool has_moments = false;
+  bool lists_built = false;  // the last evaluation built its particle-target lists
   DBuf<double> mom64;
   DBuf<float> mom32;
   std::vector<long long> h_mom_off;  // first moment of each node (systems may differ in nterms)
@@ -245,8 +256,10 @@ void tree_sync_host(Tree* t);
 void tree_set_charges(Tree* t, const double* dq, const double* dw);
 void tree_moments(Tree* t, int nterms);
 void tree_moments_sys(Tree* t, const std::vector<int>& nterms_per_system);
+// alt (single-system keys only, or nullptr): a second MAC checked during the traversal.
 void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const double* tx,
-                 const double* ty, const double* tz, const SysEval* d_sys);
+                 const double* ty, const double* tz, const SysEval* d_sys,
+                 const ListKey* alt = nullptr);
 // Evaluation plan of one call: per-system parameters on the device and the groups of
 // each launch class, ordered by class and then by decreasing work.
 void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,

@@ -17,6 +17,12 @@
 // The lists are written in place, into arrays sized from an estimate.  A group whose
 // entries do not fit its staging area, or whose reservation runs past the arrays, makes
 // the whole build fall back to a count pass, a prefix sum and a fill pass.
+//
+// Optionally the walk also evaluates a second MAC (another kernel's parameters, e.g. the
+// Coulomb test's (r^2 + del) - del next to the screened r^2 - mac_del) at every (target,
+// node) it visits.  If no decision differs, that MAC's own walk would take the same path
+// and emit the same entries, so the lists serve both MACs bit for bit; one differing
+// decision anywhere and they serve only their own.
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -51,9 +57,17 @@ struct ListArgs {
   unsigned *far_mask, *near_mask;
   unsigned long long* totals;  // far entries, far words, near entries, near words
   unsigned long long* pairs;   // far pairs, near pairs
-  int* err;                    // 1: stack overflow, 2: staging or arena overflow
+  int* err;                    // 1: stack overflow, 2: staging or arena overflow,
+                               // 4: the alternative MAC disagreed somewhere
   unsigned long long cap[4];   // MODE_STAGE: room in the four output arrays
+  int has_alt;                 // also evaluate a second MAC and compare its decisions
+  double alt_acc, alt_add, alt_sub;
 };
+
+// The alternative MAC's decision for squared distance s and node sqradius w.
+__device__ __forceinline__ bool alt_ok(const ListArgs& a, double s, double w) {
+  return w < dmul(a.alt_acc, dsub(dadd(s, a.alt_add), a.alt_sub));
+}
 
 template <int MODE>
 __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
@@ -89,7 +103,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   long long nf = 0, nn = 0, fpairs = 0, npairs = 0;
   const long long fo = MODE == MODE_FILL ? a.far_off[g] : 0, no = MODE == MODE_FILL ? a.near_off[g] : 0;
   const long long fmo = MODE == MODE_FILL ? a.far_moff[g] : 0, nmo = MODE == MODE_FILL ? a.near_moff[g] : 0;
-  bool overflow = false, full = false;
+  bool overflow = false, full = false, differ = false;
   __syncthreads();
   // One barrier per visited node, after every warp has published its accept / reject
   // words.  Every warp pushes the same children onto its own stack (all threads see the
@@ -107,6 +121,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
       double dx = dsub(x, c.x), dy = dsub(y, c.y), dz = dsub(z, c.z);
       double s = dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
       ok = c.w < dmul(macc, dsub(dadd(s, madd), msub));
+      if (a.has_alt) differ |= ok != alt_ok(a, s, c.w);
     }
     const unsigned am = __ballot_sync(0xffffffffu, ok) & word;
     const unsigned rm = word & ~am;
@@ -159,6 +174,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
     __syncwarp();  // this warp's pushes, before its next pop
   }
   if (threadIdx.x == 0 && (overflow || full)) atomicOr(a.err, overflow ? 1 : 2);
+  if (a.has_alt && __any_sync(0xffffffffu, differ) && lane == 0) atomicOr(a.err, 4);
   if (MODE != MODE_FILL && lane == 0 && (fpairs || npairs)) {
     atomicAdd(&a.pairs[0], (unsigned long long)fpairs);
     atomicAdd(&a.pairs[1], (unsigned long long)npairs);
@@ -297,7 +313,10 @@ static void particle_groups(Tree* t, int G, std::vector<int>& ts, std::vector<in
 }
 
 void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const double* tx,
-                 const double* ty, const double* tz, const SysEval* d_sys) {
+                 const double* ty, const double* tz, const SysEval* d_sys, const ListKey* alt) {
+  if (alt && (!alt->sysmac.empty() || !key.sysmac.empty() || t->nsys != 1)) alt = nullptr;
+  L->valid = false;  // the arrays are rewritten below; valid again once the build completes
+  L->alt_valid = false;
   Ctx* c = t->ctx;
   cudaStream_t s = c->stream;
   std::vector<int> ts, tc, gsys;
@@ -344,6 +363,12 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   a.totals = cnt.p;
   a.pairs = cnt.p + 4;
   a.err = reinterpret_cast<int*>(cnt.p + 6);
+  if (alt) {
+    a.has_alt = 1;
+    a.alt_acc = alt->acc;
+    a.alt_add = alt->add_del;
+    a.alt_sub = alt->sub_del;
+  }
   // Single pass straight into the lists, sized from an estimate: the last build's totals
   // scaled by the group count, else a per-group allowance.  A group that does not fit
   // its staging area or the arrays makes the build fall back to count, scan and fill.
@@ -390,7 +415,8 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
     BIT_CUDA(cudaMemcpyAsync(hf.data(), L->far_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaMemcpyAsync(hn.data(), L->near_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
-    if ((int)(h[6] & 0xffffffffu) & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded");
+    err = (int)(h[6] & 0xffffffffu);  // this pass walked every group to the end
+    if (err & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded");
     L->far_node.ensure(c, h[0]);
     L->far_mask.ensure(c, h[1]);
     L->near_node.ensure(c, h[2]);
@@ -419,6 +445,13 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   L->key = key;
   L->valid = true;
   L->version++;
+  L->alt_valid = alt && !(err & 4);
+  if (L->alt_valid) {
+    L->alt_key = key;
+    L->alt_key.acc = alt->acc;
+    L->alt_key.add_del = alt->add_del;
+    L->alt_key.sub_del = alt->sub_del;
+  }
 }
 
 }  // namespace bit

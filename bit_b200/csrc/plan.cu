@@ -186,15 +186,28 @@ void plan_classes(Tree* t, Lists* L, EvalPlan* P) {
   P->class_key = key;
 }
 
+// Particle-target lists for this call's MAC: the tree's own lists when they were built
+// for it, or built for another MAC and checked against this one; else a new build, which
+// also checks the context's previous MAC (an evaluation that alternates two kernels on
+// each new tree then walks the tree once per tree when their decisions agree).
 void prepare_particles(Tree* t, const std::vector<bit_eval_params>& prm, int force) {
   plan_sys(t, &t->pplan, prm, 0, force);
   const ListKey k = plan_key(t, t->pplan, 0);
-  if (!(t->plists.valid && t->plists.key == k)) {
-    if (t->ev[4]) BIT_CUDA(cudaEventRecord(t->ev[4], t->ctx->stream));
-    build_lists(t, &t->plists, k, t->n, t->sx.p, t->sy.p, t->sz.p, t->pplan.sys.p);
-    if (t->ev[5]) BIT_CUDA(cudaEventRecord(t->ev[5], t->ctx->stream));
+  Lists& L = t->plists;
+  Ctx* c = t->ctx;
+  const bool own = L.valid && L.key == k;
+  const bool shared = !own && L.valid && L.alt_valid && L.alt_key == k;
+  t->lists_built = !own && !shared;
+  if (t->lists_built) {
+    const ListKey alt = c->mac_hint;
+    const bool check = alt.acc >= 0 && !alt.same_mac(k);
+    if (t->ev[4]) BIT_CUDA(cudaEventRecord(t->ev[4], c->stream));
+    build_lists(t, &L, k, t->n, t->sx.p, t->sy.p, t->sz.p, t->pplan.sys.p, check ? &alt : nullptr);
+    if (t->ev[5]) BIT_CUDA(cudaEventRecord(t->ev[5], c->stream));
   }
-  plan_classes(t, &t->plists, &t->pplan);
+  L.shared = shared;
+  c->mac_hint = k;
+  plan_classes(t, &L, &t->pplan);
 }
 
 }  // namespace bit

@@ -772,6 +772,7 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
   t->gen++;
   t->has_moments = false;
   t->plists.valid = false;
+  t->plists.alt_valid = false;
 }
 
 template struct DBuf<signed char>;

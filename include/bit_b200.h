@@ -88,6 +88,10 @@ typedef struct {
   int numtree, nleaves, depth, nterms;
   int far_launches, near_launches;
   int list_fallback; /* the last list build used the count / scan / fill passes */
+  int lists_shared;  /* the last evaluation reused lists built for another MAC (the
+                        context's previous one): every acceptance decision of that
+                        traversal was also checked under this MAC and agreed, so the
+                        lists are the ones this MAC's own traversal would build */
 } bit_stats;
 
 const char* bit_status_string(bit_status s);

@@ -252,3 +252,75 @@ def test_mixed_coincident_duplicates_follow_the_fp64_rules(ctx):
     p32 = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.MIXED, del_=0.0, acc=0.5))
     assert np.all(np.isfinite(p64)) and np.all(np.isfinite(p32))
     assert workloads.rel_l2(p32, p64) < TOL_MIXED
+
+
+def shared_steps(c, x, y, z, q, prec, ps, pc, steps=2):
+    """The benchmark's step on a fresh tree each time: screened, then Coulomb."""
+    import bit_b200 as B
+    out = []
+    for _ in range(steps):
+        t = c.treemake(x, y, z, 1000)
+        t.treemoments(q, 9)
+        s_pot = t.evaluate(B.params(B.SCREENED, B.CONSISTENT, prec, **ps))
+        c_pot = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, prec, **pc))
+        out.append((s_pot, c_pot, t.stats()))
+        t.treeempty()
+    return out
+
+
+def own_lists(c, x, y, z, q, prm):
+    t = c.treemake(x, y, z, 1000)
+    t.treemoments(q, 9)
+    pot = t.evaluate(prm)
+    assert t.stats()["lists_shared"] == 0
+    t.treeempty()
+    return pot
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_lists_shared_between_kernels_match_their_own(orc, prec):
+    """From the second tree on, the screened build also checks the Coulomb MAC (the
+    context's previous one); every decision agrees, so the Coulomb evaluation reuses those
+    lists. Its potential is bit-identical to a context that walks the tree for Coulomb
+    itself, and the FP64 one matches the oracle."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    pr = B.FP64 if prec == "fp64" else B.MIXED
+    x, y, z, q = workloads.clustered_blobs(50000, seed=21)
+    ps, pc = dict(kappa=1.0, acc=0.7), dict(del_=0.005, acc=0.7)
+    a, b = B.Context(), B.Context()
+    try:
+        steps = shared_steps(a, x, y, z, q, pr, ps, pc)
+        assert steps[0][2]["lists_shared"] == 0
+        s_pot, c_pot, st = steps[1]
+        assert st["lists_shared"] == 1 and st["t_lists"] == 0.0
+        np.testing.assert_array_equal(c_pot, own_lists(b, x, y, z, q, B.params(B.COULOMB, B.CONSISTENT, pr, **pc)))
+        np.testing.assert_array_equal(s_pot, own_lists(b, x, y, z, q, B.params(B.SCREENED, B.CONSISTENT, pr, **ps)))
+        np.testing.assert_array_equal(c_pot, steps[0][1])
+        if pr == B.FP64:
+            T = orc.Tree(x, y, z, 1000)
+            T.compute_moments(q, 9)
+            ref = T.evaluate(orc.params(orc.COULOMB, orc.MODE_CONSISTENT, del_=0.005, acc=0.7))
+            assert rel(c_pot, ref) < TOL64
+    finally:
+        a.close()
+        b.close()
+
+
+@pytest.mark.parametrize("ps", [dict(kappa=1.0, acc=0.5), dict(kappa=1.0, acc=0.7, mac_del=0.01)])
+def test_lists_not_shared_when_the_macs_decide_differently(ps):
+    """A different acc, or the screened MAC's r^2 - mac_del: some decision differs, so the
+    Coulomb evaluation walks the tree itself and gets exactly its own lists."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.clustered_blobs(50000, seed=22)
+    pc = dict(del_=0.01, acc=0.7)
+    a, b = B.Context(), B.Context()
+    try:
+        for s_pot, c_pot, st in shared_steps(a, x, y, z, q, B.FP64, ps, pc):
+            assert st["lists_shared"] == 0 and st["t_lists"] > 0
+        np.testing.assert_array_equal(c_pot, own_lists(b, x, y, z, q, B.params(B.COULOMB, B.CONSISTENT, B.FP64, **pc)))
+        np.testing.assert_array_equal(s_pot, own_lists(b, x, y, z, q, B.params(B.SCREENED, B.CONSISTENT, B.FP64, **ps)))
+    finally:
+        a.close()
+        b.close()
