@@ -214,7 +214,8 @@ def run_bit(args):
     phases = {}
     for name, st in (("screened", st_s), ("coulomb", st_c)):
         phases[name] = {k: st[k] for k in ("t_far", "t_near", "t_lists", "far_pairs", "near_pairs",
-                                           "far_entries", "near_entries", "batches")}
+                                           "far_entries", "near_entries", "batches",
+                                           "lists_shared")}
     phases["build_s"] = st_s["t_build"]
     phases["moments_s"] = st_s["t_moments"]
     phases["numtree"] = st_s["numtree"]
@@ -469,18 +470,20 @@ def serve(reqs, arrivals, prec, slots, budget):
 
 
 def run_serving(ctx, args):
-    """Serving stream: open-loop Poisson arrivals of the request mix, admitted by a 150 GB
-    HBM budget into a continuous-batching server (mixed precision, several slots), next to
-    the plain FP64 GPU path serving one request at a time on the same arrivals."""
+    """Serving stream: open-loop Poisson arrivals of the request mix at 80% of the mixed
+    server's measured capacity, admitted by a 150 GB HBM budget into a continuous-batching
+    server (mixed precision, several slots), next to the plain FP64 GPU path serving one
+    request at a time on the same arrivals."""
     import bit_b200 as B
     from bit_b200 import workloads
     reqs = serving_requests(args.serve_requests, seed=5, ctx=ctx)
     budget = 150 * 10 ** 9
-    # arrival rate: 1.5x what one mixed slot serves back to back (calibrated on 12 requests)
-    cal, _ = serve(reqs[:12], [0.0] * 12, B.MIXED, 1, budget)
-    _, cal_stats = serve(reqs[:12], [0.0] * 12, B.MIXED, 1, budget)
-    service = 1.0 / cal_stats["requests_per_s"]
-    rate = 1.5 / service
+    # arrival rate: 80% of the mixed server's capacity, measured closed-loop (every request
+    # queued at t = 0) on the whole request set after a warm-up on its first 12 requests
+    serve(reqs[:12], [0.0] * 12, B.MIXED, args.serve_slots, budget)
+    _, cap = serve(reqs, [0.0] * len(reqs), B.MIXED, args.serve_slots, budget)
+    load = 0.8
+    rate = load * cap["requests_per_s"]
     rng = np.random.default_rng(6)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
     res32, mixed = serve(reqs, arrivals, B.MIXED, args.serve_slots, budget)
@@ -497,9 +500,12 @@ def run_serving(ctx, args):
         derr.append(workloads.rel_l2(res32[i][tg], ctx.direct(x, y, z, q, p, tg)))
     kinds = [r["kind"] for r in reqs]
     return {"workload": f"{len(reqs)} requests, Poisson arrivals at {rate:.1f}/s "
+                        f"({load:.0%} of the mixed server's closed-loop capacity, "
+                        f"{cap['requests_per_s']:.1f}/s) "
                         f"({kinds.count('eval')} evaluate: N lognormal median 2e4 in [1e3, 1e6], "
                         f"blobs, p in {{4,6,8}}, theta 0.6; {kinds.count('solve')} solves: "
                         "icosphere level 4..7, p=6, theta=0.5, GMRES(50) to 1e-8), 150 GB budget",
+            "offered_load": load, "mixed_closed_loop_requests_per_s": cap["requests_per_s"],
             "mixed_continuous_batching": mixed, "fp64_one_at_a_time": plain,
             "throughput_ratio": mixed["requests_per_s"] / plain["requests_per_s"],
             "p99_ratio": plain["p99_latency_s"] / mixed["p99_latency_s"],
