@@ -263,6 +263,21 @@ int vel_update(int npart, PARTICLE* part, double dt) {
   return 0;
 }
 
+// output_potential (src/tree3d.cpp:4918-4937) through bit_write_potential, which writes
+// the reference's bytes; a file that cannot be written is reported by
+// bit_tree3d_last_error() (the reference's ofstream fails silently).
+void output_potential(int npart, PARTICLE* part, double* pot, std::string filename) {
+  std::vector<double> x(npart), y(npart), z(npart);
+  for (int i = 0; i < npart; i++) {
+    x[i] = part[i].x;
+    y[i] = part[i].y;
+    z[i] = part[i].z;
+  }
+  const bit_status st = bit_write_potential(filename.c_str(), npart, x.data(), y.data(),
+                                            z.data(), pot);
+  if (st != BIT_OK) g_err = "output_potential: cannot write " + filename;
+}
+
 int loc_update(int npart, PARTICLE* part, double dt) {
   for (int i = 0; i < npart; i++) {
     part[i].x += dt * part[i].u;

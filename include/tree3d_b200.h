@@ -24,6 +24,7 @@
 #define TREE3D_B200_H
 
 #include <cstdio>
+#include <string>
 
 const int MAXPART = 1000000;  /* src/constants.h:8  */
 const int NUMCHILD = 8;       /* src/constants.h:9  */
@@ -82,6 +83,8 @@ void freespace_particles_tree(int npart, PARTICLE* part, int nterms, double acc,
 /* src/tree3d.cpp:4842-4850 and :4880-4888: explicit velocity and position updates */
 int vel_update(int npart, PARTICLE* part, double dt);
 int loc_update(int npart, PARTICLE* part, double dt);
+/* src/tree3d.cpp:4918-4937: "i\tx\ty\tz\tpot" per particle, 14 significant digits */
+void output_potential(int npart, PARTICLE* part, double* pot, std::string filename);
 
 /* src/solver.h:31-315: dense GMRES, on the device */
 class solver {
