@@ -250,6 +250,16 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 
+// FP32 moments are stored normalised: M_v / h^|v| with h = 2^e the smallest power of two
+// above the cluster radius (sqrt(sqradius)), so the scaling is exact (exponent shifts) and
+// the FP32 far field works with (h/r)^n, which stays bounded at any scale.  Both the
+// moment pass and the far kernels call this on the same FP64 sqradius.
+__device__ __forceinline__ int mom32_scale_exp(double sqradius) {
+  if (!(sqradius > 0.0) || !(sqradius < 1e300)) return 0;
+  const int e = ilogb(sqrt(sqradius)) + 1;
+  return e < -100 ? -100 : (e > 100 ? 100 : e);
+}
+
 // ---- entry points implemented in the .cu files -----------------------------------------
 void tree_build(Tree* t, const double* dx, const double* dy, const double* dz);
 void tree_sync_host(Tree* t);

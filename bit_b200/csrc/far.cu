@@ -147,14 +147,21 @@ __global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArg
     T* M = msb + w * TP;
     const T* mn = mom + a.mom_off[node];
     for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
+    // FP32: moments normalised by h^|v|, h = 2^e; the scaled recurrences take h
+    const T h = sizeof(T) == 4 ? (T)ldexpf(1.f, mom32_scale_exp(c.w)) : T(1);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
       const int i = tl[r];
       const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
       const T r2 = dx * dx + dy * dy + dz * dz + tadd;
       T v;
-      if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb<T>(dx, dy, dz, r2, M);
-      else v = FarField<NT>::template screened<T>(dx, dy, dz, r2, tk, M);
+      if constexpr (sizeof(T) == 4) {
+        if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb_s<T>(dx, dy, dz, r2, h, M);
+        else v = FarField<NT>::template screened_s<T>(dx, dy, dz, r2, tk, h, M);
+      } else {
+        if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb<T>(dx, dy, dz, r2, M);
+        else v = FarField<NT>::template screened<T>(dx, dy, dz, r2, tk, M);
+      }
       WarpAcc<T>::add(row, i, v);
     }
     __syncwarp();
@@ -201,7 +208,18 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
     const double4 c = a.nodec[node];
     T* M = msb + w * TP;
     const T* mn = mom + a.mom_off[node];
-    for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
+    // FP32 moments are stored normalised by h^|v| (h = 2^e): undo it exactly here, since
+    // the force recurrence takes the moments themselves
+    const int se = sizeof(T) == 4 ? mom32_scale_exp(c.w) : 0;
+    for (int k = lane; k < TP; k += 32) {
+      T m = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
+      if constexpr (sizeof(T) == 4) {
+        int d = 0;  // degree of shell-order index k
+        while (num_terms(d + 1) <= k) d++;
+        m = ldexpf(m, se * d);
+      }
+      M[k] = m;
+    }
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
       const int i = tl[r];

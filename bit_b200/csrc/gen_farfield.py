@@ -196,6 +196,163 @@ def gen_screened(nt):
     return L
 
 
+# ------------------------------------------------------- scaled forms (FP32 path)
+# The same recurrences on scaled coefficients: with R the (regularised) distance, u = d/R
+# the unit vector and n = |v|, the Coulomb b~_v = b_v R^(n+1), the screened a~_v = a_v R^(n+1)
+# and c~_v = c_v R^n, rho = kappa R.  Substituting d = R u and fac = R^-2 into each pattern
+# of the reference's recurrence removes the fac multiply (e.g. the screened generic pattern
+# a~_v = u_f a~_{v-f} + 2 u_a a~_{v-a} - a~_{v-2a} + rho u_f c~_{v-f}).  The moments come
+# normalised by h^n (h = 2^e above the cluster radius), so the potential is
+# sum_n S_n (h/R)^n / R with S_n the dot product of shell n: q_n = (h/R)^n / R <= 1/R at
+# any scale, where the unscaled coefficients (~R^-(n+1)) overflow FP32 for R below ~1e-4.
+# Subtracted terms start each fma chain, so they cost no separate instruction.
+
+
+def _chain(start, terms):
+    """fma_t chain: terms [(mult, var)] added in order onto `start` (None: the first term
+    is a plain product)."""
+    e = start
+    for m, v in terms:
+        e = f"{m}*{v}" if e is None else f"fma_t({m}, {v}, {e})"
+    return e
+
+
+def _neg_sum(vs):
+    return None if not vs else ("-" + vs[0] if len(vs) == 1 else "-(" + " + ".join(vs) + ")")
+
+
+class ShellSum:
+    """Per-shell dot products folded into s with the factor q_n = (h/R)^n / R."""
+
+    def __init__(self, L, mi):
+        self.L, self.mi, self.ml, self.deg, self.first = L, mi, MomentLoads(), 0, True
+
+    def add(self, v, var):
+        L = self.L
+        d = sum(v)
+        if d != self.deg:
+            self.flush()
+            self.deg, self.first = d, True
+        m = self.ml.get(L, self.mi[v])
+        if self.first:
+            L.append(f"  S = {m} * {var};")
+            self.first = False
+        else:
+            L.append(f"  S = fma_t({m}, {var}, S);")
+
+    def flush(self):
+        if self.deg == 0:
+            self.L.append("  T s = S * q;")
+        else:
+            self.L.append("  q = q * eta;")
+            self.L.append("  s = fma_t(S, q, s);")
+
+    def done(self):
+        self.flush()
+        self.L.append("  return s;")
+
+
+def coul_scaled_expr(v):
+    b = lambda w: "E" if w == (0, 0, 0) else name("B", w)
+    U = lambda a: "u" + AX[a]
+    U2 = lambda a: "u" + AX[a] + "2"
+    nz, n1, ax = classify(v)
+    if nz == 2:
+        u, k = ax[0], v[ax[0]]
+        if k == 1:
+            return U(u)
+        ik = 1.0 / k
+        return f"fma_t({U(u)}, {lit(2.0 - ik)}*{b(sub(v, u, 1))}, -({lit(1 - ik)}*{b(sub(v, u, 2))}))"
+    if nz == 1 and n1 == 2:
+        u, w = ax
+        return _chain(None, [(U(u), b(sub(v, u, 1))), (U2(w), b(sub(v, w, 1)))])
+    if nz == 1 and n1 == 0:
+        u, w = ax
+        ii = 1.0 / v[u]
+        e = f"fma_t({lit(-(1 - ii))}, {b(sub(v, u, 2))}, -{b(sub(v, w, 2))})"
+        e = _chain(e, [(U2(w), b(sub(v, w, 1)))])
+        return f"fma_t({U(u)}, {lit(2.0 - ii)}*{b(sub(v, u, 1))}, {e})"
+    if n1 >= 1:
+        f = next(a for a in range(3) if v[a] == 1)
+        subs = [b(sub(v, a, 2)) for a in range(3) if a != f and v[a] >= 2]
+        ns = _neg_sum(subs)
+        e = f"{U(f)}*{b(sub(v, f, 1))}" if ns is None else f"fma_t({U(f)}, {b(sub(v, f, 1))}, {ns})"
+        return _chain(e, [(U2(a), b(sub(v, a, 1))) for a in range(3) if a != f and v[a] > 0])
+    ii = 1.0 / v[0]
+    e = f"fma_t({lit(-(1.0 - ii))}, {b(sub(v, 0, 2))}, -({b(sub(v, 1, 2))} + {b(sub(v, 2, 2))}))"
+    e = _chain(e, [("uy2", b(sub(v, 1, 1))), ("uz2", b(sub(v, 2, 1)))])
+    return f"fma_t(ux, {lit(2.0 - ii)}*{b(sub(v, 0, 1))}, {e})"
+
+
+def gen_coulomb_scaled(nt):
+    mi = shell_index(nt)
+    L = ["  const T rinv = rsqrt_t(rs);",
+         "  const T ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;",
+         "  const T ux2 = ux + ux, uy2 = uy + uy, uz2 = uz + uz;",
+         "  const T eta = h * rinv;",
+         "  const T E = T(1);",
+         "  T q = rinv, S;"]
+    sh = ShellSum(L, mi)
+    for v in shells(nt - 1):
+        if v != (0, 0, 0):
+            L.append(f"  const T {name('B', v)} = {coul_scaled_expr(v)};")
+        sh.add(v, "E" if v == (0, 0, 0) else name("B", v))
+    sh.done()
+    return L
+
+
+def scr_scaled_expr(v):
+    A = lambda w: "E" if w == (0, 0, 0) else name("A", w)
+    C = lambda w: "E" if w == (0, 0, 0) else name("C", w)
+    U = lambda a: "u" + AX[a]
+    U2 = lambda a: "u" + AX[a] + "2"
+    K = lambda a: "ku" + AX[a]
+    nz, n1, ax = classify(v)
+    if nz == 2 and n1 == 1:
+        u = ax[0]
+        return f"{K(u)}*E", f"{U(u)}*E1"
+    if n1 == 0:
+        u = ax[0]
+        i = v[u]
+        cf1, cf2, cf3 = 1.0 / i, 1.0 - 1.0 / (2.0 * i), 1.0 - 1.0 / i
+        cexp = f"{lit(cf1)}*fma_t({K(u)}, {A(sub(v, u, 1))}, -(rho*{A(sub(v, u, 2))}))"
+        ns = _neg_sum([A(sub(v, a, 2)) for a in ax[1:]])
+        e = f"{lit(-cf3)}*{A(sub(v, u, 2))}" if ns is None else f"fma_t({lit(-cf3)}, {A(sub(v, u, 2))}, {ns})"
+        e = _chain(e, [(U2(a), A(sub(v, a, 1))) for a in ax[1:]])
+        e = f"fma_t({U(u)}, {lit(2.0 * cf2)}*{A(sub(v, u, 1))}, {e})"
+        e = f"fma_t({lit(cf1)}, fma_t({K(u)}, {C(sub(v, u, 1))}, -(rho*{C(sub(v, u, 2))})), {e})"
+        return cexp, e
+    f = next(a for a in range(3) if v[a] == 1)
+    cexp = f"{K(f)}*{A(sub(v, f, 1))}"
+    ns = _neg_sum([A(sub(v, a, 2)) for a in range(3) if a != f and v[a] >= 2])
+    e = f"{U(f)}*{A(sub(v, f, 1))}" if ns is None else f"fma_t({U(f)}, {A(sub(v, f, 1))}, {ns})"
+    e = _chain(e, [(U2(a), A(sub(v, a, 1))) for a in range(3) if a != f and v[a] > 0])
+    e = _chain(e, [(K(f), C(sub(v, f, 1)))])
+    return cexp, e
+
+
+def gen_screened_scaled(nt):
+    mi = shell_index(nt)
+    L = ["  const T rinv = rsqrt_t(dist2);",
+         "  const T ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;",
+         "  const T ux2 = ux + ux, uy2 = uy + uy, uz2 = uz + uz;",
+         "  const T rho = kappa * (dist2 * rinv);",
+         "  const T kux = rho * ux, kuy = rho * uy, kuz = rho * uz;",
+         "  const T eta = h * rinv;",
+         "  const T E = exp_t(-rho);",
+         "  const T E1 = fma_t(rho, E, E);",
+         "  T q = rinv, S;"]
+    sh = ShellSum(L, mi)
+    for v in shells(nt - 1):
+        if v != (0, 0, 0):
+            cexp, aexp = scr_scaled_expr(v)
+            L.append(f"  const T {name('C', v)} = {cexp};")
+            L.append(f"  const T {name('A', v)} = {aexp};")
+        sh.add(v, "E" if v == (0, 0, 0) else name("A", v))
+    sh.done()
+    return L
+
+
 # ---------------------------------------------------------------------------- force
 def force_expr(v):
     b = lambda w: name("b", w)
@@ -313,6 +470,15 @@ def main(out):
         parts.append("  template <class T> static __device__ __forceinline__ T screened("
                      "T dx, T dy, T dz, T dist2, T kappa, const T* __restrict__ M) {")
         parts += gen_screened(nt)
+        parts.append("  }")
+        parts.append("  // scaled forms for normalised moments (M_v / h^|v|), used by the FP32 path")
+        parts.append("  template <class T> static __device__ __forceinline__ T coulomb_s("
+                     "T dx, T dy, T dz, T rs, T h, const T* __restrict__ M) {")
+        parts += gen_coulomb_scaled(nt)
+        parts.append("  }")
+        parts.append("  template <class T> static __device__ __forceinline__ T screened_s("
+                     "T dx, T dy, T dz, T dist2, T kappa, T h, const T* __restrict__ M) {")
+        parts += gen_screened_scaled(nt)
         parts.append("  }")
         parts.append("  template <class T> static __device__ __forceinline__ void force("
                      "T dx, T dy, T dz, T rs, const T* __restrict__ M, T& fx, T& fy, T& fz) {")

@@ -114,19 +114,31 @@ __global__ void __launch_bounds__(MTB) k_moments_partial(const int4* chunks, con
     part[(long long)ck.w * TMAX + t] = s_part[t] + s_part[TMAX + t];
 }
 
-// Per node: the sum of its chunks' partials, in chunk order.
+// Degree i + j + k of canonical moment index t (i outer, j, k inner, i + j + k < nt).
+__device__ int canon_degree(int t, int nt) {
+  int i = 0, j = 0;
+  for (; t >= (nt - i) * (nt - i + 1) / 2; i++) t -= (nt - i) * (nt - i + 1) / 2;
+  for (; t >= nt - i - j; j++) t -= nt - i - j;
+  return i + j + t;
+}
+
+// Per node: the sum of its chunks' partials, in chunk order.  The FP32 copy is normalised
+// by h^degree, h = 2^mom32_scale_exp(sqradius) (exact: an exponent shift).
 __global__ void k_moments_reduce(const int* node_c0, const int* node_c1, const int* node_T,
-                                 const long long* mom_off, const double* part, double* mom64,
-                                 float* mom32) {
+                                 const long long* mom_off, const double4* nodec,
+                                 const double* part, double* mom64, float* mom32) {
   constexpr int TMAX = num_terms(kNtermsMax);
   const int node = blockIdx.x;
   const int c0 = node_c0[node], c1 = node_c1[node], T = node_T[node];
   const long long o = mom_off[node];
+  int nt = 1;
+  while (num_terms(nt) < T) nt++;
+  const int e = mom32_scale_exp(nodec[node].w);
   for (int t = threadIdx.x; t < T; t += blockDim.x) {
     double s = 0.0;
     for (int c = c0; c < c1; c++) s += part[(long long)c * TMAX + t];
     mom64[o + t] = s;
-    mom32[o + t] = (float)s;
+    mom32[o + t] = (float)ldexp(s, -e * canon_degree(t, nt));
   }
 }
 
@@ -246,8 +258,9 @@ void tree_moments_sys(Tree* t, const std::vector<int>& nt_sys) {
     }
   }
   count_launch(), k_moments_reduce<<<t->numtree, 256, 0, s>>>(t->mplan_c0.p, t->mplan_c1.p, t->mplan_T.p,
-                                                              t->mom_off.p, t->mplan_part.p,
-                                                              t->mom64.p, t->mom32.p);
+                                                              t->mom_off.p, t->nodec.p,
+                                                              t->mplan_part.p, t->mom64.p,
+                                                              t->mom32.p);
   BIT_CHECK_LAUNCH();
   int mx = 0;
   for (int v : nt_sys) mx = std::max(mx, v);

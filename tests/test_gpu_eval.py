@@ -254,6 +254,31 @@ def test_mixed_coincident_duplicates_follow_the_fp64_rules(ctx):
     assert workloads.rel_l2(p32, p64) < TOL_MIXED
 
 
+@pytest.mark.parametrize("kern", ["screened", "coulomb"])
+def test_mixed_far_field_at_tiny_scales(ctx, kern):
+    """Four tight clusters (sigma 1e-6, about 2e-5 apart) with small leaves: far-field
+    clusters are accepted at r ~ 1e-6..1e-5, where coefficients of size r^-(n+1) exceed
+    the FP32 range.  The FP32 far field works on moments normalised by the cluster size,
+    with terms (h/r)^n / r, so the mixed path stays finite and within 1e-6 of FP64."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    rng = np.random.default_rng(12)
+    centres = np.array([[0.5, 0.5, 0.5], [0.5 + 2e-5, 0.5, 0.5], [0.5, 0.5 + 2e-5, 0.5],
+                        [0.5, 0.5, 0.5 + 3e-5]])
+    p = np.concatenate([c + 1e-6 * rng.standard_normal((4000, 3)) for c in centres])
+    x, y, z = (np.ascontiguousarray(p[:, a]) for a in range(3))
+    q = rng.uniform(-1.0, 1.0, len(p))
+    t = ctx.treemake(x, y, z, 64)
+    t.treemoments(q, 9)
+    kw = dict(kappa=1.0) if kern == "screened" else dict(del_=0.0)
+    k = B.SCREENED if kern == "screened" else B.COULOMB
+    p64 = t.evaluate(B.params(k, B.CONSISTENT, B.FP64, acc=0.5, **kw))
+    p32 = t.evaluate(B.params(k, B.CONSISTENT, B.MIXED, acc=0.5, **kw))
+    assert t.stats()["far_pairs"] > 0
+    assert np.all(np.isfinite(p64)) and np.all(np.isfinite(p32))
+    assert workloads.rel_l2(p32, p64) < TOL_MIXED
+
+
 def shared_steps(c, x, y, z, q, prec, ps, pc, steps=2):
     """The benchmark's step on a fresh tree each time: screened, then Coulomb."""
     import bit_b200 as B
