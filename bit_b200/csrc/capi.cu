@@ -266,6 +266,10 @@ bit_status bit_ctx_destroy(bit_ctx* h) {
   }
   c.trees.clear();
   c.scratch_ll.release();
+  c.close_cnt.release();
+  c.close_n.release();
+  c.close_rec.release();
+  c.close_list.release();
   release_cache(&c);
   if (c.h_pinned) cudaFreeHost(c.h_pinned);
   for (int i = 0; i < 2; i++) {

@@ -143,6 +143,7 @@ struct Lists {
   ListKey key;
   bool valid = false;
   int ngroups = 0;
+  int ntargets = 0;                         // targets the groups cover
   long long nfar = 0, nnear = 0;            // entries
   long long far_pairs = 0, near_pairs = 0;  // interactions
   DBuf<int> g_tstart, g_tcount;             // group: first target, count
@@ -185,6 +186,9 @@ struct Ctx {
   std::vector<Tree*> trees;                       // trees built by this context
   long long launches = 0;                         // kernels launched by this context
   int* err_flag = nullptr;                        // device word kernels raise errors in
+  // mixed near field: close pairs left to the FP64 pass, per target
+  DBuf<int> close_cnt, close_n;
+  DBuf<int2> close_rec, close_list;
   void* stage[2] = {nullptr, nullptr};            // pinned staging chunks for host copies
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   int* dev_err() {
@@ -204,6 +208,7 @@ struct Tree {
   // [sys_start[s], sys_start[s] + sys_n[s]) and its root is node s.
   int nsys = 1;
   std::vector<int> h_sys_start, h_sys_n, h_sys_maxmemb, h_sys_nterms, h_node_sys;
+  std::vector<double> h_sys_leaf_sqr;  // per system: largest leaf sqradius
   DBuf<int> sys_start, sys_n, sys_maxmemb, node_sys;
   // particles in tree order (sorted position e); perm[e] = original index
   DBuf<int> perm, iperm;

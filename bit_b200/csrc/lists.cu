@@ -332,6 +332,7 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   }
   const int ng = (int)ts.size();
   L->ngroups = ng;
+  L->ntargets = ntargets;
   L->g_tstart.ensure(c, ng);
   L->g_tcount.ensure(c, ng);
   BIT_CUDA(cudaMemcpyAsync(L->g_tstart.p, ts.data(), ng * sizeof(int), cudaMemcpyHostToDevice, s));

@@ -43,7 +43,14 @@ struct NearArgs {
   const int* g_sys;    // per group: system
   double *out, *out_y, *out_z;  // potential, or the three field components
   int* err;
+  // mixed potentials: close pairs left out of the FP32 sums, per target (k_close)
+  int* ccnt;    // tiles recorded for the target
+  int2* crec;   // up to kCloseRec (near entry, first source of the tile) per target
+  int2* clist;  // (target, group) of every target with a record
+  int* cn;      // entries of clist
 };
+
+constexpr int kCloseRec = 2;  // record slots per target; beyond them k_close scans them all
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
   float y;
@@ -167,17 +174,15 @@ __device__ __forceinline__ void sweep_pot(const float4* fs, int j, int je, int t
   p1 += p2 + p3;
 }
 
-// FP64 sum of this lane's pairs with FP32 r^2 < thr (self skipped).
-template <int KER, bool EPS>
-__device__ __forceinline__ double close_pot(float xt, float yt, float zt, double x, double y,
-                                         double z, const float4* fs, const double4* s64,
-                                         int slice, int tpt, int ns, int selfj, float del,
-                                         float thr, double del64, double kappa) {
-  double acc = 0.0;
-  for (int j = slice; j < ns; j += tpt)
-    if (j != selfj && r2_32(xt, yt, zt, fs[j], del) < thr)
-      acc += pair<KER, EPS>(x, y, z, s64[j], del64, kappa);
-  return acc;
+// Target t left close pairs out of this job's FP32 sum (near entry e, tile at toff).  One
+// thread handles a target per job, and the CTA's jobs are separated by barriers, so the
+// target's records need no atomics and come in job order.
+__device__ __forceinline__ void record_close(const NearArgs& a, int t, int g, long long e,
+                                             int toff) {
+  const int c = a.ccnt[t];
+  if (c < kCloseRec) a.crec[(long long)t * kCloseRec + c] = make_int2((int)e, toff);
+  a.ccnt[t] = c + 1;
+  if (c == 0) a.clist[atomicAdd(a.cn, 1)] = make_int2(t, g);
 }
 
 // Field of one pair, q (x - x_j) / r^3 (eval_grad_kernel_reg, src/tree3d.cpp:73-97,
@@ -372,6 +377,7 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
         const int je = self_in ? selfj : ns;
         if (!FORCE) {
           T part = 0;
+          bool close = false;  // mixed: a pair of this lane was left for the FP64 pass
           if constexpr (F32) {
             const float4* fs = reinterpret_cast<const float4*>(ts);
             const float xt = (float)(cx[t0 + i] - c.x), yt = (float)(cy[t0 + i] - c.y),
@@ -379,7 +385,6 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
             const bool chk = __any_sync(0xffffffffu, valid && box_d2(xt, yt, zt, hb) < thr);
             if (valid) {
               float p0 = 0.f, p1 = 0.f;
-              bool close = false;
               if (!chk) {
                 sweep_pot<KER, false>(fs, slice, je, tpt, xt, yt, zt, del, kl2, thr, p0, p1, close);
                 if (self_in)
@@ -390,9 +395,6 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
                   sweep_pot<KER, true>(fs, selfj + tpt, ns, tpt, xt, yt, zt, del, kl2, thr, p0, p1, close);
               }
               part = p0 + p1;
-              if (close)
-                part += (float)close_pot<KER, EPS>(xt, yt, zt, cx[t0 + i], cy[t0 + i], cz[t0 + i], fs,
-                                                   s64, slice, tpt, ns, selfj, del, thr, sdel, skappa);
             }
           } else {
             if (valid) {
@@ -412,6 +414,13 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
           if (valid && slice == 0) {
             if constexpr (F32) two_sum(acch[i], acch[kGroupMax + i], (float)part);
             else accd[i] += (double)part;
+          }
+          if constexpr (F32) {
+            if (a.ccnt) {  // (null where no pair can be close)
+              // a target's tpt slices share a warp: one record per target and tile
+              for (int o = tpt >> 1; o; o >>= 1) close |= __shfl_xor_sync(0xffffffffu, (int)close, o) != 0;
+              if (valid && slice == 0 && close) record_close(a, t0 + i, g, e, toff);
+            }
           }
         } else {
           T fx = 0, fy = 0, fz = 0;
@@ -493,6 +502,69 @@ void launch(const NearArgs& a, int ngroups, cudaStream_t s) {
   count_launch(), k_near<KER, EPS, F32, FORCE><<<ngroups, NT, bytes, s>>>(a);
 }
 
+// FP64 sum of the close pairs that the mixed near kernel left out (FP32 r^2 < thr, the
+// target's own source excluded), one warp per recorded target: the recorded tiles in job
+// order, or, for a target with more tiles than record slots, every near entry of its group
+// that covers it (tiles without close pairs add nothing, so the sum is the same).  Lanes
+// take the sources in the kernel's order and the warp reduces in a fixed order, so the
+// result does not depend on scheduling.
+template <int KER, bool EPS>
+__device__ double close_sum(const NearArgs& a, const SysEval* se, int t, int g, double x,
+                            double y, double z) {
+  const int lane = threadIdx.x & 31;
+  const double sdel = se->near_del, skappa = se->kappa;
+  const float del = (float)sdel;
+  const int self = se->particles ? t : -1;  // sorted position of the target's own source
+  const float4* fs = reinterpret_cast<const float4*>(a.src);
+  double acc = 0.0;
+  auto tile = [&](int node, int j0, int j1) {
+    const double4 c = a.nodec[node];
+    const float xt = (float)(x - c.x), yt = (float)(y - c.y), zt = (float)(z - c.z);
+    const float thr = fmaxf((float)c.w * kCloseFrac, kThrMin);
+    const int s0 = a.start[node];
+    for (int j = s0 + j0 + lane; j < s0 + j1; j += 32)
+      if (j != self && r2_32(xt, yt, zt, fs[j], del) < thr)
+        acc += pair<KER, EPS>(x, y, z, a.src64[j], sdel, skappa);
+  };
+  const int nrec = a.ccnt[t];
+  if (nrec <= kCloseRec) {
+    for (int k = 0; k < nrec; k++) {
+      const int2 r = a.crec[(long long)t * kCloseRec + k];
+      const int node = a.node[r.x];
+      tile(node, r.y, min(r.y + Prec<true>::TILE, a.nummemb[node]));
+    }
+  } else {
+    const int i = t - a.g_tstart[g], W = (a.g_tcount[g] + 31) >> 5;
+    const long long e0 = a.off[g], e1 = e0 + a.cnt[g], m0 = a.moff[g];
+    for (long long e = e0; e < e1; e++)
+      if ((a.mask[m0 + (e - e0) * W + (i >> 5)] >> (i & 31)) & 1u) {
+        const int node = a.node[e];
+        tile(node, 0, a.nummemb[node]);
+      }
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
+}
+
+__global__ void __launch_bounds__(256) k_close(NearArgs a) {
+  const int lane = threadIdx.x & 31;
+  const int n = *a.cn;
+  for (int w = blockIdx.x * 8 + (threadIdx.x >> 5); w < n; w += gridDim.x * 8) {
+    const int2 tg = a.clist[w];
+    const int t = tg.x, g = tg.y;
+    const SysEval* se = a.sys + a.g_sys[g];
+    const double x = a.tx[t], y = a.ty[t], z = a.tz[t];
+    double v;
+    if (se->kernel == BIT_KERNEL_COULOMB)
+      v = se->eps_check ? close_sum<BIT_KERNEL_COULOMB, true>(a, se, t, g, x, y, z)
+                        : close_sum<BIT_KERNEL_COULOMB, false>(a, se, t, g, x, y, z);
+    else
+      v = se->eps_check ? close_sum<BIT_KERNEL_SCREENED, true>(a, se, t, g, x, y, z)
+                        : close_sum<BIT_KERNEL_SCREENED, false>(a, se, t, g, x, y, z);
+    if (lane == 0) a.out[t] += se->near_sign * v;
+  }
+}
+
 NearArgs base_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
                    const double* tz) {
   NearArgs a{};
@@ -522,10 +594,36 @@ NearArgs base_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const
 // One launch per (kernel, eps check) class, each over its groups (P.near_ord + begin).
 void eval_near(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
                const double* tz, double* out) {
-  cudaStream_t s = t->ctx->stream;
+  Ctx* c = t->ctx;
+  cudaStream_t s = c->stream;
   NearArgs a = base_args(t, L, P, tx, ty, tz);
   a.out = out;
+  // Mixed: close pairs need r^2 < thr = max(sqradius / 1024, 2e-14) of some leaf, and the
+  // FP32 r^2 is at least the system's del (a rounded sum of non-negative terms and del);
+  // where del reaches the largest leaf threshold no pair can be close, and the records
+  // and the FP64 pass are skipped.
+  bool close_possible = false;
+  if (P.f32)
+    for (size_t sy = 0; sy < P.h_sys.size(); sy++) {
+      const float thr_max = fmaxf((float)t->h_sys_leaf_sqr[sy] * kCloseFrac, kThrMin);
+      close_possible |= (float)P.h_sys[sy].near_del < thr_max;
+    }
   const bool f32 = P.f32;
+  if (close_possible) {
+    // close-pair records, cleared for this evaluation (k_close consumes them)
+    const int nt = L->ntargets;
+    if (L->nnear >= INT_MAX) fail(BIT_ERR_CAPACITY, "too many near entries");
+    c->close_cnt.ensure(c, nt);
+    c->close_rec.ensure(c, (size_t)nt * kCloseRec);
+    c->close_list.ensure(c, nt);
+    c->close_n.ensure(c, 1);
+    BIT_CUDA(cudaMemsetAsync(c->close_cnt.p, 0, (size_t)nt * sizeof(int), s));
+    BIT_CUDA(cudaMemsetAsync(c->close_n.p, 0, sizeof(int), s));
+    a.ccnt = c->close_cnt.p;
+    a.crec = c->close_rec.p;
+    a.clist = c->close_list.p;
+    a.cn = c->close_n.p;
+  }
   for (const LaunchClass& k : P.near_classes) {
     a.order = P.near_ord + k.begin;
     const int ng = k.count;
@@ -540,6 +638,10 @@ void eval_near(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const dou
       else { if (eps) GO(BIT_KERNEL_SCREENED, true, false); else GO(BIT_KERNEL_SCREENED, false, false); }
     }
 #undef GO
+    BIT_CHECK_LAUNCH();
+  }
+  if (close_possible) {
+    count_launch(), k_close<<<c->num_sms * 4, 256, 0, s>>>(a);
     BIT_CHECK_LAUNCH();
   }
 }

@@ -44,10 +44,11 @@ struct Request {
 using Clock = std::chrono::steady_clock;
 
 // Device memory a request may need: particles in tree order (coordinates, sources in FP64
-// and FP32, permutations), build scratch, interaction lists, moments, outputs; a solve
-// adds its Krylov basis and work vectors.  Measured peaks stay below these figures.
+// and FP32, permutations), build scratch, interaction lists, moments, outputs, the mixed
+// near field's close-pair records (28 B per target); a solve adds its Krylov basis and
+// work vectors.  Measured peaks stay below these figures.
 size_t estimate_bytes(int kind, int n, int restart) {
-  size_t per = 420;
+  size_t per = 448;
   if (kind == 1) per += 8ull * (restart + 10);
   return (64ull << 20) + per * (size_t)n;
 }

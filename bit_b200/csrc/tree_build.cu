@@ -792,6 +792,12 @@ void tree_sync_host(Tree* t) {
   BIT_CUDA(cudaMemcpyAsync(t->h_fields.data(), t->fields.p, 13LL * b * sizeof(double), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaMemcpyAsync(t->h_node_sys.data(), t->node_sys.p, b * sizeof(int), cudaMemcpyDeviceToHost, s));
   BIT_CUDA(cudaStreamSynchronize(s));
+  t->h_sys_leaf_sqr.assign(t->nsys, 0.0);
+  for (int i = 0; i < b; i++)
+    if (t->h_children[8LL * i] == -1) {
+      double& m = t->h_sys_leaf_sqr[t->h_node_sys[i]];
+      m = std::max(m, t->h_fields[13LL * i + 12]);
+    }
 }
 
 }  // namespace bit

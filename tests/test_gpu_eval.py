@@ -239,6 +239,32 @@ def test_mixed_force_close_pairs_within_tolerance(ctx):
     assert workloads.rel_l2(f32, f64) < TOL_MIXED
 
 
+@pytest.mark.parametrize("kern", ["screened", "coulomb"])
+@pytest.mark.parametrize("blob,maxmemb", [(1500, 2000), (3000, 4000)])
+def test_mixed_close_pairs_across_source_tiles(ctx, kern, blob, maxmemb):
+    """A blob of radius 1e-6 at (0.3, 0.3, 0.3) inside 20,000 uniform points: its leaf
+    holds 1,821 sources (N0 = 2000: 2 source tiles) or 3,661 (N0 = 4000: 4 tiles), and
+    every blob pair is a close pair.  A blob target records each of those tiles for the
+    FP64 pass: 2 fit the record slots, 4 overflow them, and the pass then scans all of the
+    target's near entries instead.  Both must match the FP64 path."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    rng = np.random.default_rng(13)
+    p = np.concatenate([rng.uniform(0.0, 1.0, (20000, 3)),
+                        [0.3, 0.3, 0.3] + 1e-6 * rng.standard_normal((blob, 3))])
+    x, y, z = (np.ascontiguousarray(p[:, a]) for a in range(3))
+    q = rng.uniform(-1.0, 1.0, len(p))
+    t = ctx.treemake(x, y, z, maxmemb)
+    t.treemoments(q, 5)
+    kw = dict(kappa=2.0) if kern == "screened" else dict(del_=1e-14)
+    k = B.SCREENED if kern == "screened" else B.COULOMB
+    p64 = t.evaluate(B.params(k, B.CONSISTENT, B.FP64, acc=0.5, **kw))
+    p32 = t.evaluate(B.params(k, B.CONSISTENT, B.MIXED, acc=0.5, **kw))
+    assert np.all(np.isfinite(p32))
+    assert workloads.rel_l2(p32, p64) < TOL_MIXED
+    np.testing.assert_array_equal(p32, t.evaluate(B.params(k, B.CONSISTENT, B.MIXED, acc=0.5, **kw)))
+
+
 def test_mixed_coincident_duplicates_follow_the_fp64_rules(ctx):
     """Exact duplicates: the Coulomb sum skips r^2 + del <= 1e-14 in both precisions."""
     import bit_b200 as B

@@ -16,7 +16,7 @@ MB = 1 << 20
 
 def est_eval(n):
     """Admission estimate of an evaluate request (the server's formula)."""
-    return 64 * MB + 420 * n
+    return 64 * MB + 448 * n
 
 
 def eval_requests(B, count, seed):
