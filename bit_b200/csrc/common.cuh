@@ -221,6 +221,7 @@ struct Tree {
   DBuf<double> fields;   // 13 per node
   DBuf<double4> nodec;   // (xmid, ymid, zmid, sqradius)
   DBuf<float4> nodeh;    // half extents of the box about the midpoint (rounded up)
+  DBuf<int2> kids;       // children: (first index or -1, count | slot order 3 bits each)
   DBuf<int> leaves;
   // host mirror of the node structure
   std::vector<int> h_nummemb, h_start, h_children, h_level, h_perm;

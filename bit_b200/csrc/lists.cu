@@ -46,7 +46,7 @@ struct ListArgs {
   const int *g_tstart, *g_tcount;
   const double *tx, *ty, *tz;
   const double4* nodec;
-  const int *children, *nummemb;
+  const int2* kids;  // per node: (first child, count | slot order), a leaf (-1, members)
   const SysEval* sys;  // per system: MAC parameters
   const int* g_sys;    // per group: system (its root is node g_sys[g])
   // per group
@@ -115,6 +115,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
     sp--;
     const int node = s_node[w][sp];
     const unsigned word = s_mask[sp][w];
+    const int2 kd = a.kids[node];  // loads alongside the centre, needed only to descend
     bool ok = false;
     if ((word >> lane) & 1u) {
       const double4 c = a.nodec[node];
@@ -143,8 +144,7 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
       if (lane == 0) fpairs += __popc(am);
     }
     if (anyR) {
-      const int* ch = a.children + 8LL * node;
-      if (ch[0] == -1) {
+      if (kd.x < 0) {
         if (MODE == MODE_FILL) {
           if (threadIdx.x == 0) a.near_node[no + nn] = node;
           if (lane == 0 && w < W) a.near_mask[nmo + nn * W + w] = rm;
@@ -154,20 +154,16 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
           if (lane == 0 && w < W) sn_mask[nn * W + w] = rm;
         }
         nn++;
-        if (lane == 0) npairs += (long long)__popc(rm) * a.nummemb[node];
+        if (lane == 0) npairs += (long long)__popc(rm) * kd.y;
       } else {
-        int cnt = 0;
-        for (int k = 0; k < 8; k++) cnt += ch[k] != -1;
+        const int cnt = kd.y & 15;
         if (sp + cnt > LSTK) { overflow = true; break; }
-        int q = sp;
-        for (int k = 7; k >= 0; k--) {
-          if (ch[k] == -1) continue;
-          if (lane == 0) {
-            s_node[w][q] = ch[k];
+        // children[k] = kd.x + order[k]; the last slot goes deepest, so children[0] pops first
+        if (lane == 0)
+          for (int k = cnt - 1, q = sp; k >= 0; k--, q++) {
+            s_node[w][q] = kd.x + ((kd.y >> (4 + 3 * k)) & 7);
             s_mask[q][w] = rm;
           }
-          q++;
-        }
         sp += cnt;
       }
     }
@@ -354,8 +350,7 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   a.g_tcount = L->g_tcount.p;
   a.tx = tx; a.ty = ty; a.tz = tz;
   a.nodec = t->nodec.p;
-  a.children = t->children.p;
-  a.nummemb = t->nummemb.p;
+  a.kids = t->kids.p;
   a.sys = d_sys;
   a.g_sys = L->g_sys.p;
   a.far_off = L->far_off.p; a.near_off = L->near_off.p;

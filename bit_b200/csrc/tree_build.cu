@@ -570,9 +570,22 @@ __global__ void k_make_children(int a, int b, int nlev, const SplitState* st, co
   for (int c = 0; c < 8; c++) children[8LL * p + c] = c < S->nchild ? base + S->order[c] : -1;
 }
 
-__global__ void k_node_centres(int numtree, const double* fields, double4* nodec, float4* nodeh) {
+__global__ void k_node_centres(int numtree, const double* fields, const int* children,
+                               const int* nummemb, double4* nodec, float4* nodeh, int2* kids) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < numtree) {
+    // children[] holds base + order[c] in its first nchild slots (consecutive node
+    // indices, in another order), so one int2 gives the traversal all of them:
+    // (base, nchild | order[c] << (4 + 3c)); a leaf is (-1, nummemb)
+    const int* ch = children + 8LL * i;
+    int base = ch[0], cnt = 0;
+    for (int c = 0; c < 8 && ch[c] != -1; c++) {
+      base = min(base, ch[c]);
+      cnt++;
+    }
+    int code = cnt;
+    for (int c = 0; c < cnt; c++) code |= (ch[c] - base) << (4 + 3 * c);
+    kids[i] = cnt ? make_int2(base, code) : make_int2(-1, nummemb[i]);
     const double* f = fields + 13LL * i;
     nodec[i] = make_double4(f[6], f[7], f[8], f[12]);
     // half extents about the midpoint, rounded up to FP32 (a box the members are inside of)
@@ -752,7 +765,9 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
   t->cap = cap;
   t->nodec.ensure(c, b);
   t->nodeh.ensure(c, b);
-  count_launch(), k_node_centres<<<grid_for(b, 128), 128, 0, s>>>(b, t->fields.p, t->nodec.p, t->nodeh.p);
+  t->kids.ensure(c, b);
+  count_launch(), k_node_centres<<<grid_for(b, 128), 128, 0, s>>>(b, t->fields.p, t->children.p, t->nummemb.p,
+                                                                 t->nodec.p, t->nodeh.p, t->kids.p);
   tree_sync_host(t);
   // leaves in node order
   std::vector<int> leaves;
