@@ -235,7 +235,8 @@ __global__ void k_root_init(int nsys, const int* sys_start, const int* sys_n, co
 
 // Per level node: active flag and the number of member chunks it needs.
 __global__ void k_level_init(int a, int nlev, const int* nummemb, const int* node_sys,
-                             const int* sys_maxmemb, SplitState* st, SplitAcc* acc, int* nchunk) {
+                             const int* sys_maxmemb, SplitState* st, SplitAcc* acc, int* nchunk,
+                             int* done) {
   int li = blockIdx.x * blockDim.x + threadIdx.x;
   if (li >= nlev) return;
   SplitState* S = &st[li];
@@ -244,6 +245,7 @@ __global__ void k_level_init(int a, int nlev, const int* nummemb, const int* nod
   S->finished = 0; S->ndone = 0; S->has_cur = 0; S->has_prev = 0; S->nchild = 0;
   acc_reset(&acc[li]);
   nchunk[li] = S->active ? (cnt + CH - 1) / CH : 0;
+  done[li] = 0;
 }
 
 // Exclusive scan of a small int array in one block; total in out[n].
@@ -289,11 +291,10 @@ __global__ void k_fill_chunks(int a, int nlev, const int* start, const int* numm
   for (int c = cbeg[li]; c < cbeg[li + 1]; c++) chunks[c] = make_int2(li, s + (c - cbeg[li]) * CH);
 }
 
-__global__ void k_split_decide(int a, int nlev, const double* fields, const int* node_sys,
-                               const int* sys_maxmemb, SplitState* st, SplitAcc* acc, double lim,
-                               int* err) {
-  int li = blockIdx.x * blockDim.x + threadIdx.x;
-  if (li >= nlev) return;
+// Record the bisection step just reduced for node a + li and plan its next one.
+__device__ __noinline__ void decide_node(int a, int li, const double* fields, const int* node_sys,
+                                         const int* sys_maxmemb, SplitState* st, SplitAcc* acc,
+                                         double lim, int* err) {
   SplitState* S = &st[li];
   if (!S->active) return;
   SplitAcc* A = &acc[li];
@@ -338,22 +339,45 @@ __global__ void k_split_decide(int a, int nlev, const double* fields, const int*
   if (nchild < 2) atomicOr(err, 2);  // one child == the node itself: never terminates
 }
 
+__global__ void k_split_decide(int a, int nlev, const double* fields, const int* node_sys,
+                               const int* sys_maxmemb, SplitState* st, SplitAcc* acc, double lim,
+                               int* err) {
+  int li = blockIdx.x * blockDim.x + threadIdx.x;
+  if (li < nlev) decide_node(a, li, fields, node_sys, sys_maxmemb, st, acc, lim, err);
+}
+
 __device__ __forceinline__ double coord(int dir, const double* sx, const double* sy,
                                         const double* sz, int e) {
   return dir == 0 ? sx[e] : (dir == 1 ? sy[e] : sz[e]);
 }
 
+// Per-level inputs of the decision a split pass makes for each node when its last chunk
+// is done (decide = 0: the level's final pass, which only relabels).
+struct DecideArgs {
+  const int* nchunk;
+  int* done;
+  const double* fields;
+  const int* node_sys;
+  const int* sys_maxmemb;
+  double lim;
+  int* err;
+  int decide;
+};
+
 // One bisection step for every active node of the level: apply the previous step's
-// relabel, then reduce counts / bounding boxes of both halves of the current step.
-__global__ void __launch_bounds__(TB) k_split_pass(const int2* chunks, int a, const int* start,
+// relabel, then reduce counts / bounding boxes of both halves of the current step.  The
+// CTA that finishes a node's last chunk then makes the node's decision for the next step.
+// 6 CTAs per SM as without the decision (40 registers); whatever the call to decide_node
+// needs beyond that is spilled on the deciding thread's path only
+__global__ void __launch_bounds__(TB, 6) k_split_pass(const int2* chunks, int a, const int* start,
                                                    const int* nummemb, const double* sx,
                                                    const double* sy, const double* sz,
-                                                   signed char* lab, const SplitState* st,
-                                                   SplitAcc* acc) {
+                                                   signed char* lab, SplitState* st,
+                                                   SplitAcc* acc, DecideArgs da) {
   const int2 ck = chunks[blockIdx.x];
   const SplitState* S = &st[ck.x];
   const int hp = S->has_prev, hc = S->has_cur;
-  if (!hp && !hc) return;
+  if (!hp && !hc) return;  // (its decision would change nothing)
   const Divide pv = S->prev, cu = S->cur;
   const int pc2 = S->prev_c2eff;
   const int node = a + ck.x;
@@ -379,7 +403,6 @@ __global__ void __launch_bounds__(TB) k_split_pass(const int2* chunks, int a, co
       }
     }
   }
-  if (!hc) return;
   // warp, then CTA reductions; one set of global atomics per CTA (min / max / sum are
   // order-independent, so the result is exact whatever the order)
   constexpr int NW = TB / 32;
@@ -396,7 +419,7 @@ __global__ void __launch_bounds__(TB) k_split_pass(const int2* chunks, int a, co
     }
   }
   __syncthreads();
-  if (threadIdx.x < 2 * 7) {  // thread (h, v): v = 0..5 min/max of one axis, v = 6 count
+  if (hc && threadIdx.x < 2 * 7) {  // thread (h, v): v = 0..5 min/max of one axis, v = 6 count
     const int h = threadIdx.x / 7, v = threadIdx.x % 7;
     int c = 0;
     for (int q = 0; q < NW; q++) c += s_c[q][h];
@@ -415,6 +438,20 @@ __global__ void __launch_bounds__(TB) k_split_pass(const int2* chunks, int a, co
           atomicMin(&acc[ck.x].mn[h][d], m);
         }
       }
+    }
+  }
+  if (!da.decide) return;
+  // the CTA that completes the node's chunk count decides (its atomics, and every other
+  // chunk's, are visible after the fences)
+  __shared__ int s_last;
+  __threadfence();  // this thread's atomics, before the count that may complete the node
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_last = atomicAdd(&da.done[ck.x], 1) == da.nchunk[ck.x] - 1;
+    if (s_last) {
+      __threadfence();
+      decide_node(a, ck.x, da.fields, da.node_sys, da.sys_maxmemb, st, acc, da.lim, da.err);
+      da.done[ck.x] = 0;
     }
   }
 }
@@ -681,7 +718,7 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
 
   const double lim = 1.0 / std::sqrt(2.0);  // src/tree3d.cpp:1371
   DBuf<SplitState> st;
-  DBuf<int> nchunk, cbeg, cc, coff, nch, cscan;
+  DBuf<int> nchunk, cbeg, cc, coff, nch, cscan, done;
   DBuf<int2> chunks;
   int a = 0, b = nsys, depth = 1;
   while (true) {
@@ -693,8 +730,9 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     nch.ensure(c, nlev);
     cscan.ensure(c, nlev + 1);
     const unsigned gl = grid_for(nlev, 128);
+    done.ensure(c, nlev);
     count_launch(), k_level_init<<<gl, 128, 0, s>>>(a, nlev, t->nummemb.p, t->node_sys.p,
-                                                    t->sys_maxmemb.p, st.p, acc.p, nchunk.p);
+                                                    t->sys_maxmemb.p, st.p, acc.p, nchunk.p, done.p);
     count_launch(), k_scan_small<<<1, 1024, 0, s>>>(nchunk.p, cbeg.p, nlev);
     BIT_CUDA(cudaMemcpyAsync(hp, cbeg.p + nlev, sizeof(int), cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
@@ -706,14 +744,12 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     count_launch(), k_fill_chunks<<<gl, 128, 0, s>>>(a, nlev, t->start.p, t->nummemb.p, cbeg.p, chunks.p);
     count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, t->node_sys.p,
                                                       t->sys_maxmemb.p, st.p, acc.p, lim, err.p);
-    for (int step = 0; step < 7; step++) {
+    DecideArgs da{nchunk.p, done.p, t->fields.p, t->node_sys.p, t->sys_maxmemb.p, lim, err.p, 1};
+    for (int step = 0; step < 8; step++) {  // 7 bisection steps at most, then the last relabel
+      da.decide = step < 7;
       count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
-                                                            t->sy.p, t->sz.p, lab.p, st.p, acc.p);
-      count_launch(), k_split_decide<<<gl, 128, 0, s>>>(a, nlev, t->fields.p, t->node_sys.p,
-                                                        t->sys_maxmemb.p, st.p, acc.p, lim, err.p);
+                                                            t->sy.p, t->sz.p, lab.p, st.p, acc.p, da);
     }
-    count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
-                                                          t->sy.p, t->sz.p, lab.p, st.p, acc.p);
     count_launch(), k_scatter_count<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, cc.p);
     count_launch(), k_scatter_offsets<<<nlev, TB, 0, s>>>(a, t->start.p, cbeg.p, cc.p, coff.p, st.p, err.p);
     count_launch(), k_scatter<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, coff.p,
