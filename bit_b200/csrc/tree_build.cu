@@ -15,6 +15,7 @@
 // original index (the reference's member order).  Field arithmetic (midpoints, aspect
 // ratios, sqradius) is the reference's, with no FMA contraction.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 
 #include "common.cuh"
@@ -369,11 +370,12 @@ struct DecideArgs {
 // CTA that finishes a node's last chunk then makes the node's decision for the next step.
 // 6 CTAs per SM as without the decision (40 registers); whatever the call to decide_node
 // needs beyond that is spilled on the deciding thread's path only
-__global__ void __launch_bounds__(TB, 6) k_split_pass(const int2* chunks, int a, const int* start,
+__global__ void __launch_bounds__(TB, 6) k_split_pass(const int2* chunks, const int* nch, int a, const int* start,
                                                    const int* nummemb, const double* sx,
                                                    const double* sy, const double* sz,
                                                    signed char* lab, SplitState* st,
                                                    SplitAcc* acc, DecideArgs da) {
+  if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
   const SplitState* S = &st[ck.x];
   const int hp = S->has_prev, hc = S->has_cur;
@@ -456,8 +458,9 @@ __global__ void __launch_bounds__(TB, 6) k_split_pass(const int2* chunks, int a,
   }
 }
 
-__global__ void k_scatter_count(const int2* chunks, int a, const int* start, const int* nummemb,
+__global__ void k_scatter_count(const int2* chunks, const int* nch, int a, const int* start, const int* nummemb,
                                 const signed char* lab, int* cc) {
+  if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
   const int node = a + ck.x;
   const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
@@ -525,12 +528,13 @@ __global__ void __launch_bounds__(TB) k_scatter_offsets(int a, const int* start,
 }
 
 // Stable scatter of each chunk's members to their child's range (order kept).
-__global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, int a, const int* start,
+__global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, const int* nch, int a, const int* start,
                                                 const int* nummemb, const signed char* lab,
                                                 const int* coff, const int* perm,
                                                 const double* sx, const double* sy,
                                                 const double* sz, int* perm2, double* sx2,
                                                 double* sy2, double* sz2) {
+  if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
   const int node = a + ck.x;
   const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
@@ -568,9 +572,10 @@ __global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, int a, const
   }
 }
 
-__global__ void k_copy_back(const int2* chunks, int a, const int* start, const int* nummemb,
+__global__ void k_copy_back(const int2* chunks, const int* nch, int a, const int* start, const int* nummemb,
                             const int* perm2, const double* sx2, const double* sy2,
                             const double* sz2, int* perm, double* sx, double* sy, double* sz) {
+  if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
   const int node = a + ck.x;
   const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
@@ -734,10 +739,12 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     count_launch(), k_level_init<<<gl, 128, 0, s>>>(a, nlev, t->nummemb.p, t->node_sys.p,
                                                     t->sys_maxmemb.p, st.p, acc.p, nchunk.p, done.p);
     count_launch(), k_scan_small<<<1, 1024, 0, s>>>(nchunk.p, cbeg.p, nlev);
-    BIT_CUDA(cudaMemcpyAsync(hp, cbeg.p + nlev, sizeof(int), cudaMemcpyDeviceToHost, s));
-    BIT_CUDA(cudaStreamSynchronize(s));
-    const int nch_total = *reinterpret_cast<int*>(hp);
-    if (nch_total == 0) break;
+    // The level's chunk count stays on the device (cbeg[nlev]): the chunk kernels run on a
+    // grid sized from its bound, n / CH + one partial chunk per node, and CTAs past the
+    // count return.  A level of leaves only runs empty kernels, and ends the loop below
+    // with no children.
+    const int* nchk = cbeg.p + nlev;
+    const int nch_total = (int)std::min<long long>((long long)n / CH + nlev + 1, INT_MAX);
     chunks.ensure(c, nch_total);
     cc.ensure(c, 8LL * nch_total);
     coff.ensure(c, 8LL * nch_total);
@@ -747,15 +754,15 @@ void tree_build(Tree* t, const double* x, const double* y, const double* z) {
     DecideArgs da{nchunk.p, done.p, t->fields.p, t->node_sys.p, t->sys_maxmemb.p, lim, err.p, 1};
     for (int step = 0; step < 8; step++) {  // 7 bisection steps at most, then the last relabel
       da.decide = step < 7;
-      count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, t->sx.p,
+      count_launch(), k_split_pass<<<nch_total, TB, 0, s>>>(chunks.p, nchk, a, t->start.p, t->nummemb.p, t->sx.p,
                                                             t->sy.p, t->sz.p, lab.p, st.p, acc.p, da);
     }
-    count_launch(), k_scatter_count<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, cc.p);
+    count_launch(), k_scatter_count<<<nch_total, TB, 0, s>>>(chunks.p, nchk, a, t->start.p, t->nummemb.p, lab.p, cc.p);
     count_launch(), k_scatter_offsets<<<nlev, TB, 0, s>>>(a, t->start.p, cbeg.p, cc.p, coff.p, st.p, err.p);
-    count_launch(), k_scatter<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, lab.p, coff.p,
+    count_launch(), k_scatter<<<nch_total, TB, 0, s>>>(chunks.p, nchk, a, t->start.p, t->nummemb.p, lab.p, coff.p,
                                                        t->perm.p, t->sx.p, t->sy.p, t->sz.p, perm2.p, sx2.p,
                                                        sy2.p, sz2.p);
-    count_launch(), k_copy_back<<<nch_total, TB, 0, s>>>(chunks.p, a, t->start.p, t->nummemb.p, perm2.p, sx2.p,
+    count_launch(), k_copy_back<<<nch_total, TB, 0, s>>>(chunks.p, nchk, a, t->start.p, t->nummemb.p, perm2.p, sx2.p,
                                                          sy2.p, sz2.p, t->perm.p, t->sx.p, t->sy.p, t->sz.p);
     // the next level's members start unlabelled
     BIT_CUDA(cudaMemsetAsync(lab.p, -1, n, s));
