@@ -446,15 +446,22 @@ class Tree:
         self.ctx.check(lib().bit_tree_export_moments(self.h, _d(m)), "bit_tree_export_moments")
         return m.reshape(self.numtree, T)
 
-    def evaluate(self, prm, points=None):
+    def evaluate(self, prm, points=None, out=None):
+        """Potential at every particle (or at `points`).  `out`: an optional C-contiguous
+        float64 array of the right length to write into, so that repeated calls reuse one
+        buffer instead of faulting in fresh pages each time."""
+        m = self.n if points is None else len(points)
+        if out is None:
+            out = np.zeros(m)
+        elif (not isinstance(out, np.ndarray) or out.dtype != np.float64 or out.shape != (m,)
+              or not out.flags["C_CONTIGUOUS"] or not out.flags["WRITEABLE"]):
+            raise ValueError(f"out must be a writeable C-contiguous float64 array of length {m}")
         if points is not None:
             pts = _f64(points)
             tx, ty, tz = [np.ascontiguousarray(pts[:, a]) for a in range(3)]
-            out = np.zeros(len(pts))
             self.ctx.check(lib().bit_eval_points(self.h, C.byref(prm), len(pts), _d(tx), _d(ty),
                                                  _d(tz), _d(out)), "bit_eval_points")
             return out
-        out = np.zeros(self.n)
         self.ctx.check(lib().bit_eval_particles(self.h, C.byref(prm), _d(out)),
                        "bit_eval_particles")
         return out

@@ -151,6 +151,28 @@ def test_repeat_and_stats(ctx):
     assert st["numtree"] == t.numtree and st["far_pairs"] > 0 and st["t_far"] > 0
 
 
+def test_evaluate_into_a_caller_buffer(ctx):
+    """evaluate(out=...) writes the same bits into the caller's array and returns it, for
+    particles and points; a wrong dtype or length is refused before anything runs."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.uniform_cube(20000, seed=3)
+    t = ctx.treemake(x, y, z, 500)
+    t.treemoments(q, 7)
+    p = B.params(B.SCREENED, B.CONSISTENT, B.MIXED, kappa=1.5, acc=0.5)
+    buf = np.full(20000, 7.0)
+    got = t.evaluate(p, out=buf)
+    assert got is buf
+    np.testing.assert_array_equal(buf, t.evaluate(p))
+    pts = np.random.default_rng(4).uniform(0.0, 1.0, (300, 3))
+    pbuf = np.empty(300)
+    np.testing.assert_array_equal(t.evaluate(p, points=pts, out=pbuf), t.evaluate(p, points=pts))
+    with pytest.raises(ValueError):
+        t.evaluate(p, out=np.zeros(20000, dtype=np.float32))
+    with pytest.raises(ValueError):
+        t.evaluate(p, out=np.zeros(19999))
+
+
 def test_whole_pipeline_host_buffers(ctx, orc):
     import bit_b200 as B
     from bit_b200 import workloads
