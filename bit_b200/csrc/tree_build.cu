@@ -6,11 +6,12 @@
 // reference runs a short sequential program of up to seven bisections (treedivide,
 // src/tree3d.cpp:1163-1304), each needing the member count and bounding box of both
 // halves of the slot it splits.  Here every node keeps the results of its completed
-// bisections; a one-thread-per-node "decide" kernel replays the program from the start
-// on those cached results until it reaches the first bisection it has no result for,
-// and a "pass" kernel over all members of the level's nodes computes that bisection's
-// counts and bounding boxes (block reduction + atomics; min/max are order independent,
-// so the result is exact).  Members carry a slot label; a final stable counting scatter
+// bisections; a one-thread "decide" step replays the program from the start on those
+// cached results until it reaches the first bisection it has no result for, and a
+// "pass" kernel over all members of the level's nodes computes that bisection's counts
+// and bounding boxes (block reduction + atomics; min/max are order independent, so the
+// result is exact).  The first decision of a level is a kernel of its own; each later one
+// is made inside the pass, by the CTA that finishes the node's last chunk.  Members carry a slot label; a final stable counting scatter
 // lays each node's children out contiguously in slot order, members in ascending
 // original index (the reference's member order).  Field arithmetic (midpoints, aspect
 // ratios, sqradius) is the reference's, with no FMA contraction.
