@@ -27,6 +27,7 @@ namespace {
 
 constexpr int CH = 2048;  // members per chunk (one block)
 constexpr int TB = 256;   // threads per block
+static_assert(CH % TB == 0, "a chunk is a whole number of block strides");
 
 __device__ __forceinline__ unsigned long long okey(double v) {
   long long b = __double_as_longlong(v);
@@ -389,8 +390,20 @@ __global__ void __launch_bounds__(TB, 6) k_split_pass(const int2* chunks, const 
   unsigned long long mn[2][3], mx[2][3];
   for (int h = 0; h < 2; h++)
     for (int d = 0; d < 3; d++) { mn[h][d] = ~0ULL; mx[h][d] = 0ULL; }
-  for (int e = ck.y + threadIdx.x; e < e1; e += TB) {
-    int l = lab[e];
+  // this thread's members e = ck.y + tid + k TB: every label first, then the unrolled
+  // loop, so the members' loads overlap instead of waiting one after the other
+  constexpr int PER = CH / TB;
+  signed char lb[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const int e = ck.y + threadIdx.x + k * TB;
+    lb[k] = e < e1 ? lab[e] : (signed char)-128;  // no slot has label -128
+  }
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    const int e = ck.y + threadIdx.x + k * TB;
+    int l = lb[k];
+    if (l == -128) continue;
     if (hp && l == pv.src) {
       l = (coord(pv.dir, sx, sy, sz, e) <= pv.mid) ? pv.c1 : pc2;
       lab[e] = (signed char)l;
