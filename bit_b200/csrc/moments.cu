@@ -122,24 +122,37 @@ __device__ int canon_degree(int t, int nt) {
   return i + j + t;
 }
 
-// Per node: the sum of its chunks' partials, in chunk order.  The FP32 copy is normalised
-// by h^degree, h = 2^mom32_scale_exp(sqradius) (exact: an exponent shift).
-__global__ void k_moments_reduce(const int* node_c0, const int* node_c1, const int* node_T,
-                                 const long long* mom_off, const double4* nodec,
-                                 const double* part, double* mom64, float* mom32) {
+constexpr int kReduceSlices = 4;  // chunk-sum slices per term (a top node has ~n/1024 chunks)
+
+// Per node: the sum of its chunks' partials.  Slice k of term t sums chunks c0 + k,
+// c0 + k + 4, ... in order and the slices are added in slice order, so the result is fixed;
+// the slices shorten the serial sums of the top nodes, which set the kernel's length.
+// The FP32 copy is normalised by h^degree, h = 2^mom32_scale_exp(sqradius) (exact: an
+// exponent shift).
+__global__ void __launch_bounds__(256 * kReduceSlices)
+    k_moments_reduce(const int* node_c0, const int* node_c1, const int* node_T,
+                     const long long* mom_off, const double4* nodec, const double* part,
+                     double* mom64, float* mom32) {
   constexpr int TMAX = num_terms(kNtermsMax);
+  static_assert(TMAX <= 256, "one slice of 256 threads covers every term");
+  __shared__ double s_part[kReduceSlices][256];
   const int node = blockIdx.x;
   const int c0 = node_c0[node], c1 = node_c1[node], T = node_T[node];
-  const long long o = mom_off[node];
+  const int t = threadIdx.x & 255, slice = threadIdx.x >> 8;
+  if (t < T) {
+    double s = 0.0;
+    for (int c = c0 + slice; c < c1; c += kReduceSlices) s += part[(long long)c * TMAX + t];
+    s_part[slice][t] = s;
+  }
+  __syncthreads();
+  if (slice != 0 || t >= T) return;
+  double s = s_part[0][t];
+  for (int k = 1; k < kReduceSlices; k++) s += s_part[k][t];
   int nt = 1;
   while (num_terms(nt) < T) nt++;
-  const int e = mom32_scale_exp(nodec[node].w);
-  for (int t = threadIdx.x; t < T; t += blockDim.x) {
-    double s = 0.0;
-    for (int c = c0; c < c1; c++) s += part[(long long)c * TMAX + t];
-    mom64[o + t] = s;
-    mom32[o + t] = (float)ldexp(s, -e * canon_degree(t, nt));
-  }
+  const long long o = mom_off[node];
+  mom64[o + t] = s;
+  mom32[o + t] = (float)ldexp(s, -mom32_scale_exp(nodec[node].w) * canon_degree(t, nt));
 }
 
 __global__ void k_gather_charges(int n, const int* perm, const double* q, const double* w,
@@ -257,7 +270,7 @@ void tree_moments_sys(Tree* t, const std::vector<int>& nt_sys) {
 #undef CASE
     }
   }
-  count_launch(), k_moments_reduce<<<t->numtree, 256, 0, s>>>(t->mplan_c0.p, t->mplan_c1.p, t->mplan_T.p,
+  count_launch(), k_moments_reduce<<<t->numtree, 256 * kReduceSlices, 0, s>>>(t->mplan_c0.p, t->mplan_c1.p, t->mplan_T.p,
                                                               t->mom_off.p, t->nodec.p,
                                                               t->mplan_part.p, t->mom64.p,
                                                               t->mom32.p);
