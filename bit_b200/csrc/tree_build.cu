@@ -373,9 +373,10 @@ struct DecideArgs {
 // 6 CTAs per SM as without the decision (40 registers); whatever the call to decide_node
 // needs beyond that is spilled on the deciding thread's path only
 __global__ void __launch_bounds__(TB, 6) k_split_pass(const int2* chunks, const int* nch, int a, const int* start,
-                                                   const int* nummemb, const double* sx,
-                                                   const double* sy, const double* sz,
-                                                   signed char* lab, SplitState* st,
+                                                   const int* nummemb, const double* __restrict__ sx,
+                                                   const double* __restrict__ sy,
+                                                   const double* __restrict__ sz,
+                                                   signed char* __restrict__ lab, SplitState* st,
                                                    SplitAcc* acc, DecideArgs da) {
   if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
@@ -586,13 +587,18 @@ __global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, const int* n
   }
 }
 
+// (restrict: the two copies never overlap, so a thread's members' loads need not wait
+// for its earlier stores)
 __global__ void k_copy_back(const int2* chunks, const int* nch, int a, const int* start, const int* nummemb,
-                            const int* perm2, const double* sx2, const double* sy2,
-                            const double* sz2, int* perm, double* sx, double* sy, double* sz) {
+                            const int* __restrict__ perm2, const double* __restrict__ sx2,
+                            const double* __restrict__ sy2, const double* __restrict__ sz2,
+                            int* __restrict__ perm, double* __restrict__ sx,
+                            double* __restrict__ sy, double* __restrict__ sz) {
   if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
   const int node = a + ck.x;
   const int e1 = min(ck.y + CH, start[node] + nummemb[node]);
+#pragma unroll
   for (int e = ck.y + threadIdx.x; e < e1; e += TB) {
     perm[e] = perm2[e]; sx[e] = sx2[e]; sy[e] = sy2[e]; sz[e] = sz2[e];
   }
