@@ -544,11 +544,13 @@ __global__ void __launch_bounds__(TB) k_scatter_offsets(int a, const int* start,
 
 // Stable scatter of each chunk's members to their child's range (order kept).
 __global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, const int* nch, int a, const int* start,
-                                                const int* nummemb, const signed char* lab,
-                                                const int* coff, const int* perm,
-                                                const double* sx, const double* sy,
-                                                const double* sz, int* perm2, double* sx2,
-                                                double* sy2, double* sz2) {
+                                                const int* nummemb, const signed char* __restrict__ lab,
+                                                const int* coff, const int* __restrict__ perm,
+                                                const double* __restrict__ sx,
+                                                const double* __restrict__ sy,
+                                                const double* __restrict__ sz, int* __restrict__ perm2,
+                                                double* __restrict__ sx2, double* __restrict__ sy2,
+                                                double* __restrict__ sz2) {
   if ((int)blockIdx.x >= *nch) return;  // the grid is sized from a bound
   const int2 ck = chunks[blockIdx.x];
   const int node = a + ck.x;
@@ -562,6 +564,10 @@ __global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, const int* n
   for (int t0 = ck.y; t0 < e1; t0 += TB) {
     int e = t0 + threadIdx.x;
     int l = e < e1 ? lab[e] : -2;
+    // the member's record loads while its rank among the block's members is formed
+    int pv = 0;
+    double xv = 0.0, yv = 0.0, zv = 0.0;
+    if (l >= 0) { pv = perm[e]; xv = sx[e]; yv = sy[e]; zv = sz[e]; }
     int my_rank = 0;
     for (int v = 0; v < 8; v++) {
       unsigned m = __ballot_sync(0xffffffffu, l == v);
@@ -572,10 +578,10 @@ __global__ void __launch_bounds__(TB) k_scatter(const int2* chunks, const int* n
     if (l >= 0) {
       int dst = run[l] + my_rank;
       for (int q = 0; q < w; q++) dst += wcnt[q][l];
-      perm2[dst] = perm[e];
-      sx2[dst] = sx[e];
-      sy2[dst] = sy[e];
-      sz2[dst] = sz[e];
+      perm2[dst] = pv;
+      sx2[dst] = xv;
+      sy2[dst] = yv;
+      sz2[dst] = zv;
     }
     __syncthreads();
     if (threadIdx.x < 8) {
