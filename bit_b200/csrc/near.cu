@@ -121,8 +121,9 @@ __device__ __forceinline__ T shfl_sum(T v, int tpt) {
 // reference's rules (including its r^2 <= 1e-14 skip, which only such pairs can meet:
 // thr >= 2e-14).  Every other pair keeps at most ~4e-6 relative error, far below 1e-6 of a
 // target's total.  Close pairs can only occur where a target lies within r_t of the source
-// leaf's box (its own leaf, or a neighbour's boundary), so a warp runs the checked loop on
-// those tiles and the plain loop, with no test at all, everywhere else.
+// leaf's box (its own leaf, or a neighbour's boundary), and only where the kernel's del is
+// below thr (FP32 r^2 >= del), so a warp runs the checked loop on those tiles and the plain
+// loop, with no test at all, everywhere else.
 constexpr float kCloseFrac = 1.0f / 1024.0f;  // (1/32)^2
 constexpr float kThrMin = 2e-14f;             // above the 1e-14 skip of src/constants.h:35
 
@@ -363,7 +364,11 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
       const int units = cnt * tpt;
       const int lt = __ffs(tpt) - 1;
       // close-pair checks are needed only where a target comes within r_t of this leaf's box
-      const float thr = fmaxf((float)c.w * kCloseFrac, kThrMin);  // r_t^2 = sqradius / 1024
+      float thr = fmaxf((float)c.w * kCloseFrac, kThrMin);  // r_t^2 = sqradius / 1024
+      // the FP32 r^2 is at least del (fmaf of non-negative squares onto del), so where del
+      // reaches thr no pair of this tile can be close: thr = 0 keeps every warp on the
+      // plain loop (no box distance is below 0), which is then exact
+      if (!(del < thr)) thr = 0.f;
       const float4 hb = a.nodeh[node];
       const double4* s64 = a.src64 + j0 + toff;
       for (int u0 = 0; u0 < units; u0 += NT) {
