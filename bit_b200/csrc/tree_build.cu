@@ -302,17 +302,20 @@ __device__ __noinline__ void decide_node(int a, int li, const double* fields, co
   if (!S->active) return;
   SplitAcc* A = &acc[li];
   if (S->has_cur) {
+    // The sums arrived as atomics in L2 from other CTAs of this launch (when the decision
+    // is made inside k_split_pass); __ldcg reads them there, never from a line this SM's
+    // L1 may hold from a neighbouring node's decision.
     int d = S->ndone;
     for (int h = 0; h < 2; h++) {
-      S->res_cnt[d][h] = A->cnt[h];
+      S->res_cnt[d][h] = __ldcg(&A->cnt[h]);
       for (int q = 0; q < 3; q++) {
-        S->res_bb[d][h][2 * q] = okey_inv(A->mn[h][q]);
-        S->res_bb[d][h][2 * q + 1] = okey_inv(A->mx[h][q]);
+        S->res_bb[d][h][2 * q] = okey_inv(__ldcg(&A->mn[h][q]));
+        S->res_bb[d][h][2 * q + 1] = okey_inv(__ldcg(&A->mx[h][q]));
       }
     }
     S->ndone = d + 1;
     S->prev = S->cur;
-    S->prev_c2eff = A->cnt[0] > 0 ? S->cur.c2 : S->cur.c1;
+    S->prev_c2eff = S->res_cnt[d][0] > 0 ? S->cur.c2 : S->cur.c1;
     S->has_prev = 1;
     S->has_cur = 0;
     acc_reset(A);
