@@ -6,11 +6,16 @@ build (N0 = 1000), FP64 moments for p = 8 (nterms 9), then the potential at ever
 particle twice: screened kernel exp(-kappa r)/r with kappa = 1, and regularised Coulomb
 1/sqrt(r^2 + delta^2) with delta = 0.005, both with MAC theta = 0.7.  evals = 2 N per step.
 
-value  -- evals/s with the inputs resident in HBM (mixed precision: FP32 near/far field in
-          cluster-centred coordinates with compensated accumulation; FP64 MAC and moments)
+value  -- evals/s of the plain FP64 GPU path (the reference's arithmetic) with the inputs
+          resident in HBM
 e2e    -- the same through the C ABI with host buffers (H2D inputs, D2H potentials inside
           the timed region)
-fp64   -- the plain FP64 GPU path on the same step, for the mixed-vs-FP64 speed-up
+mixed  -- the mixed-precision path on the same step (FP32 near/far field in cluster-centred
+          coordinates with compensated accumulation; FP64 MAC and moments), its e2e and its
+          speed-up over FP64
+accuracy_matched -- the clustered step, the boundary-integral solve, the batched systems
+          and the serving stream at (p, theta) where the FP64 treecode reaches 1e-6 against
+          the FP64 direct sum: FP64 and mixed throughput, errors and ratios
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bit|reference] [--n N]
 
@@ -38,6 +43,17 @@ ACC = 0.7           # theta
 KAPPA = 1.0
 DEL = 0.005 ** 2    # delta^2
 FLOPS_NEAR = {"screened": 14, "coulomb": 11}     # per near pair (rsqrt, exp counted as 1)
+# Accuracy-matched parameters: (p, theta, N0) at which the plain FP64 treecode reaches 1e-6
+# relative L2 against the FP64 direct sum on these workloads (measured; the run reports
+# the errors it reaches)
+MATCHED_C2 = dict(nterms=10, acc=0.15, maxmemb=1000)
+MATCHED_BIE = dict(nterms=10, acc=0.15, maxmemb=500)
+MATCHED_BATCH_ACC = {5: 0.05, 7: 0.1, 9: 0.15}   # theta by nterms (p = 4, 6, 8)
+# DRAM bytes (read + write) per launch of the full-size kernels, from single-kernel ncu
+# captures of the 200k clustered case scaled by the pairs each launch processes; None
+# where no capture of the current kernel exists.
+TRAFFIC = {}
+TRAFFIC_SOURCE = None
 METRIC = "treecode evals/s (clustered N=2M, p=8, theta=0.7, N0=1000, screened+Coulomb)"
 
 
@@ -102,7 +118,6 @@ def workload(n, seed):
 def run_bit(args):
     import torch
     import bit_b200 as B
-    from bit_b200 import workloads
 
     from bit_b200 import replicas
     rank, world, local = replicas.rank_info()
@@ -116,15 +131,17 @@ def run_bit(args):
     out_c = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
     ctx = B.Context(local, stream=stream.cuda_stream)
+    # measured CUDA-core FMA peaks of this device: the roofline denominators
+    peaks = {"fp64": ctx.fma_peak(B.FP64) / 1e12, "fp32": ctx.fma_peak(B.MIXED) / 1e12}
 
-    def step(prec, keep=False):
-        t = ctx.treemake_device(n, X[0].data_ptr(), X[1].data_ptr(), X[2].data_ptr(), MAXMEMB)
+    def step(prec, keep=False, nterms=NTERMS, maxmemb=MAXMEMB, acc=ACC):
+        t = ctx.treemake_device(n, X[0].data_ptr(), X[1].data_ptr(), X[2].data_ptr(), maxmemb)
         t.set_charges_device(X[3].data_ptr())
-        t.moments(NTERMS)
-        t.evaluate_device(B.params(B.SCREENED, B.CONSISTENT, prec, kappa=KAPPA, acc=ACC),
+        t.moments(nterms)
+        t.evaluate_device(B.params(B.SCREENED, B.CONSISTENT, prec, kappa=KAPPA, acc=acc),
                           out_s.data_ptr())
         st_s = t.stats() if keep else None
-        t.evaluate_device(B.params(B.COULOMB, B.CONSISTENT, prec, del_=DEL, acc=ACC),
+        t.evaluate_device(B.params(B.COULOMB, B.CONSISTENT, prec, del_=DEL, acc=acc),
                           out_c.data_ptr())
         st_c = t.stats() if keep else None
         if keep:
@@ -134,9 +151,9 @@ def run_bit(args):
 
     launches = {}
 
-    def timed(prec, steps, warmup):
+    def timed(prec, steps, warmup, **kw):
         for _ in range(warmup):
-            step(prec)
+            step(prec, **kw)
         torch.cuda.synchronize()
         replicas.barrier(dist)
         torch.cuda.synchronize()
@@ -145,148 +162,228 @@ def run_bit(args):
         l0 = B.kernel_launches()
         e0.record(stream)
         for _ in range(steps):
-            step(prec)
+            step(prec, **kw)
         e1.record(stream)
         torch.cuda.synchronize()
         launches[prec] = (B.kernel_launches() - l0) // steps
         return replicas.max_over_ranks(e0.elapsed_time(e1) / steps, dist, dev)
 
-    # mixed precision (the product path): timed with clocks sampled
+    # plain FP64 (the headline: the reference's arithmetic), timed with clocks sampled
     with ClockSampler(local) as clk:
-        ms = timed(B.MIXED, args.steps, args.warmup)
+        ms64 = timed(B.FP64, args.steps, args.warmup)
     clocks = clk.summary()
-    ms64 = timed(B.FP64, max(1, args.steps // 2), 1)
+    ms32 = timed(B.MIXED, args.steps, args.warmup)
     # per-kernel device times of one step (events on the library's stream)
+    t, st64_s, st64_c = step(B.FP64, keep=True)
+    res64_s = out_s.cpu().numpy()
+    res64_c = out_c.cpu().numpy()
+    t.treeempty()
     t, st_s, st_c = step(B.MIXED, keep=True)
     res_s = out_s.cpu().numpy()
     res_c = out_c.cpu().numpy()
     t.treeempty()
-    _, st64_s, st64_c = step(B.FP64, keep=True)
-    res64_s = out_s.cpu().numpy()
-    res64_c = out_c.cpu().numpy()
 
     # e2e through the C ABI with host buffers: the caller's input arrays, and two result
     # arrays it allocates once and reuses every step
     host_s, host_c = np.zeros(n), np.zeros(n)
 
-    def e2e_step():
+    def e2e_step(prec):
         t = ctx.treemake(x, y, z, MAXMEMB)
         t.treemoments(q, NTERMS)
-        a = t.evaluate(B.params(B.SCREENED, B.CONSISTENT, B.MIXED, kappa=KAPPA, acc=ACC), out=host_s)
-        b = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, B.MIXED, del_=DEL, acc=ACC), out=host_c)
+        a = t.evaluate(B.params(B.SCREENED, B.CONSISTENT, prec, kappa=KAPPA, acc=ACC), out=host_s)
+        b = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, prec, del_=DEL, acc=ACC), out=host_c)
         t.treeempty()
         return a, b
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
-    torch.cuda.synchronize()
-    replicas.barrier(dist)
-    t0 = time.perf_counter()
-    e2e_steps = max(1, args.steps // 2)
-    for _ in range(e2e_steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_ms = replicas.max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, dist, dev)
+
+    def e2e_timed(prec):
+        for _ in range(max(1, args.warmup // 2)):
+            e2e_step(prec)
+        torch.cuda.synchronize()
+        replicas.barrier(dist)
+        t0 = time.perf_counter()
+        steps = max(1, args.steps // 2)
+        for _ in range(steps):
+            e2e_step(prec)
+        torch.cuda.synchronize()
+        return replicas.max_over_ranks((time.perf_counter() - t0) * 1e3 / steps, dist, dev)
+    e2e64_ms = e2e_timed(B.FP64)
+    e2e32_ms = e2e_timed(B.MIXED)
+
+    matched = run_matched_c2(step, timed, ctx, x, y, z, q, out_s, out_c, args) if args.matched else None
 
     if rank != 0:
         replicas.finish(dist)
         return
 
     evals = 2 * n * world
+    e2e_in = 4 * n * 8
+    e2e_out = 2 * n * 8
     line = {
-        "metric": METRIC, "value": evals / (ms * 1e-3), "unit": "evals/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 near/far field, f64 MAC+moments",
+        "metric": METRIC, "value": evals / (ms64 * 1e-3), "unit": "evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms64, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded clustered blobs)",
         "config": {"workload": "clustered evaluation N=2,000,000 (80% in 8 Gaussian blobs sigma 0.1, "
                                "20% uniform), p=8, theta=0.7, N0=1000, screened kappa=1 + Coulomb "
-                               "delta=0.005, all particles as targets",
+                               "delta=0.005, all particles as targets; plain FP64 GPU path",
                    "n": n, "nterms": NTERMS, "maxmemb": MAXMEMB, "acc": ACC,
                    "parallelism": f"replicas x{world}",
                    "l2": "inputs (128 MB coordinates+charges, 64 MB sorted FP64 sources) exceed the "
                          "126 MB L2; no flush"},
         "clocks": clocks,
-        "fp64": {"value": evals / (ms64 * 1e-3), "ms_per_step": ms64,
-                 "mixed_speedup": ms64 / ms},
+        "e2e": {"value": evals / (e2e64_ms * 1e-3), "unit": "evals/s",
+                "h2d_bytes_per_step": e2e_in, "d2h_bytes_per_step": e2e_out,
+                "ms_per_step": e2e64_ms},
+        "mixed": {"dtype": "f32 near/far field in cluster-centred coordinates with compensated "
+                           "accumulation, f64 MAC+moments",
+                  "value": evals / (ms32 * 1e-3), "ms_per_step": ms32,
+                  "speedup_vs_fp64": ms64 / ms32,
+                  "e2e": {"value": evals / (e2e32_ms * 1e-3), "unit": "evals/s",
+                          "h2d_bytes_per_step": e2e_in, "d2h_bytes_per_step": e2e_out,
+                          "ms_per_step": e2e32_ms},
+                  "e2e_speedup_vs_fp64": e2e64_ms / e2e32_ms,
+                  "gpu_launches_per_step": launches[B.MIXED]},
+        "fma_peaks_tflops": peaks,
     }
-    e2e_in = 4 * n * 8
-    e2e_out = 2 * n * 8
-    line["e2e"] = {"value": 2 * n * world / (e2e_ms * 1e-3), "unit": "evals/s",
-                   "h2d_bytes_per_step": e2e_in, "d2h_bytes_per_step": e2e_out,
-                   "ms_per_step": e2e_ms}
-    # per-phase device times and interaction counts (mixed, screened + Coulomb)
+    # per-phase device times and interaction counts (screened + Coulomb)
     phases = {}
-    for name, st in (("screened", st_s), ("coulomb", st_c)):
-        phases[name] = {k: st[k] for k in ("t_far", "t_near", "t_lists", "far_pairs", "near_pairs",
+    for prec, (ss, sc) in (("fp64", (st64_s, st64_c)), ("mixed", (st_s, st_c))):
+        ph = {}
+        for name, st in (("screened", ss), ("coulomb", sc)):
+            ph[name] = {k: st[k] for k in ("t_far", "t_near", "t_lists", "far_pairs", "near_pairs",
                                            "far_entries", "near_entries", "batches",
                                            "lists_shared")}
-    phases["build_s"] = st_s["t_build"]
-    phases["moments_s"] = st_s["t_moments"]
-    phases["numtree"] = st_s["numtree"]
-    phases["fp64"] = {name: {"t_far": s["t_far"], "t_near": s["t_near"]}
-                      for name, s in (("screened", st64_s), ("coulomb", st64_c))}
+        ph["build_s"] = ss["t_build"]
+        ph["moments_s"] = ss["t_moments"]
+        ph["numtree"] = ss["numtree"]
+        phases[prec] = ph
     line["phases"] = phases
-    # roofline of the dominant kernel, the screened far field (k_far, FP32 FMA pipe), and of
-    # the screened near field (FP32 + MUFU) beside it
-    peak = fp32_peak_from_clock(clocks)
+    # rooflines: the dominant kernel of the FP64 step first, then the others
     fpp = far_flops_per_pair(NTERMS)
-    far_flops = fpp["screened"] * st_s["far_pairs"]
-    far_ach = far_flops / st_s["t_far"] / 1e12
-    line["roofline"] = {"bound": "fp32", "kernel": "k_far<nterms 9, SCREENED, float>",
-                        "achieved": far_ach, "peak": peak["tflops"], "unit": "TFLOP/s",
-                        "frac": far_ach / peak["tflops"], "peak_source": peak["source"],
-                        "traffic": profiled_traffic("k_far_screened_f32"),
-                        "traffic_unit": "bytes per launch (dram read+write, one ncu pass at full size, "
-                                        "profiles/launches_clustered2M_step.md)",
-                        "algorithmic": f"{fpp['screened']} flops (the reference's screened recurrence "
-                                       f"to degree 8 and the moment dot product) x {st_s['far_pairs']} "
-                                       "(target, cluster) pairs per launch"}
-    pairs = st_s["near_pairs"] - n
-    t_near = st_s["t_near"]
-    near_ach = FLOPS_NEAR["screened"] * pairs / t_near / 1e12
-    line["roofline_near"] = {"bound": "fp32+mufu", "kernel": "k_near<SCREENED, F32>",
-                             "achieved": near_ach, "peak": peak["tflops"], "unit": "TFLOP/s",
-                             "frac": near_ach / peak["tflops"],
-                             "mufu_frac": (2 * pairs / t_near) / peak["mufu_ops"],
-                             "traffic": profiled_traffic("k_near_screened_f32"),
-                             "algorithmic": f"{FLOPS_NEAR['screened']} flops x {pairs} near pairs per launch"}
+    roofs = []
+    for prec, st, pk in (("fp64", st64_s, peaks["fp64"]), ("fp64", st64_c, peaks["fp64"]),
+                         ("mixed", st_s, peaks["fp32"]), ("mixed", st_c, peaks["fp32"])):
+        kname = "screened" if st is st64_s or st is st_s else "coulomb"
+        roofs.append(roofline_far(prec, kname, st, fpp[kname], pk))
+        roofs.append(roofline_near(prec, kname, st, n, pk))
+    fp64_roofs = sorted((r for r in roofs if r["precision"] == "fp64"), key=lambda r: -r["seconds"])
+    line["roofline"] = fp64_roofs[0]
+    line["roofline_others"] = [r for r in roofs if r is not fp64_roofs[0]]
     # accuracy of this step against the FP64 GPU path and the FP64 direct sum (sampled)
     line["accuracy"] = accuracy(ctx, x, y, z, q, res_s, res_c, res64_s, res64_c, args)
+    if matched is not None:
+        line["accuracy_matched"] = {"clustered_2M": matched}
     if args.bie:
         line["bie"] = run_bie(ctx, args)
+        if args.matched:
+            line["accuracy_matched"]["bie"] = run_bie(ctx, args, **MATCHED_BIE)
     if args.batched:
         line["batched"] = run_batched(ctx, args, dev)
+        if args.matched:
+            line["accuracy_matched"]["batched"] = run_batched(ctx, args, dev, acc_by_nterms=MATCHED_BATCH_ACC)
     if args.serve_requests:
         line["serving"] = run_serving(ctx, args)
+        if args.matched:
+            line["accuracy_matched"]["serving"] = run_serving(ctx, args, matched=True)
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x, y, z, q, n, args)
-    line["gpu_launches"] = launches[B.MIXED] * args.steps
-    line["gpu_launches_per_step"] = launches[B.MIXED]
+    line["gpu_launches"] = launches[B.FP64] * args.steps
+    line["gpu_launches_per_step"] = launches[B.FP64]
     print(json.dumps(line), flush=True)
     replicas.finish(dist)
 
 
-def run_bie(ctx, args):
+def roofline_far(prec, kname, st, flops_pair, peak_tflops):
+    """Far field (k_far): the reference recurrence's flops per (target, cluster) pair, as the
+    generator counts them, times the pairs of the launch, over its device time."""
+    ach = flops_pair * st["far_pairs"] / st["t_far"] / 1e12
+    t = "double" if prec == "fp64" else "float"
+    key = f"k_far<{NTERMS}, {kname.upper()}, {t}>"
+    return {"bound": "fp64" if prec == "fp64" else "fp32", "kernel": key, "precision": prec,
+            "achieved": ach, "peak": peak_tflops, "unit": "TFLOP/s", "frac": ach / peak_tflops,
+            "peak_source": f"measured {'FP64 DFMA' if prec == 'fp64' else 'FP32 FFMA'} throughput of "
+                           "this device (bit_device_fma_peak: FMA-chain kernel, CUDA events)",
+            "traffic": TRAFFIC.get(key), "traffic_unit": "bytes per launch (dram read+write)",
+            "traffic_source": TRAFFIC_SOURCE if TRAFFIC.get(key) else None,
+            "seconds": st["t_far"],
+            "algorithmic": f"{flops_pair} flops (the reference's {kname} recurrence to degree "
+                           f"{NTERMS - 1} and the moment dot product) x {st['far_pairs']} "
+                           "(target, cluster) pairs per launch"}
+
+
+def roofline_near(prec, kname, st, n, peak_tflops):
+    """Near field (k_near): the per-pair flops of the reference's leaf loop (rsqrt and exp
+    counted as 1) times the (target, source) pairs of the launch, self pairs excluded."""
+    pairs = st["near_pairs"] - n
+    fl = FLOPS_NEAR[kname]
+    ach = fl * pairs / st["t_near"] / 1e12
+    t = "F64" if prec == "fp64" else "F32"
+    key = f"k_near<{kname.upper()}, {t}>"
+    return {"bound": "fp64" if prec == "fp64" else "fp32+mufu", "kernel": key, "precision": prec,
+            "achieved": ach, "peak": peak_tflops, "unit": "TFLOP/s", "frac": ach / peak_tflops,
+            "peak_source": f"measured {'FP64 DFMA' if prec == 'fp64' else 'FP32 FFMA'} throughput of "
+                           "this device (bit_device_fma_peak)",
+            "traffic": TRAFFIC.get(key), "traffic_unit": "bytes per launch (dram read+write)",
+            "traffic_source": TRAFFIC_SOURCE if TRAFFIC.get(key) else None,
+            "seconds": st["t_near"],
+            "algorithmic": f"{fl} flops x {pairs} near pairs per launch"}
+
+
+def run_matched_c2(step, timed, ctx, x, y, z, q, out_s, out_c, args):
+    """The clustered 2M step at (p, theta, N0) where the plain FP64 treecode reaches 1e-6
+    relative L2 against the FP64 direct sum: FP64 and mixed evals/s and errors."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    kw = dict(nterms=MATCHED_C2["nterms"], maxmemb=MATCHED_C2["maxmemb"], acc=MATCHED_C2["acc"])
+    steps = max(2, args.steps // 4)
+    ms64 = timed(B.FP64, steps, 1, **kw)
+    step(B.FP64, **kw)
+    r64 = (out_s.cpu().numpy(), out_c.cpu().numpy())
+    ms32 = timed(B.MIXED, steps, 1, **kw)
+    step(B.MIXED, **kw)
+    r32 = (out_s.cpu().numpy(), out_c.cpu().numpy())
+    tg = workloads.sample_targets(len(x), args.sample, seed=11)
+    ds = (ctx.direct(x, y, z, q, B.params(B.SCREENED, B.CONSISTENT, B.FP64, kappa=KAPPA), tg),
+          ctx.direct(x, y, z, q, B.params(B.COULOMB, B.CONSISTENT, B.FP64, del_=DEL), tg))
+    evals = 2 * len(x)
+    out = {"workload": f"clustered N={len(x)}, screened kappa=1 + Coulomb delta=0.005, "
+                       f"p={kw['nterms'] - 1}, theta={kw['acc']}, N0={kw['maxmemb']}",
+           "fp64": {"evals_per_s": evals / (ms64 * 1e-3), "ms_per_step": ms64},
+           "mixed": {"evals_per_s": evals / (ms32 * 1e-3), "ms_per_step": ms32},
+           "mixed_speedup": ms64 / ms32, "error_targets": int(len(tg))}
+    for i, name in enumerate(("screened", "coulomb")):
+        out[name] = {"fp64_vs_direct": workloads.rel_l2(r64[i][tg], ds[i]),
+                     "mixed_vs_direct": workloads.rel_l2(r32[i][tg], ds[i]),
+                     "mixed_vs_fp64": workloads.rel_l2(r32[i], r64[i])}
+    errs = [out[k][m] for k in ("screened", "coulomb") for m in ("fp64_vs_direct", "mixed_vs_direct")]
+    out["max_error_vs_direct"] = max(errs)
+    out["at_most_1e-6"] = max(errs) <= 1e-6
+    return out
+
+
+def run_bie(ctx, args, nterms=7, acc=0.5, maxmemb=500):
     """Boundary-integral GMRES solve: icosphere level 6 (81,920 centroids, weights = areas),
     (I/2 + K) sigma = f, K the area-weighted screened kernel (kappa = 1) regularised with
     delta = mean edge length, f = real spherical harmonics of degree <= 8 with seeded
-    N(0,1) coefficients; p = 6, theta = 0.5, N0 = 500, GMRES(50) to 1e-8.  Plain FP64
-    matvecs vs FP32 matvecs inside FP64 iterative refinement; device seconds per solve."""
+    N(0,1) coefficients; p = 6, theta = 0.5, N0 = 500 (or the given p, theta, N0),
+    GMRES(50) to 1e-8.  Plain FP64 matvecs vs FP32 matvecs inside FP64 iterative
+    refinement; device seconds per solve."""
     import bit_b200 as B
     from bit_b200 import workloads
     cen, area, h = workloads.icosphere(args.bie_level)
     f = workloads.sh_rhs(cen, lmax=8, seed=1)
     cx, cy, cz = [np.ascontiguousarray(cen[:, a]) for a in range(3)]
-    p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=h * h, kappa=1.0, acc=0.5)
-    t = ctx.treemake(cx, cy, cz, 500)
+    p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=h * h, kappa=1.0, acc=acc)
+    t = ctx.treemake(cx, cy, cz, maxmemb)
     out = {"workload": f"icosphere level {args.bie_level} ({len(cen)} nodes), screened kappa=1 "
-                       f"regularised with delta = mean edge ({h:.4g}), p=6, theta=0.5, N0=500, "
-                       "GMRES(50) to 1e-8", "n": int(len(cen))}
+                       f"regularised with delta = mean edge ({h:.4g}), p={nterms - 1}, "
+                       f"theta={acc}, N0={maxmemb}, GMRES(50) to 1e-8", "n": int(len(cen))}
     tg = workloads.sample_targets(len(cen), 2000, seed=4)
     for name, prec in (("fp64", B.FP64), ("mixed", B.MIXED)):
-        t.bie_solve(p, 7, 0.5, area, f, restart=50, tol=1e-8, precision=prec)  # warm-up
+        t.bie_solve(p, nterms, 0.5, area, f, restart=50, tol=1e-8, precision=prec)  # warm-up
         secs, info, sol, st = [], None, None, None
         for _ in range(args.bie_solves):
-            sol, info, st = t.bie_solve(p, 7, 0.5, area, f, restart=50, tol=1e-8, precision=prec)
+            sol, info, st = t.bie_solve(p, nterms, 0.5, area, f, restart=50, tol=1e-8, precision=prec)
             secs.append(info["seconds"])
         # residual of the solution against the direct-sum operator on sampled rows
         Ks = ctx.direct(cx, cy, cz, area * sol, p, tg)
@@ -297,17 +394,22 @@ def run_bie(ctx, args):
                      "matvecs_fp64": info["matvecs_fp64"], "matvecs_fp32": info["matvecs_fp32"],
                      "relres_treecode": info["relres"], "relres_direct_sum_2000_rows": res}
     out["mixed_speedup"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    errs = [out[k]["relres_direct_sum_2000_rows"] for k in ("fp64", "mixed")]
+    out["max_error_vs_direct"] = max(errs)
+    out["at_most_1e-6"] = max(errs) <= 1e-6
     t.treeempty()
     return out
 
 
-def run_batched(ctx, args, dev):
+def run_batched(ctx, args, dev, acc_by_nterms=None):
     """Batched uneven systems in one pass: 2048 independent systems, N log-uniform in
     [1e3, 1e5], each uniform in its own unit cube; half regularised Coulomb (delta = 0.01),
     half screened (kappa ~ U[0.5, 4]); p from {4, 6, 8}; theta = 0.6; N0 per (p, kernel)
     from the autotuner.  Mixed precision as one forest (build, moments, far and near
-    launches per class) vs a per-system loop of the plain FP64 path; error vs the FP64
-    direct sum on 1,000 sampled targets per system."""
+    launches per class) vs a per-system loop of the plain FP64 path, and the plain FP64
+    path as one forest (which separates the precision gain from the batching gain); error
+    vs the FP64 direct sum on 1,000 sampled targets per system.  acc_by_nterms: theta per
+    expansion order instead of 0.6 (the accuracy-matched run)."""
     import torch
     import bit_b200 as B
     from bit_b200 import autotune, workloads
@@ -318,7 +420,8 @@ def run_batched(ctx, args, dev):
     for s in systems:
         key = (s["nterms"], s["kernel"])
         if key not in n0:
-            n0[key] = autotune.tune_n0(ctx, s["nterms"], s["kernel"], med, acc=0.6,
+            n0[key] = autotune.tune_n0(ctx, s["nterms"], s["kernel"], med,
+                                       acc=0.6 if acc_by_nterms is None else acc_by_nterms[s["nterms"]],
                                        del_=1e-4 if s["kernel"] == B.COULOMB else 0.0,
                                        kappa=2.0)[0]
     mm = np.array([n0[(s["nterms"], s["kernel"])] for s in systems], dtype=np.int32)
@@ -329,18 +432,25 @@ def run_batched(ctx, args, dev):
                      dtype=torch.float64, device=dev)
     out32 = torch.empty(total, dtype=torch.float64, device=dev)
     out64 = torch.empty(total, dtype=torch.float64, device=dev)
+    outf64 = torch.empty(total, dtype=torch.float64, device=dev)
+
+    def theta(s):
+        return 0.6 if acc_by_nterms is None else acc_by_nterms[s["nterms"]]
 
     def prm(s, prec):
-        return B.params(s["kernel"], B.CONSISTENT, prec, del_=s["del_"], kappa=s["kappa"], acc=0.6)
+        return B.params(s["kernel"], B.CONSISTENT, prec, del_=s["del_"], kappa=s["kappa"], acc=theta(s))
     p32 = [prm(s, B.MIXED) for s in systems]
     p64 = [prm(s, B.FP64) for s in systems]
     ptr = [X[k].data_ptr() for k in range(4)]
 
-    def forest_step():
+    def forest_step(prec=B.MIXED):
         F = ctx.forest_device(sizes, mm, ptr[0], ptr[1], ptr[2])
         F.set_charges_device(ptr[3])
         F.moments(nt)
-        F.evaluate_device(p32, out32.data_ptr())
+        if prec == B.MIXED:
+            F.evaluate_device(p32, out32.data_ptr())
+        else:
+            F.evaluate_device(p64, outf64.data_ptr())
         st = F.stats()
         F.treeempty()
         return st
@@ -369,11 +479,14 @@ def run_batched(ctx, args, dev):
     group, gtimes = autotune.tune_group(ctx, lambda c: timed(forest_step, 1)[0])
     forest_step()  # warm-up
     t32, st = timed(forest_step, 2)
+    forest_step(B.FP64)  # warm-up
+    tf64, _ = timed(lambda: forest_step(B.FP64), 2)
     ctx.set_group_size(0)  # the plain FP64 path in its default configuration
     loop_step(B.FP64, out64)  # warm-up
     t64, _ = timed(lambda: loop_step(B.FP64, out64), 1)
     r32 = out32.cpu().numpy()
     r64 = out64.cpu().numpy()
+    rf64 = outf64.cpu().numpy()
     e32, e64 = [], []
     for i, s in enumerate(systems):
         tg = workloads.sample_targets(int(sizes[i]), 1000, seed=i)
@@ -382,9 +495,14 @@ def run_batched(ctx, args, dev):
         e64.append(workloads.rel_l2(r64[off[i]:off[i + 1]][tg], ds))
     mix_vs_64 = [workloads.rel_l2(r32[off[i]:off[i + 1]], r64[off[i]:off[i + 1]])
                  for i in range(len(systems))]
+    forest_vs_loop = max(workloads.rel_l2(rf64[off[i]:off[i + 1]], r64[off[i]:off[i + 1]])
+                         for i in range(len(systems)))
+    th = ("theta=0.6" if acc_by_nterms is None else
+          "theta by p: " + ", ".join(f"p={k - 1}: {v}" for k, v in sorted(acc_by_nterms.items())))
+    err_all = e32 + e64
     return {"workload": f"{len(systems)} systems, N log-uniform in [1e3, 1e5] (total {total}), "
                         "half Coulomb delta=0.01, half screened kappa~U[0.5,4], p in {4,6,8}, "
-                        "theta=0.6, N0 autotuned per (p, kernel), leaf packing autotuned for the batch",
+                        f"{th}, N0 autotuned per (p, kernel), leaf packing autotuned for the batch",
             "systems": len(systems), "particles": total,
             "n0": {f"nterms{k[0]}_{'coulomb' if k[1] == 0 else 'screened'}": v
                    for k, v in sorted(n0.items())},
@@ -392,17 +510,25 @@ def run_batched(ctx, args, dev):
             "mixed_forest": {"evals_per_s": total / t32, "s_per_step": t32,
                              "far_launches": st["far_launches"], "near_launches": st["near_launches"]},
             "fp64_per_system_loop": {"evals_per_s": total / t64, "s_per_step": t64},
+            "fp64_forest": {"evals_per_s": total / tf64, "s_per_step": tf64,
+                            "max_rel_diff_vs_loop": forest_vs_loop},
             "speedup": t64 / t32,
+            "speedup_precision_only": tf64 / t32,
+            "speedup_batching_only": t64 / tf64,
+            "max_error_vs_direct": float(np.max(err_all)),
+            "at_most_1e-6": bool(np.max(err_all) <= 1e-6),
             "error_vs_direct_1000_per_system": {
                 "mixed_median": float(np.median(e32)), "mixed_max": float(np.max(e32)),
                 "fp64_median": float(np.median(e64)), "fp64_max": float(np.max(e64)),
                 "mixed_vs_fp64_max": float(np.max(mix_vs_64))}}
 
 
-def serving_requests(count, seed, ctx):
+def serving_requests(count, seed, ctx, matched=False):
     """The request stream: 70% evaluate requests (N lognormal, median 20,000, clipped to
     [1e3, 1e6], Gaussian blobs; kernel and parameters as in the batched run) and 30%
-    GMRES solves on icospheres of level 4..7 (system as in the boundary-integral solve)."""
+    GMRES solves on icospheres of level 4..7 (system as in the boundary-integral solve).
+    matched: theta per p of the accuracy-matched batched run, and the accuracy-matched
+    boundary-integral parameters for the solves."""
     import bit_b200 as B
     from bit_b200 import autotune, workloads
     rng = np.random.default_rng(seed)
@@ -416,10 +542,11 @@ def serving_requests(count, seed, ctx):
             nterms = int(rng.choice([4, 6, 8])) + 1
             kappa = 0.0 if coul else float(rng.uniform(0.5, 4.0))
             kern = B.COULOMB if coul else B.SCREENED
-            n0 = autotune.tune_n0(ctx, nterms, kern, 20000, acc=0.6, del_=1e-4 if coul else 0.0,
+            acc = MATCHED_BATCH_ACC[nterms] if matched else 0.6
+            n0 = autotune.tune_n0(ctx, nterms, kern, 20000, acc=acc, del_=1e-4 if coul else 0.0,
                                   kappa=2.0, dist="clustered")[0]
             reqs.append(dict(kind="eval", n=n, data=(x, y, z, q), nterms=nterms, n0=n0,
-                             kernel=kern, del_=1e-4 if coul else 0.0, kappa=kappa))
+                             kernel=kern, del_=1e-4 if coul else 0.0, kappa=kappa, acc=acc))
         else:
             level = int(rng.integers(4, 8))
             if level not in spheres:
@@ -427,8 +554,10 @@ def serving_requests(count, seed, ctx):
             cen, area, h = spheres[level]
             f = workloads.sh_rhs(cen, lmax=8, seed=seed * 100000 + i)
             cx, cy, cz = [np.ascontiguousarray(cen[:, a]) for a in range(3)]
-            reqs.append(dict(kind="solve", n=len(cen), data=(cx, cy, cz, area, f), nterms=7,
-                             n0=500, del_=h * h, level=level))
+            sp = MATCHED_BIE if matched else dict(nterms=7, acc=0.5, maxmemb=500)
+            reqs.append(dict(kind="solve", n=len(cen), data=(cx, cy, cz, area, f),
+                             nterms=sp["nterms"], n0=sp["maxmemb"], acc=sp["acc"], del_=h * h,
+                             level=level))
     return reqs
 
 
@@ -446,10 +575,10 @@ def serve(reqs, arrivals, prec, srv, slots):
             if dt > 0:
                 time.sleep(dt)
             if r["kind"] == "eval":
-                p = B.params(r["kernel"], B.CONSISTENT, prec, del_=r["del_"], kappa=r["kappa"], acc=0.6)
+                p = B.params(r["kernel"], B.CONSISTENT, prec, del_=r["del_"], kappa=r["kappa"], acc=r["acc"])
                 ids[i] = srv.submit_eval(*r["data"], r["nterms"], r["n0"], p)
             else:
-                p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=r["del_"], kappa=1.0, acc=0.5)
+                p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=r["del_"], kappa=1.0, acc=r["acc"])
                 x, y, z, w, f = r["data"]
                 ids[i] = srv.submit_solve(x, y, z, w, f, r["nterms"], r["n0"], p, 0.5, restart=50,
                                           tol=1e-8, precision=prec)
@@ -473,14 +602,14 @@ def serve(reqs, arrivals, prec, srv, slots):
                  "failed": int(sum(1 for i in infos if i["status"] not in (0,)))}
 
 
-def run_serving(ctx, args):
+def run_serving(ctx, args, matched=False):
     """Serving stream: open-loop Poisson arrivals of the request mix at 80% of the warm mixed
     server's measured capacity, admitted by a 150 GB HBM budget into a continuous-batching
     server (mixed precision, several slots), next to the plain FP64 GPU path serving one
-    request at a time on the same arrivals."""
+    request at a time on the same arrivals.  matched: the accuracy-matched parameters."""
     import bit_b200 as B
     from bit_b200 import workloads
-    reqs = serving_requests(args.serve_requests, seed=5, ctx=ctx)
+    reqs = serving_requests(args.serve_requests, seed=5, ctx=ctx, matched=matched)
     budget = 150 * 10 ** 9
     # Each server is long-lived, as in deployment: it first serves the whole request set
     # once (every buffer grown, every plan made), then the timed streams.  Arrival rate:
@@ -506,28 +635,41 @@ def run_serving(ctx, args):
         srv.close()
     # accuracy: mixed vs plain FP64 per request; evaluate requests also vs the direct sum
     diff = [workloads.rel_l2(a, b) for a, b in zip(res32, res64)]
-    derr = []
+    derr, serr = [], []
     for i, r in enumerate(reqs):
-        if r["kind"] != "eval":
-            continue
-        x, y, z, q = r["data"]
         tg = workloads.sample_targets(r["n"], 200, seed=i)
-        p = B.params(r["kernel"], B.CONSISTENT, B.FP64, del_=r["del_"], kappa=r["kappa"])
-        derr.append(workloads.rel_l2(res32[i][tg], ctx.direct(x, y, z, q, p, tg)))
+        if r["kind"] == "eval":
+            x, y, z, q = r["data"]
+            p = B.params(r["kernel"], B.CONSISTENT, B.FP64, del_=r["del_"], kappa=r["kappa"])
+            for res in (res32, res64):
+                derr.append(workloads.rel_l2(res[i][tg], ctx.direct(x, y, z, q, p, tg)))
+        else:
+            x, y, z, w, f = r["data"]
+            p = B.params(B.SCREENED_REG, B.CONSISTENT, B.FP64, del_=r["del_"], kappa=1.0)
+            for res in (res32, res64):
+                Ks = ctx.direct(x, y, z, w * res[i], p, tg)
+                serr.append(workloads.rel_l2(0.5 * res[i][tg] + Ks, f[tg]))
     kinds = [r["kind"] for r in reqs]
+    th = "theta by p " + str({k - 1: v for k, v in sorted(MATCHED_BATCH_ACC.items())}) if matched else "theta 0.6"
+    sp = MATCHED_BIE if matched else dict(nterms=7, acc=0.5, maxmemb=500)
     return {"workload": f"{len(reqs)} requests, Poisson arrivals at {rate:.1f}/s "
                         f"({load:.0%} of the warm mixed server's closed-loop capacity, "
                         f"{cap['requests_per_s']:.1f}/s) "
                         f"({kinds.count('eval')} evaluate: N lognormal median 2e4 in [1e3, 1e6], "
-                        f"blobs, p in {{4,6,8}}, theta 0.6; {kinds.count('solve')} solves: "
-                        "icosphere level 4..7, p=6, theta=0.5, GMRES(50) to 1e-8), 150 GB budget",
+                        f"blobs, p in {{4,6,8}}, {th}; {kinds.count('solve')} solves: "
+                        f"icosphere level 4..7, p={sp['nterms'] - 1}, theta={sp['acc']}, "
+                        f"N0={sp['maxmemb']}, GMRES(50) to 1e-8), 150 GB budget",
             "offered_load": load, "mixed_closed_loop_requests_per_s": cap["requests_per_s"],
             "mixed_continuous_batching": mixed, "fp64_one_at_a_time": plain,
             "throughput_ratio": mixed["requests_per_s"] / plain["requests_per_s"],
             "p99_ratio": plain["p99_latency_s"] / mixed["p99_latency_s"],
             "mixed_vs_fp64_max": float(max(diff)),
             "eval_error_vs_direct_200_targets": {"median": float(np.median(derr)),
-                                                 "max": float(np.max(derr))}}
+                                                 "max": float(np.max(derr))},
+            "solve_residual_vs_direct_200_rows": {"median": float(np.median(serr)) if serr else None,
+                                                  "max": float(np.max(serr)) if serr else None},
+            "max_error_vs_direct": float(max(derr + serr)),
+            "at_most_1e-6": bool(max(derr + serr) <= 1e-6)}
 
 
 def far_flops_per_pair(nterms):
@@ -539,28 +681,6 @@ def far_flops_per_pair(nterms):
     g = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(g)
     return g.flops_per_pair(nterms)
-
-
-def profiled_traffic(key="k_near_screened_f32"):
-    """DRAM bytes per launch of the dominant kernel, from the committed one-pass ncu launch
-    list of this workload (profiles/launches_clustered2M_step.md); None if absent."""
-    path = os.path.join(ROOT, "profiles", "launches_clustered2M_step.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch") and key in line:
-                return int(line.split("=")[1].strip())
-    except OSError:
-        pass
-    return None
-
-
-def fp32_peak_from_clock(clocks):
-    """Nominal B200 CUDA-core FP32 peak at the sampled SM clock: 148 SMs x 128 FFMA/clk x 2
-    flops; MUFU (rsqrt / ex2) peak 148 x 16 ops/clk."""
-    mhz = clocks.get("sm_mhz") or 1965.0
-    return {"tflops": 148 * 128 * 2 * mhz * 1e6 / 1e12, "mufu_ops": 148 * 16 * mhz * 1e6,
-            "source": f"nominal 148x128 FFMA/clk at the sampled median SM clock ({mhz:.0f} MHz); "
-                      "MEASURED_PEAKS.json has no CUDA-core FP32 figure"}
 
 
 def accuracy(ctx, x, y, z, q, s32, c32, s64, c64, args):
@@ -637,22 +757,33 @@ def run_reference(args):
         return
     threads = os.cpu_count() or 1
     x, y, z, q = workload(args.n, seed=1)
-    times = []
+    est, measured = [], []
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         r = cpu_reference_time(x, y, z, q, args.n, args.ref_sample, threads)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference build (oracle/_ref) not present"}))
             return
         if i >= args.warmup:
-            times.append(r["est_step_s"])
-    ms = 1e3 * statistics.mean(times)
-    v = 2 * args.n / (ms * 1e-3)
+            est.append(r["est_step_s"])
+            measured.append(time.perf_counter() - t0)
+    est_ms = 1e3 * statistics.mean(est)
+    ms = 1e3 * statistics.mean(measured)
+    v = 2 * args.n / (est_ms * 1e-3)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded clustered blobs)",
-            "config": {"workload": "clustered evaluation N=2,000,000, p=8, theta=0.7, N0=1000, "
-                                   "screened kappa=1 + Coulomb delta=0.005", "n": args.n},
+            "config": {"workload": "clustered evaluation N=2,000,000 (80% in 8 Gaussian blobs sigma "
+                                   "0.1, 20% uniform), p=8, theta=0.7, N0=1000, screened kappa=1 + "
+                                   "Coulomb delta=0.005, all particles as targets",
+                       "n": args.n, "nterms": NTERMS, "maxmemb": MAXMEMB, "acc": ACC},
+            "value_basis": f"extrapolated: each step times the full treemake + treemoments and the "
+                           f"evaluation of {args.ref_sample} seeded targets (both kernels), and the "
+                           f"evaluation time is scaled to all {args.n} targets; ms_per_step is the "
+                           "measured time of one such sampled step, extrapolated_ms_per_full_step "
+                           "the estimate for all targets",
+            "extrapolated_ms_per_full_step": est_ms,
             "cpu_baseline": {"value": v, "unit": "evals/s", "cores": threads, "kind": "reference",
                              "sample": f"per step: full tree build + moments, evaluation of "
                                        f"{args.ref_sample} seeded targets scaled to all N"},
@@ -682,6 +813,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=120,
                     help="requests of the serving stream (0: skip)")
     ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--no-matched", dest="matched", action="store_false",
+                    help="skip the accuracy-matched (1e-6 vs direct sum) runs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -65,6 +65,16 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class FieldParams(C.Structure):
+    _fields_ = [("kind", C.c_int), ("precision", C.c_int), ("del_", C.c_double),
+                ("mac_del", C.c_double), ("kappa", C.c_double), ("acc", C.c_double),
+                ("kernel_order", C.c_int)]
+
+
+FIELD_COULOMB, FIELD_SCREENED = 0, 1
+KERNEL_ORDER_MAX = 8
+
+
 class GmresOpts(C.Structure):
     _fields_ = [("restart", C.c_int), ("maxit", C.c_int), ("tol", C.c_double),
                 ("precision", C.c_int), ("inner_tol", C.c_double),
@@ -149,9 +159,13 @@ SIGNATURES = [
     ("bit_eval_particles_device", C.c_int, [_vp, C.POINTER(EvalParams), _vp]),
     ("bit_eval_points", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _dp, _dp, _dp, _dp]),
     ("bit_eval_force", C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp]),
+    ("bit_eval_field", C.c_int, [_vp, C.POINTER(FieldParams), _dp, _dp, _dp]),
+    ("bit_direct_field", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, C.c_int, C.c_double,
+                                   C.c_int, C.c_int, _ip, _dp, _dp, _dp]),
     ("bit_treecode_potential", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int,
                                          C.c_int, C.POINTER(EvalParams), _dp]),
     ("bit_tree_stats", C.c_int, [_vp, C.POINTER(Stats)]),
+    ("bit_device_fma_peak", C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
     ("bit_tree_target_lists", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _ip, _ip, C.c_int,
                                         _ip]),
     ("bit_bie_solve", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, C.c_double, _dp, _dp, _dp,
@@ -288,6 +302,12 @@ class Context:
         lib().bit_ctx_stream(self.h, C.byref(s))
         return s.value
 
+    def fma_peak(self, precision):
+        """Measured FMA throughput of the device in flop/s (FP64 or MIXED = FP32)."""
+        v = C.c_double()
+        self.check(lib().bit_device_fma_peak(self.h, precision, C.byref(v)), "bit_device_fma_peak")
+        return v.value
+
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()
         lib().bit_ctx_memory(self.h, C.byref(a), C.byref(b))
@@ -332,6 +352,18 @@ class Context:
                                               C.byref(prm), len(tg), tg.ctypes.data_as(_ip),
                                               _d(out)), "bit_direct_potential")
         return out
+
+    def direct_field(self, x, y, z, q, targets, del_=0.0, regularised=True, kernel_order=0):
+        """FP64 field direct sum at particle targets (bit_direct_field):
+        force_particle_ds_reg / force_particle_ds_noreg.  Returns (fx, fy, fz)."""
+        x, y, z, q = map(_f64, (x, y, z, q))
+        tg = np.ascontiguousarray(targets, dtype=np.int32)
+        fx, fy, fz = np.zeros(len(tg)), np.zeros(len(tg)), np.zeros(len(tg))
+        self.check(lib().bit_direct_field(self.h, len(x), _d(x), _d(y), _d(z), _d(q),
+                                          int(bool(regularised)), del_, kernel_order, len(tg),
+                                          tg.ctypes.data_as(_ip), _d(fx), _d(fy), _d(fz)),
+                   "bit_direct_field")
+        return fx, fy, fz
 
     def direct_device(self, n, xp, yp, zp, qp, prm, m, tgp, outp):
         self.check(lib().bit_direct_potential_device(self.h, n, xp, yp, zp, qp, C.byref(prm), m,
@@ -482,6 +514,16 @@ class Tree:
         fx, fy, fz = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
         self.ctx.check(lib().bit_eval_force(self.h, del_, acc, precision, _d(fx), _d(fy), _d(fz)),
                        "bit_eval_force")
+        return fx, fy, fz
+
+    def field(self, kind=FIELD_COULOMB, acc=0.5, del_=0.0, kappa=0.0, mac_del=0.0,
+              kernel_order=0, precision=FP64):
+        """bit_eval_field: treeforce with KERNEL_ORDER (FIELD_COULOMB) or shielded_treeforce's
+        screened 2-D field (FIELD_SCREENED) at every particle; returns (fx, fy, fz)."""
+        fx, fy, fz = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        prm = FieldParams(kind, precision, del_, mac_del, kappa, acc, kernel_order)
+        self.ctx.check(lib().bit_eval_field(self.h, C.byref(prm), _d(fx), _d(fy), _d(fz)),
+                       "bit_eval_field")
         return fx, fy, fz
 
     def stats(self):

@@ -639,19 +639,41 @@ bit_status bit_eval_points(bit_tree* th, const bit_eval_params* prm, int m, cons
 
 bit_status bit_eval_force(bit_tree* th, double del, double acc, bit_precision prec, double* fx,
                           double* fy, double* fz) {
-  if (!th || !fx || !fy || !fz) return BIT_ERR_INVALID_ARGUMENT;
+  bit_field_params f{};
+  f.kind = BIT_FIELD_COULOMB;
+  f.precision = prec;
+  f.del = del;
+  f.acc = acc;
+  return bit_eval_field(th, &f, fx, fy, fz);
+}
+
+bit_status bit_eval_field(bit_tree* th, const bit_field_params* fp, double* fx, double* fy,
+                          double* fz) {
+  if (!th || !fp || !fx || !fy || !fz) return BIT_ERR_INVALID_ARGUMENT;
   Tree* t = &th->t;
   Ctx* c = t->ctx;
   return guard(c, [&] {
     if (!t->has_moments) fail(BIT_ERR_STATE, "moments not computed");
     if (t->nterms > kNtermsMax) fail(BIT_ERR_INVALID_ARGUMENT, "nterms too large for the force");
+    if (fp->kind != BIT_FIELD_COULOMB && fp->kind != BIT_FIELD_SCREENED)
+      fail(BIT_ERR_INVALID_ARGUMENT, "unknown field kind");
+    if (fp->precision != BIT_PREC_FP64 && fp->precision != BIT_PREC_MIXED)
+      fail(BIT_ERR_INVALID_ARGUMENT, "unknown precision");
+    if (fp->kernel_order < 0 || fp->kernel_order > BIT_KERNEL_ORDER_MAX)
+      fail(BIT_ERR_INVALID_ARGUMENT, "kernel_order out of range");
+    if (fp->precision == BIT_PREC_MIXED && (fp->kind == BIT_FIELD_SCREENED || fp->kernel_order > 0))
+      fail(BIT_ERR_INVALID_ARGUMENT, "this field is evaluated in FP64 only");
+    if (!(fp->acc >= 0.0) || !std::isfinite(fp->del) || !std::isfinite(fp->kappa))
+      fail(BIT_ERR_INVALID_ARGUMENT, "acc, del and kappa must be finite, acc >= 0");
     BIT_CUDA(cudaSetDevice(c->device));
     bit_eval_params p{};
-    p.kernel = BIT_KERNEL_COULOMB;
-    p.del = del;
-    p.acc = acc;
-    p.precision = prec;
-    prepare_particles(t, {p}, 1);
+    p.kernel = fp->kind == BIT_FIELD_SCREENED ? BIT_KERNEL_SCREENED : BIT_KERNEL_COULOMB;
+    p.del = fp->del;
+    p.mac_del = fp->mac_del;
+    p.kappa = fp->kappa;
+    p.acc = fp->acc;
+    p.precision = fp->precision;
+    prepare_particles(t, {p}, fp->kind == BIT_FIELD_SCREENED ? 2 : 1, fp->kernel_order);
     const int n = t->n;
     t->fx_sorted.ensure(c, n); t->fy_sorted.ensure(c, n); t->fz_sorted.ensure(c, n);
     ev_rec(t, EV_FAR);
@@ -809,6 +831,50 @@ bit_status bit_direct_potential_device(bit_ctx* h, int n, const double* x, const
     check_params(prm);
     BIT_CUDA(cudaSetDevice(c->device));
     direct_potential(c, n, x, y, z, q, *prm, m, targets, pot);
+  });
+}
+
+bit_status bit_direct_field(bit_ctx* h, int n, const double* x, const double* y,
+                            const double* z, const double* q, int regularised, double del,
+                            int kernel_order, int m, const int* targets, double* fx, double* fy,
+                            double* fz) {
+  if (!h || !x || !y || !z || !q || !targets || !fx || !fy || !fz || n < 1 || m < 0)
+    return BIT_ERR_INVALID_ARGUMENT;
+  if (m == 0) return BIT_OK;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    if (kernel_order < 0 || kernel_order > BIT_KERNEL_ORDER_MAX)
+      fail(BIT_ERR_INVALID_ARGUMENT, "kernel_order out of range");
+    if (!std::isfinite(del)) fail(BIT_ERR_INVALID_ARGUMENT, "del must be finite");
+    for (int i = 0; i < m; i++)
+      if (targets[i] < 0 || targets[i] >= n) fail(BIT_ERR_INVALID_ARGUMENT, "target index out of range");
+    BIT_CUDA(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    DBuf<double> dx, dy, dz, dq, out;
+    DBuf<int> dt;
+    dx.ensure(c, n); dy.ensure(c, n); dz.ensure(c, n); dq.ensure(c, n);
+    dt.ensure(c, m); out.ensure(c, 3LL * m);
+    copy_h2d(c, dx.p, x, n * sizeof(double));
+    copy_h2d(c, dy.p, y, n * sizeof(double));
+    copy_h2d(c, dz.p, z, n * sizeof(double));
+    copy_h2d(c, dq.p, q, n * sizeof(double));
+    copy_h2d(c, dt.p, targets, m * sizeof(int));
+    direct_field(c, n, dx.p, dy.p, dz.p, dq.p, regularised, del, kernel_order, m, dt.p, out.p);
+    copy_d2h(c, fx, out.p, m * sizeof(double));
+    copy_d2h(c, fy, out.p + m, m * sizeof(double));
+    copy_d2h(c, fz, out.p + 2LL * m, m * sizeof(double));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    check_dev_err(c);
+  });
+}
+
+bit_status bit_device_fma_peak(bit_ctx* h, bit_precision prec, double* flops_per_s) {
+  if (!h || !flops_per_s || (prec != BIT_PREC_FP64 && prec != BIT_PREC_MIXED))
+    return BIT_ERR_INVALID_ARGUMENT;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    *flops_per_s = fma_peak(c, prec == BIT_PREC_MIXED);
   });
 }
 

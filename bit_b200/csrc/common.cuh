@@ -102,6 +102,8 @@ struct SysEval {
   double intg;                   // reference-mode screened self term
   int kernel, nterms;
   int near_sign, eps_check, self_term, particles;
+  int kernel_order;  // regularised Coulomb field: the reference's KERNEL_ORDER (src/problem.h:13)
+  int pad_;
 };
 
 // One launch of a far / near kernel: the groups of one (nterms, kernel) class.
@@ -288,19 +290,29 @@ void direct_potential(Ctx* c, int n, const double* x, const double* y, const dou
                       const double* q, const bit_eval_params& p, int m, const int* tg,
                       double* out);
 void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz);
+// Measured FMA throughput of the context's device, flop/s (2 per FMA), FP32 or FP64.
+double fma_peak(Ctx* c, bool f32);
+// FP64 field direct sum at m particle targets tg (device pointers); out = fx | fy | fz.
+void direct_field(Ctx* c, int n, const double* x, const double* y, const double* z,
+                  const double* q, int regularised, double del, int korder, int m,
+                  const int* tg, double* out);
 
-// Per-system parameters of a potential (force = 0) or field (force = 1) evaluation.
-SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int force);
+// Per-system parameters of a potential (force = 0) or field evaluation: force = 1 the
+// regularised Coulomb field of treeforce (kernel_order: the reference's KERNEL_ORDER),
+// force = 2 the screened 2-D field of shielded_treeforce.
+SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int force,
+                      int kernel_order = 0);
 // Fill P->h_sys (one entry per system; prm holds one entry for all or one per system) and
 // its device copy.
 void plan_sys(Tree* t, EvalPlan* P, const std::vector<bit_eval_params>& prm, int points,
-              int force);
+              int force, int kernel_order = 0);
 // Key of the lists the plan's MAC needs.
 ListKey plan_key(const Tree* t, const EvalPlan& P, int points);
 // Launch classes and class-ordered groups of P over the lists L.
 void plan_classes(Tree* t, Lists* L, EvalPlan* P);
 // Particle-target lists and plan of a tree (t->plists, t->pplan) for these parameters.
-void prepare_particles(Tree* t, const std::vector<bit_eval_params>& prm, int force);
+void prepare_particles(Tree* t, const std::vector<bit_eval_params>& prm, int force,
+                       int kernel_order = 0);
 
 inline unsigned grid_for(long long work, int per_block) {
   long long g = (work + per_block - 1) / per_block;

@@ -66,6 +66,66 @@ __global__ void __launch_bounds__(DT) k_direct(int n, const double* x, const dou
   if (ti < m) part[(long long)blockIdx.y * m + ti] = acc;
 }
 
+// Field direct sums, force_particle_ds_reg (src/tree3d.cpp:298-330, with the KERNEL_ORDER
+// family of eval_grad_kernel_reg, :73-97) and force_particle_ds_noreg (:182-213):
+// sum over j != target of q_j G(x_j - x), G(d) = -d t, t = 1/(r rs) (+ korder terms) with
+// rs = |d|^2 + del (REG) or t = 1/(rs sqrt(rs)) with rs = |d|^2.  Three partial sums per
+// (chunk, target): part[(c * 3 + axis) * m + ti].
+template <bool REG>
+__global__ void __launch_bounds__(DT) k_direct_field(int n, const double* x, const double* y,
+                                                     const double* z, const double* q, int m,
+                                                     const int* tg, double del, int korder,
+                                                     double* part, int* err) {
+  __shared__ double4 S[DS];
+  const int ti = blockIdx.x * DT + threadIdx.x;
+  const int j0 = blockIdx.y * DCH, j1 = min(n, j0 + DCH);
+  int p = ti < m ? tg[ti] : -1;
+  if (p >= n || p < -1) {
+    if (blockIdx.y == 0) atomicOr(err, 4);
+    p = -1;
+  }
+  double X = 0, Y = 0, Z = 0;
+  if (p >= 0) { X = x[p]; Y = y[p]; Z = z[p]; }
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  for (int s0 = j0; s0 < j1; s0 += DS) {
+    const int cnt = min(DS, j1 - s0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < cnt; k += DT)
+      S[k] = make_double4(x[s0 + k], y[s0 + k], z[s0 + k], q[s0 + k]);
+    __syncthreads();
+    if (p < 0) continue;
+    const int self = p - s0;
+    for (int k = 0; k < cnt; k++) {
+      if (k == self) continue;
+      const double4 s = S[k];
+      const double dx = s.x - X, dy = s.y - Y, dz = s.z - Z;
+      double t;
+      if (REG) {
+        const double rs = dx * dx + dy * dy + dz * dz + del;
+        const double r = sqrt(rs);
+        t = 1.0 / (r * rs);
+        double f = t;
+        for (int l = 1; l <= korder; l++) {
+          f = f * (l + 0.5) / l * del / rs;
+          t += f;
+        }
+      } else {
+        const double rs = dx * dx + dy * dy + dz * dz;
+        t = 1 / (rs * sqrt(rs));
+      }
+      ax += s.w * (-dx * t);
+      ay += s.w * (-dy * t);
+      az += s.w * (-dz * t);
+    }
+  }
+  if (ti < m) {
+    const long long b = (long long)blockIdx.y * 3 * m + ti;
+    part[b] = ax;
+    part[b + m] = ay;
+    part[b + 2LL * m] = az;
+  }
+}
+
 // out[i] = sign * sum over chunks of part[c][i], in chunk order
 __global__ void k_direct_sum(int m, int nch, const double* part, double sign, double* out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -75,7 +135,35 @@ __global__ void k_direct_sum(int m, int nch, const double* part, double sign, do
   out[i] = sign * s;
 }
 
+// out[axis * m + i] = sum over chunks of part[(c * 3 + axis) * m + i], in chunk order
+__global__ void k_direct_field_sum(int m, int nch, const double* part, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3 * m) return;
+  const int axis = i / m, ti = i - axis * m;
+  double s = 0.0;
+  for (int c = 0; c < nch; c++) s += part[((long long)c * 3 + axis) * m + ti];
+  out[i] = s;
+}
+
 }  // namespace
+
+// All pointers on the device; out holds fx, fy, fz of the m targets (3 m doubles).
+void direct_field(Ctx* c, int n, const double* x, const double* y, const double* z,
+                  const double* q, int regularised, double del, int korder, int m,
+                  const int* tg, double* out) {
+  cudaStream_t s = c->stream;
+  const int nch = (n + DCH - 1) / DCH;
+  DBuf<double> part;
+  part.ensure(c, (size_t)nch * 3 * m);
+  const dim3 grid((m + DT - 1) / DT, nch);
+  int* err = c->dev_err();
+  if (regularised)
+    count_launch(), k_direct_field<true><<<grid, DT, 0, s>>>(n, x, y, z, q, m, tg, del, korder, part.p, err);
+  else
+    count_launch(), k_direct_field<false><<<grid, DT, 0, s>>>(n, x, y, z, q, m, tg, del, korder, part.p, err);
+  count_launch(), k_direct_field_sum<<<grid_for(3LL * m, 256), 256, 0, s>>>(m, nch, part.p, out);
+  BIT_CHECK_LAUNCH();
+}
 
 // All pointers on the device.  The screened sum is negated (src/tree3d.cpp:2014).
 void direct_potential(Ctx* c, int n, const double* x, const double* y, const double* z,

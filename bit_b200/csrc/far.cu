@@ -21,6 +21,8 @@ __device__ __forceinline__ double exp_t(double x) { return exp(x); }
 __device__ __forceinline__ float exp_t(float x) { return expf(x); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double pow_t(double a, double b) { return pow(a, b); }
+__device__ __forceinline__ float pow_t(float a, float b) { return powf(a, b); }
 template <class T>
 struct V4 {
   T x, y, z, w;
@@ -174,7 +176,12 @@ __global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArg
   }
 }
 
-template <int NT, class T>
+// Field kinds of k_far_force: the regularised Coulomb field of treetaylorforce with
+// KERNEL_ORDER = 0 (FK_COULOMB) or with the system's kernel order (FK_COULOMB_KORDER, FP64),
+// and the screened 2-D field of shielded_treetaylorforce (FK_SCREENED_CURL, FP64).
+constexpr int FK_COULOMB = 0, FK_COULOMB_KORDER = 1, FK_SCREENED_CURL = 2;
+
+template <int NT, int FK, class T>
 __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
   constexpr int TT = num_terms(NT);
   constexpr int TP = FarField<NT>::kPadded;
@@ -200,7 +207,9 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
   unsigned short* tl = tlb + w * kGroupMax;
   double* row = accb + w * 3 * kGroupMax;
   const T* mom = reinterpret_cast<const T*>(a.mom);
-  const T tadd = (T)a.sys[a.g_sys[g]].far_add;
+  const SysEval* se = a.sys + a.g_sys[g];
+  const T tadd = (T)se->far_add, tk = (T)se->kappa, tdel = (T)se->near_del;
+  const int korder = se->kernel_order;
   for (long long e = e0 + w; e < e1; e += NW) {
     const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
     const int cnt = warp_pack(wd, tl);
@@ -226,7 +235,10 @@ __global__ void __launch_bounds__(32 * NWF) k_far_force(FarArgs a) {
       const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
       const T rs = dx * dx + dy * dy + dz * dz + tadd;
       T fx = 0, fy = 0, fz = 0;
-      FarField<NT>::template force<T>(dx, dy, dz, rs, M, fx, fy, fz);
+      if constexpr (FK == FK_COULOMB) FarField<NT>::template force<T>(dx, dy, dz, rs, M, fx, fy, fz);
+      else if constexpr (FK == FK_COULOMB_KORDER)
+        FarField<NT>::template force_korder<T>(dx, dy, dz, rs, tdel, korder, M, fx, fy, fz);
+      else FarField<NT>::template screened_curl<T>(dx, dy, dz, rs, tk, M, fx, fy);
       row[i] += (double)fx;
       row[kGroupMax + i] += (double)fy;
       row[2 * kGroupMax + i] += (double)fz;
@@ -259,11 +271,11 @@ void launch_far(const FarArgs& a, int ng, cudaStream_t s) {
   count_launch(), k_far<NT, KER, T><<<ng, 32 * NWP, bytes, s>>>(a);
 }
 
-template <int NT, class T>
+template <int NT, int FK, class T>
 void launch_force(const FarArgs& a, int ng, cudaStream_t s) {
   const size_t bytes = far_smem<NWF>(3 * sizeof(double), FarField<NT>::kPadded * sizeof(T));
-  set_smem(k_far_force<NT, T>, bytes);
-  count_launch(), k_far_force<NT, T><<<ng, 32 * NWF, bytes, s>>>(a);
+  set_smem(k_far_force<NT, FK, T>, bytes);
+  count_launch(), k_far_force<NT, FK, T><<<ng, 32 * NWF, bytes, s>>>(a);
 }
 
 FarArgs far_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
@@ -323,14 +335,21 @@ void eval_far_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy
   a.out = fx; a.out_y = fy; a.out_z = fz;
   cudaStream_t s = t->ctx->stream;
   const bool f32 = P.f32;
+  // field kind of the plan: 1 Coulomb (kernel order from each system), 2 screened curl
+  const bool curl = P.force == 2;
+  bool korder = false;
+  for (const SysEval& se : P.h_sys) korder |= se.kernel_order > 0;
+  if (f32 && (curl || korder)) fail(BIT_ERR_INVALID_ARGUMENT, "this field is FP64 only");
   for (const LaunchClass& k : P.far_classes) {
     a.order = P.far_ord + k.begin;
     const int ng = k.count;
     switch (k.nterms) {
-#define CASE(N)                                           \
-  case N:                                                 \
-    if (f32) launch_force<N, float>(a, ng, s);            \
-    else launch_force<N, double>(a, ng, s);               \
+#define CASE(N)                                                            \
+  case N:                                                                  \
+    if (f32) launch_force<N, FK_COULOMB, float>(a, ng, s);                 \
+    else if (curl) launch_force<N, FK_SCREENED_CURL, double>(a, ng, s);    \
+    else if (korder) launch_force<N, FK_COULOMB_KORDER, double>(a, ng, s); \
+    else launch_force<N, FK_COULOMB, double>(a, ng, s);                    \
     break;
       CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
 #undef CASE

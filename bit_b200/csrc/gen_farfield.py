@@ -424,6 +424,94 @@ def gen_force(nt):
     return L
 
 
+def gen_screened_curl(nt):
+    """Field sum of shielded_treetaylorforce (src/tree3d.cpp:2745-2973): the screened
+    coefficients a_v of shielded_treetaylorpot's recurrence (the same index patterns and
+    formulas, :2796-2938) to degree nterms, then fx -= (j+1) M_ijk a_(i,j+1,k) and
+    fy += (i+1) M_ijk a_(i+1,j,k) (:2946-2958); the reference sets fz = 0."""
+    mi = shell_index(nt)
+    L = ["  const T dx2 = T(2)*dx, dy2 = T(2)*dy, dz2 = T(2)*dz;",
+         "  const T kdx = kappa*dx, kdy = kappa*dy, kdz = kappa*dz;",
+         "  const T rinv = rsqrt_t(dist2);",
+         "  const T fac = rinv * rinv;",
+         "  const T c0_0_0 = exp_t(-kappa * (dist2 * rinv));",
+         "  const T a0_0_0 = c0_0_0 * rinv;",
+         "  T sx = T(0), sy = T(0);"]
+    for v in shells(nt):
+        if v != (0, 0, 0):
+            bexp, aexp = scr_expr(v)
+            L.append(f"  const T {name('c', v)} = {bexp};")
+            L.append(f"  const T {name('a', v)} = {aexp};")
+        if v[1] >= 1:
+            m = sub(v, 1, 1)
+            if sum(m) < nt:
+                L.append(f"  sx = fma_t(M[{mi[m]}] * {lit(-(m[1] + 1))}, {name('a', v)}, sx);")
+        if v[0] >= 1:
+            m = sub(v, 0, 1)
+            if sum(m) < nt:
+                L.append(f"  sy = fma_t(M[{mi[m]}] * {lit(m[0] + 1)}, {name('a', v)}, sy);")
+    L.append("  fx += sx; fy += sy;")
+    return L
+
+
+def korder_expr(v):
+    """Correction of order l to the Taylor coefficient v of the regularised Coulomb field
+    (treetaylorforce's KERNEL_ORDER loop, src/tree3d.cpp:614-791).  Every index pattern of
+    that loop is the one recurrence for the coefficients of (r^2 + del)^-(l + 1/2):
+    d_v = fac/s ((1 - 2l - 2s) sum_a x_a d_(v-e_a) + (1 - 2l - s) sum_a d_(v-2e_a)),
+    s = |v| (e.g. :637-639 for s = 1, :667-669 for v = (1, 1, 0), :725-728 for v = (1, 1, 1))."""
+    d = lambda w: name("d", w)
+    s = sum(v)
+    s1 = " + ".join(f"d{AX[a]}*{d(sub(v, a, 1))}" for a in range(3) if v[a] >= 1)
+    s2 = [d(sub(v, a, 2)) for a in range(3) if v[a] >= 2]
+    e = f"(T({float(1 - 2 * s)!r}) - T(2)*lf)*({s1})"
+    if s2:
+        e += f" + (T({float(1 - s)!r}) - T(2)*lf)*({' + '.join(s2)})"
+    return f"(fac*{lit(1.0 / s)})*({e})"
+
+
+def gen_force_korder(nt):
+    """treetaylorforce with its KERNEL_ORDER loop (src/tree3d.cpp:456-810): the order-0
+    coefficients of gen_force, then for l = 1..korder the correction recurrence seeded with
+    choose(-1/2, l) (-del)^l / (r (r^2+del)^l) (:617-631), added into every coefficient;
+    the field sum of :794-808 over the corrected coefficients."""
+    mi = shell_index(nt)
+    L = ["  const T fac = T(1) / rs;",
+         "  const T sqfac = sqrt_t(fac);",
+         "  const T r = sqrt_t(rs);"]
+    for v in shells(nt):
+        L.append(f"  T {name('b', v)} = {force_expr(v)};")
+    L.append("  for (int l = 1; l <= korder; l++) {")
+    L.append("    const T lf = T(l);")
+    L.append("    T binom = T(1), fact = T(1);")
+    L.append("    for (int j = 1; j <= l; j++) {")
+    L.append("      binom = binom * (T(-0.5) - T(j) + T(1)) * (-del);")
+    L.append("      fact = fact * T(j);")
+    L.append("    }")
+    L.append("    const T d0_0_0 = (binom / fact) * T(1) / (r * pow_t(rs, lf));")
+    L.append("    b0_0_0 += d0_0_0;")
+    for v in shells(nt):
+        if v == (0, 0, 0):
+            continue
+        L.append(f"    const T {name('d', v)} = {korder_expr(v)};")
+        L.append(f"    {name('b', v)} += {name('d', v)};")
+    L.append("  }")
+    L.append("  T sx = T(0), sy = T(0), sz = T(0);")
+    for v in shells(nt):
+        if sum(v) == 0:
+            continue
+        for a, acc in ((0, "sx"), (1, "sy"), (2, "sz")):
+            if v[a] == 0:
+                continue
+            m = sub(v, a, 1)
+            if sum(m) >= nt:
+                continue
+            sign = 1.0 if (sum(m) + 1) % 2 == 0 else -1.0
+            L.append(f"  {acc} = fma_t(M[{mi[m]}] * {lit(sign * (m[a] + 1))}, {name('b', v)}, {acc});")
+    L.append("  fx += sx; fy += sy; fz += sz;")
+    return L
+
+
 def count_flops(lines):
     """Floating-point operations of generated lines: every binary + - * /, 2 per fma_t,
     1 per sqrt_t / rsqrt_t / exp_t (literals and the moment loads are not arithmetic)."""
@@ -483,6 +571,15 @@ def main(out):
         parts.append("  template <class T> static __device__ __forceinline__ void force("
                      "T dx, T dy, T dz, T rs, const T* __restrict__ M, T& fx, T& fy, T& fz) {")
         parts += gen_force(nt)
+        parts.append("  }")
+        parts.append("  template <class T> static __device__ __forceinline__ void force_korder("
+                     "T dx, T dy, T dz, T rs, T del, int korder, const T* __restrict__ M, "
+                     "T& fx, T& fy, T& fz) {")
+        parts += gen_force_korder(nt)
+        parts.append("  }")
+        parts.append("  template <class T> static __device__ __forceinline__ void screened_curl("
+                     "T dx, T dy, T dz, T dist2, T kappa, const T* __restrict__ M, T& fx, T& fy) {")
+        parts += gen_screened_curl(nt)
         parts.append("  }")
         parts.append("};")
     parts.append("}  // namespace bit")

@@ -484,10 +484,27 @@ extern "C" bit_status bit_bie_solve(bit_tree* th, const bit_eval_params* prm, in
   return st != BIT_OK ? st : result;
 }
 
+namespace bit {
+namespace {
+bool rhs_is_zero(int n, const double* b) {
+  for (int i = 0; i < n; i++)
+    if (b[i] != 0.0) return false;
+  return true;
+}
+}  // namespace
+}  // namespace bit
+
 extern "C" bit_status bit_gmres_dense(bit_ctx* h, int n, const double* a, const double* b,
                                       double* x, int* iterations) {
   if (!h || !a || !b || !x || n < 1) return BIT_ERR_INVALID_ARGUMENT;
   Ctx* c = &h->c;
+  // b = 0: x = 0 solves A x = b exactly (the reference would divide by |b| = 0 and fill
+  // its Krylov basis with NaN)
+  if (rhs_is_zero(n, b)) {
+    for (int i = 0; i < n; i++) x[i] = 0.0;
+    if (iterations) *iterations = 0;
+    return BIT_OK;
+  }
   bit_status result = BIT_OK;
   bit_status st = guard2(c, [&] {
     BIT_CUDA(cudaSetDevice(c->device));
@@ -569,10 +586,14 @@ extern "C" bit_status bit_gmres_dense(bit_ctx* h, int n, const double* a, const 
 
 // ---- bit_gmres_dense_static: the dense GMRES above with no allocation at call time ------
 // Device scratch is one file-scope array sized for n <= BIT_GMRES_STATIC_MAX; host scratch
-// (Hessenberg and the least-squares work arrays) is file-scope too.  Its address on each
-// device is looked up once (cudaGetSymbolAddress, with that device current).  Calls that
-// overlap in time (two host threads, or two streams of one device) share this scratch and
-// race; the first call on a device does the set-up and must come before any stream capture.
+// (Hessenberg and the least-squares work arrays) is file-scope too.  Every call looks up the
+// array's address in the CUDA context current on the calling thread (cudaGetSymbolAddress:
+// no allocation once the module is loaded).  The address is not cached: after
+// cudaDeviceReset, or with another context current on the same device, the module is
+// loaded anew and the array lives elsewhere.  The first call in a context may load the
+// module (CUDA's lazy loading), which creates the array: make it once as a warm-up outside
+// any region that must not allocate, and before any stream capture.  Calls that overlap in
+// time (two host threads, or two streams of one device) share this scratch and race.
 namespace bit {
 namespace {
 
@@ -589,9 +610,6 @@ constexpr size_t kSegE = 32;
 constexpr size_t kStaticDoubles = kSegA + kSegQ + kSegV + kSegH + kSegY + kSegX + kSegE;
 
 static __device__ __align__(256) double g_dense_static[kStaticDoubles];
-
-constexpr int kStaticDevices = 64;
-double* s_dense_static_ptr[kStaticDevices];  // device address of g_dense_static, per device
 
 constexpr size_t kLd = kStaticMax + 1;
 double s_H[(kStaticMax + 2) * kLd];
@@ -633,19 +651,15 @@ extern "C" bit_status bit_gmres_dense_static(void* stream, int n, const double* 
     put_err(err, errlen, "bit_gmres_dense_static", d);
     return BIT_ERR_CAPACITY;
   }
+  if (rhs_is_zero(n, b)) {  // as bit_gmres_dense: x = 0, no device work
+    for (int i = 0; i < n; i++) x[i] = 0.0;
+    if (iterations) *iterations = 0;
+    return BIT_OK;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  int dev = 0;
-  BIT_STATIC_CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kStaticDevices) {
-    put_err(err, errlen, "bit_gmres_dense_static", "device ordinal out of range");
-    return BIT_ERR_INVALID_ARGUMENT;
-  }
-  if (!s_dense_static_ptr[dev]) {
-    void* p = nullptr;
-    BIT_STATIC_CK(cudaGetSymbolAddress(&p, g_dense_static));
-    s_dense_static_ptr[dev] = static_cast<double*>(p);
-  }
-  double* base = s_dense_static_ptr[dev];
+  void* sym = nullptr;
+  BIT_STATIC_CK(cudaGetSymbolAddress(&sym, g_dense_static));
+  double* base = static_cast<double*>(sym);
   double* A = base;
   double* Q = A + kSegA;
   double* v = Q + kSegQ;

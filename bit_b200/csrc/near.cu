@@ -106,6 +106,32 @@ __device__ __forceinline__ void fpair(double x, double y, double z, double4 s, d
   const double t = s.w / (r * rs);
   ax -= dx * t; ay -= dy * t; az -= dz * t;
 }
+// The same with the reference's KERNEL_ORDER family (eval_grad_kernel_reg,
+// src/tree3d.cpp:80-91): 1/(r rs) plus korder terms, each the previous one times
+// (l + 1/2)/l * del/rs.
+__device__ __forceinline__ void fpair_order(double x, double y, double z, double4 s, double del,
+                                            int korder, double& ax, double& ay, double& az) {
+  const double dx = s.x - x, dy = s.y - y, dz = s.z - z;
+  const double rs = dx * dx + dy * dy + dz * dz + del;
+  const double r = sqrt(rs);
+  double temp = 1.0 / (r * rs), f = temp;
+  for (int l = 1; l <= korder; l++) {
+    f = f * (l + 0.5) / l * del / rs;
+    temp += f;
+  }
+  const double t = s.w * temp;
+  ax -= dx * t; ay -= dy * t; az -= dz * t;
+}
+// Screened 2-D field of one pair (shielded_treeforce's leaf loop, src/tree3d.cpp:3384-3398):
+// t = q e^{-kappa r} / r^2 (kappa + 1/r), fx -= dy t, fy += dx t, no del.
+__device__ __forceinline__ void cpair(double x, double y, double z, double4 s, double kappa,
+                                      double& ax, double& ay) {
+  const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
+  const double rs = dx * dx + dy * dy + dz * dz;
+  const double r = sqrt(rs);
+  const double t = s.w * exp(-kappa * r) / rs * (kappa + 1 / r);
+  ax -= dy * t; ay += dx * t;
+}
 
 template <class T>
 __device__ __forceinline__ T shfl_sum(T v, int tpt) {
@@ -345,15 +371,22 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
         tma_load_1d(tiles + (buf ^ 1) * TILE, src + a.start[nd] + noff,
                     cntn * (unsigned)sizeof(S), &bar[buf ^ 1]);
       }
-      __syncthreads();
+      // Every thread waits (bounded) for this job's tile; the barrier then combines the
+      // outcomes, so the whole CTA takes the same branch.  On a timeout the CTA waits,
+      // bounded again, for both copies it may still have in flight into its shared memory
+      // before it returns, and the host reports the error flag.
+      const bool landed = mbar_wait(&bar[buf], (k >> 1) & 1);
+      if (__syncthreads_or(!landed)) {
+        if (tid == 0) {
+          atomicOr(a.err, 2);
+          mbar_wait(&bar[buf], (k >> 1) & 1);
+          if (ne < e1) mbar_wait(&bar[buf ^ 1], ((k + 1) >> 1) & 1);
+        }
+        return;
+      }
       if (toff == 0) {
         cnt = s_cnt;
         tpt = split_for<F32 && !FORCE>(cnt);
-      }
-      if (!mbar_wait(&bar[buf], (k >> 1) & 1)) {
-        if (tid == 0) atomicOr(a.err, 2);
-        if (ne < e1) mbar_wait(&bar[buf ^ 1], ((k + 1) >> 1) & 1);  // let the other copy land
-        return;
       }
       const S* ts = tiles + buf * TILE;
       const double4 c = a.nodec[node];
@@ -460,8 +493,17 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
             if (valid) {
               const double4* ds = reinterpret_cast<const double4*>(ts);
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
-              for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) fpair(x, y, z, ds[j], sdel, fx, fy, fz);
+              const int korder = se->kernel_order;
+              if (KER == BIT_KERNEL_SCREENED) {
+                for (int j = slice; j < ns; j += tpt)
+                  if (j != selfj) cpair(x, y, z, ds[j], skappa, fx, fy);
+              } else if (korder > 0) {
+                for (int j = slice; j < ns; j += tpt)
+                  if (j != selfj) fpair_order(x, y, z, ds[j], sdel, korder, fx, fy, fz);
+              } else {
+                for (int j = slice; j < ns; j += tpt)
+                  if (j != selfj) fpair(x, y, z, ds[j], sdel, fx, fy, fz);
+              }
             }
           }
           fx = shfl_sum(fx, tpt);
@@ -655,10 +697,18 @@ void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* f
   cudaStream_t s = t->ctx->stream;
   NearArgs a = base_args(t, L, P, t->sx.p, t->sy.p, t->sz.p);
   a.out = fx; a.out_y = fy; a.out_z = fz;
+  // P.force: 1 the regularised Coulomb field (kernel order per system; FP64 beyond order
+  // 0), 2 the screened 2-D field of shielded_treeforce (FP64)
   for (const LaunchClass& k : P.near_classes) {
     a.order = P.near_ord + k.begin;
-    if (P.f32) launch<BIT_KERNEL_COULOMB, false, true, true>(a, k.count, s);
-    else launch<BIT_KERNEL_COULOMB, false, false, true>(a, k.count, s);
+    if (P.force == 2) {
+      if (P.f32) fail(BIT_ERR_INVALID_ARGUMENT, "the screened field is FP64 only");
+      launch<BIT_KERNEL_SCREENED, false, false, true>(a, k.count, s);
+    } else if (P.f32) {
+      launch<BIT_KERNEL_COULOMB, false, true, true>(a, k.count, s);
+    } else {
+      launch<BIT_KERNEL_COULOMB, false, false, true>(a, k.count, s);
+    }
     BIT_CHECK_LAUNCH();
   }
 }

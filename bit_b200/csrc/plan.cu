@@ -15,9 +15,10 @@
 
 namespace bit {
 
-SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int force) {
+SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int force,
+                      int kernel_order) {
   SysEval s{};
-  s.kernel = force ? BIT_KERNEL_COULOMB : p.kernel;
+  s.kernel = force == 1 ? BIT_KERNEL_COULOMB : (force == 2 ? BIT_KERNEL_SCREENED : p.kernel);
   s.nterms = nterms;
   s.acc = p.acc;
   s.kappa = p.kappa;
@@ -25,14 +26,26 @@ SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int forc
   s.particles = !points;
   const bool ref = p.mode == BIT_MODE_REFERENCE;
   // MAC, src/tree3d.cpp:4688-4692 (Coulomb: + del - del), 3472-3476 (screened: - mac_del)
-  if (!force && p.kernel == BIT_KERNEL_SCREENED) {
+  if ((!force && p.kernel == BIT_KERNEL_SCREENED) || force == 2) {
     s.mac_add = 0.0;
     s.mac_sub = p.mac_del;
   } else {
     s.mac_add = p.del;
     s.mac_sub = p.del;
   }
+  if (force == 2) {
+    // shielded_treeforce (src/tree3d.cpp:3268-3408): r^2 without del in both fields, the
+    // screened MAC with its del offset (:3279-3283), no eps check for particles (:3378-3398)
+    s.far_add = 0.0;
+    s.far_sign = 1.0;
+    s.near_del = 0.0;
+    s.near_sign = 1;
+    s.eps_check = 0;
+    s.particles = 1;
+    return s;
+  }
   if (force) {
+    s.kernel_order = kernel_order;
     // treeforce (src/tree3d.cpp:851-971): r^2 + del in both fields
     s.far_add = p.del;
     s.far_sign = 1.0;
@@ -71,7 +84,7 @@ SysEval make_sys_eval(const bit_eval_params& p, int nterms, int points, int forc
 }
 
 void plan_sys(Tree* t, EvalPlan* P, const std::vector<bit_eval_params>& prm, int points,
-              int force) {
+              int force, int kernel_order) {
   const int ns = t->nsys;
   if (prm.empty() || ((int)prm.size() != 1 && (int)prm.size() != ns))
     fail(BIT_ERR_INVALID_ARGUMENT, "one parameter set, or one per system, expected");
@@ -82,7 +95,8 @@ void plan_sys(Tree* t, EvalPlan* P, const std::vector<bit_eval_params>& prm, int
       fail(BIT_ERR_INVALID_ARGUMENT, "all systems of one call share a precision");
   std::vector<SysEval> h(ns);
   for (int s = 0; s < ns; s++)
-    h[s] = make_sys_eval(prm[prm.size() == 1 ? 0 : s], t->h_sys_nterms[s], points, force);
+    h[s] = make_sys_eval(prm[prm.size() == 1 ? 0 : s], t->h_sys_nterms[s], points, force,
+                         kernel_order);
   P->f32 = prm[0].precision == BIT_PREC_MIXED;
   P->force = force;
   const bool same = P->sys.p && P->h_sys.size() == h.size() &&
@@ -190,8 +204,9 @@ void plan_classes(Tree* t, Lists* L, EvalPlan* P) {
 // for it, or built for another MAC and checked against this one; else a new build, which
 // also checks the context's previous MAC (an evaluation that alternates two kernels on
 // each new tree then walks the tree once per tree when their decisions agree).
-void prepare_particles(Tree* t, const std::vector<bit_eval_params>& prm, int force) {
-  plan_sys(t, &t->pplan, prm, 0, force);
+void prepare_particles(Tree* t, const std::vector<bit_eval_params>& prm, int force,
+                       int kernel_order) {
+  plan_sys(t, &t->pplan, prm, 0, force, kernel_order);
   const ListKey k = plan_key(t, t->pplan, 0);
   Lists& L = t->plists;
   Ctx* c = t->ctx;

@@ -4,6 +4,7 @@
 #include "tree3d_b200.h"
 
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -14,14 +15,31 @@
 
 double bit_tree3d_del = 0.01;
 double bit_tree3d_mac_del = 0.01;
+int bit_tree3d_kernel_order = 0;
 int bit_tree3d_precision = 0;
 
 namespace {
 
+// Results of one whole-tree evaluation, valid for exactly the parameters they were computed
+// with: a later call with any other acc, kappa, kernel, del, screened MAC offset or
+// precision recomputes them (moments reset them, so nterms is covered too).
 struct Cached {
-  double acc = -1, kappa = -1;
-  int kind = -1;  // 0 coulomb, 1 screened, 2 force
+  bool valid = false;
+  double acc = 0, kappa = 0, del = 0, mac_del = 0;
+  int kind = -1;  // 0 coulomb, 1 screened, 2 force, 3 screened field
+  int prec = -1, korder = -1;
   std::vector<double> a, b, c;
+  bool matches(int k, double ac, double ka) const {
+    return valid && kind == k && acc == ac && kappa == ka && del == bit_tree3d_del &&
+           mac_del == bit_tree3d_mac_del && prec == bit_tree3d_precision &&
+           korder == bit_tree3d_kernel_order;
+  }
+  void mark(int k, double ac, double ka) {
+    valid = true;
+    kind = k; acc = ac; kappa = ka;
+    del = bit_tree3d_del; mac_del = bit_tree3d_mac_del; prec = bit_tree3d_precision;
+    korder = bit_tree3d_kernel_order;
+  }
 };
 
 struct Entry {
@@ -29,12 +47,25 @@ struct Entry {
   int n = 0, nterms = 0;
   int mom_dim = 0;  // edge of the moment arrays this library allocated (0: none)
   std::vector<double> x, y, z;
-  Cached pot[2], force;
+  Cached pot[2], force, sfield;
+};
+
+// Direct sums of one particle array (one per kind): a snapshot of the particles, the
+// results of every target, and which targets this sweep has served.
+struct DirectSweep {
+  bool valid = false;
+  int n = 0, korder = 0;
+  double param = 0;  // del (force) or alpha (screened)
+  std::vector<double> x, y, z, q;
+  std::vector<double> a, b, c;
+  std::vector<char> served;
 };
 
 std::mutex mu;
 bit_ctx* g_ctx = nullptr;
 std::map<const TREE*, Entry> g_trees;
+// kind: 0 force_particle_ds_reg, 1 force_particle_ds_noreg, 2 shielded_pot_particle_ds
+std::map<std::pair<const PARTICLE*, int>, DirectSweep> g_direct;
 thread_local std::string g_err;
 
 bit_ctx* ctx() {
@@ -43,6 +74,13 @@ bit_ctx* ctx() {
     if (bit_ctx_create(&g_ctx, &o) != BIT_OK) g_ctx = nullptr;
   }
   return g_ctx;
+}
+
+// Every failure is reported on stderr as well as through bit_tree3d_last_error(): the
+// reference's void entry points give a caller no other way to notice one.
+void complain(const std::string& m) {
+  g_err = m;
+  std::fprintf(stderr, "[tree3d_b200] %s\n", m.c_str());
 }
 
 bool ok(bit_status s, const char* what) {
@@ -75,7 +113,7 @@ const char* bit_tree3d_last_error() { return g_err.c_str(); }
 int treemake(int num, int nterms, int maxmemb, PARTICLE* part, TREE* tree) {
   std::lock_guard<std::mutex> lk(mu);
   bit_ctx* c = ctx();
-  if (!c) { g_err = "no CUDA device"; return -1; }
+  if (!c) { complain("no CUDA device"); return -1; }
   Entry e;
   e.n = num;
   e.nterms = nterms;
@@ -116,14 +154,14 @@ int treemake(int num, int nterms, int maxmemb, PARTICLE* part, TREE* tree) {
 void treemoments(int numtree, int nterms, TREE* tree, PARTICLE* part) {
   std::lock_guard<std::mutex> lk(mu);
   auto it = g_trees.find(tree);
-  if (it == g_trees.end()) { g_err = "treemoments: tree not built by treemake"; return; }
+  if (it == g_trees.end()) { complain("treemoments: tree not built by treemake"); return; }
   Entry& e = it->second;
   std::vector<double> q(e.n), w(e.n);
   for (int i = 0; i < e.n; i++) { q[i] = part[i].tot_charge; w[i] = part[i].weight; }
   if (!ok(bit_tree_set_charges(e.tree, q.data(), w.data()), "treemoments")) return;
   if (!ok(bit_tree_moments(e.tree, nterms), "treemoments")) return;
   e.nterms = nterms;
-  e.pot[0] = Cached(); e.pot[1] = Cached(); e.force = Cached();
+  e.pot[0] = Cached(); e.pot[1] = Cached(); e.force = Cached(); e.sfield = Cached();
   const int T = nterms * (nterms + 1) * (nterms + 2) / 6;
   std::vector<double> m((size_t)numtree * T);
   if (!ok(bit_tree_export_moments(e.tree, m.data()), "treemoments")) return;
@@ -174,11 +212,11 @@ static double serve_potential(int kernel, int ind, int p, double x, double y, do
                               double kappa, double acc, double* pot, TREE* tree) {
   std::lock_guard<std::mutex> lk(mu);
   if (ind != 0) {
-    g_err = "only ind == 0 (the whole tree) is served on the GPU";
+    complain("only ind == 0 (the whole tree) is served on the GPU");
     return -1;
   }
   auto it = g_trees.find(tree);
-  if (it == g_trees.end()) { g_err = "tree not built by treemake"; return -1; }
+  if (it == g_trees.end()) { complain("tree not built by treemake"); return -1; }
   Entry& e = it->second;
   bit_eval_params P = prm(kernel, acc, kappa);
   const bool same_point = p >= 0 && p < e.n && x == e.x[p] && y == e.y[p] && z == e.z[p];
@@ -189,10 +227,11 @@ static double serve_potential(int kernel, int ind, int p, double x, double y, do
     return 0;
   }
   Cached& C = e.pot[kernel == BIT_KERNEL_SCREENED];
-  if (C.acc != acc || C.kappa != kappa || C.kind != kernel) {
+  if (!C.matches(kernel, acc, kappa)) {
+    C.valid = false;
     C.a.assign(e.n, 0.0);
     if (!ok(bit_eval_particles(e.tree, &P, C.a.data()), "evaluate particles")) return -1;
-    C.acc = acc; C.kappa = kappa; C.kind = kernel;
+    C.mark(kernel, acc, kappa);
   }
   *pot += C.a[p];
   return 0;
@@ -215,24 +254,183 @@ double treeforce(int ind, int p, int nterms, double x, double y, double z, doubl
                  double* xfor, double* yfor, double* zfor, TREE* tree, PARTICLE*) {
   (void)nterms;
   std::lock_guard<std::mutex> lk(mu);
-  if (ind != 0) { g_err = "only ind == 0 is served on the GPU"; return -1; }
+  if (ind != 0) { complain("only ind == 0 is served on the GPU"); return -1; }
   auto it = g_trees.find(tree);
-  if (it == g_trees.end()) { g_err = "tree not built by treemake"; return -1; }
+  if (it == g_trees.end()) { complain("tree not built by treemake"); return -1; }
   Entry& e = it->second;
   if (!(p >= 0 && p < e.n && x == e.x[p] && y == e.y[p] && z == e.z[p])) {
-    g_err = "treeforce at a point that is not the particle p is not supported";
+    complain("treeforce at a point that is not the particle p is not supported");
     return -1;
   }
   Cached& C = e.force;
-  if (C.acc != acc) {
+  if (!C.matches(2, acc, 0.0)) {
+    C.valid = false;
     C.a.assign(e.n, 0.0); C.b.assign(e.n, 0.0); C.c.assign(e.n, 0.0);
-    if (!ok(bit_eval_force(e.tree, bit_tree3d_del, acc, (bit_precision)bit_tree3d_precision,
-                           C.a.data(), C.b.data(), C.c.data()), "treeforce"))
+    bit_field_params F{};
+    F.kind = BIT_FIELD_COULOMB;
+    F.precision = (bit_precision)bit_tree3d_precision;
+    F.del = bit_tree3d_del;
+    F.acc = acc;
+    F.kernel_order = bit_tree3d_kernel_order;
+    if (!ok(bit_eval_field(e.tree, &F, C.a.data(), C.b.data(), C.c.data()), "treeforce"))
       return -1;
-    C.acc = acc;
+    C.mark(2, acc, 0.0);
   }
   *xfor += C.a[p]; *yfor += C.b[p]; *zfor += C.c[p];
   return 0;
+}
+
+// shielded_treeforce (src/tree3d.cpp:3268-3408): the reference accumulates fx, fy and
+// assigns fz = 0 wherever it adds a term.
+double shielded_treeforce(int ind, int p, int nterms, double x, double y, double z,
+                          double alpha, double acc, double* xfor, double* yfor, double* zfor,
+                          TREE* tree, PARTICLE*) {
+  (void)nterms;
+  std::lock_guard<std::mutex> lk(mu);
+  if (ind != 0) { complain("only ind == 0 is served on the GPU"); return -1; }
+  auto it = g_trees.find(tree);
+  if (it == g_trees.end()) { complain("tree not built by treemake"); return -1; }
+  Entry& e = it->second;
+  if (!(p >= 0 && p < e.n && x == e.x[p] && y == e.y[p] && z == e.z[p])) {
+    complain("shielded_treeforce at a point that is not the particle p is not supported");
+    return -1;
+  }
+  Cached& C = e.sfield;
+  if (!C.matches(3, acc, alpha)) {
+    C.valid = false;
+    C.a.assign(e.n, 0.0); C.b.assign(e.n, 0.0); C.c.assign(e.n, 0.0);
+    bit_field_params F{};
+    F.kind = BIT_FIELD_SCREENED;
+    F.precision = (bit_precision)bit_tree3d_precision;
+    F.mac_del = bit_tree3d_mac_del;
+    F.kappa = alpha;
+    F.acc = acc;
+    if (!ok(bit_eval_field(e.tree, &F, C.a.data(), C.b.data(), C.c.data()), "shielded_treeforce"))
+      return -1;
+    C.mark(3, acc, alpha);
+  }
+  *xfor += C.a[p]; *yfor += C.b[p]; *zfor = 0.0;
+  return 0;
+}
+
+// shielded_freespace_particles_tree (src/tree3d.cpp:2368-2436)
+void shielded_freespace_particles_tree(int npart, PARTICLE* part, double alpha, int nterms,
+                                       double acc, TREE* tree, int numtree, int maxmemb) {
+  numtree = treemake(npart, nterms, maxmemb, part, tree);
+  if (numtree < 0) return;
+  treemoments(numtree, nterms, tree, part);
+  for (int i = 0; i < npart; i++) {
+    double xf = 0, yf = 0, zf = 0;
+    if (shielded_treeforce(0, i, nterms, part[i].x, part[i].y, part[i].z, alpha, acc, &xf, &yf,
+                           &zf, tree, part))
+      return;
+    part[i].xforce = xf * charge_constant * part[i].tot_charge;
+    part[i].yforce = yf * charge_constant * part[i].tot_charge;
+    part[i].zforce = zf * charge_constant * part[i].tot_charge;
+  }
+  treeempty(numtree, tree);
+}
+
+// ---- direct sums ----------------------------------------------------------------------
+namespace {
+
+// The sweep of (part, kind) that serves target ind: the current one while ind has not been
+// served yet and the target still matches the snapshot, else a fresh GPU evaluation of
+// every target from the current particles.  Caller holds mu.
+DirectSweep* direct_sweep(int kind, int ind, int npart, PARTICLE* part, double param) {
+  if (!part || npart < 1 || ind < 0 || ind >= npart) {
+    complain("direct sum: invalid particle index or count");
+    return nullptr;
+  }
+  DirectSweep& S = g_direct[{part, kind}];
+  const int korder = kind == 0 ? bit_tree3d_kernel_order : 0;
+  const PARTICLE& t = part[ind];
+  const bool fresh = S.valid && S.n == npart && S.param == param && S.korder == korder &&
+                     !S.served[ind] && S.x[ind] == t.x && S.y[ind] == t.y && S.z[ind] == t.z &&
+                     S.q[ind] == t.tot_charge;
+  if (fresh) return &S;
+  bit_ctx* c = ctx();
+  if (!c) { complain("no CUDA device"); return nullptr; }
+  S.valid = false;
+  S.n = npart; S.param = param; S.korder = korder;
+  S.x.resize(npart); S.y.resize(npart); S.z.resize(npart); S.q.resize(npart);
+  for (int i = 0; i < npart; i++) {
+    S.x[i] = part[i].x; S.y[i] = part[i].y; S.z[i] = part[i].z; S.q[i] = part[i].tot_charge;
+  }
+  std::vector<int> tg(npart);
+  for (int i = 0; i < npart; i++) tg[i] = i;
+  S.a.assign(npart, 0.0);
+  bit_status st;
+  if (kind == 2) {
+    bit_eval_params P{};
+    P.kernel = BIT_KERNEL_SCREENED;
+    P.mode = BIT_MODE_REFERENCE;
+    P.precision = BIT_PREC_FP64;
+    P.kappa = param;
+    st = bit_direct_potential(c, npart, S.x.data(), S.y.data(), S.z.data(), S.q.data(), &P, npart,
+                              tg.data(), S.a.data());
+  } else {
+    S.b.assign(npart, 0.0);
+    S.c.assign(npart, 0.0);
+    st = bit_direct_field(c, npart, S.x.data(), S.y.data(), S.z.data(), S.q.data(), kind == 0,
+                          param, korder, npart, tg.data(), S.a.data(), S.b.data(), S.c.data());
+  }
+  if (!ok(st, "direct sum")) return nullptr;
+  S.served.assign(npart, 0);
+  S.valid = true;
+  return &S;
+}
+
+}  // namespace
+
+void force_particle_ds_reg(int ind, int npart, PARTICLE* part, double* xfor, double* yfor,
+                           double* zfor) {
+  std::lock_guard<std::mutex> lk(mu);
+  DirectSweep* S = direct_sweep(0, ind, npart, part, bit_tree3d_del);
+  if (!S) return;
+  S->served[ind] = 1;
+  *xfor = S->a[ind]; *yfor = S->b[ind]; *zfor = S->c[ind];
+}
+
+void force_particle_ds_noreg(int ind, int npart, PARTICLE* part, double* xfor, double* yfor,
+                             double* zfor) {
+  std::lock_guard<std::mutex> lk(mu);
+  DirectSweep* S = direct_sweep(1, ind, npart, part, 0.0);
+  if (!S) return;
+  S->served[ind] = 1;
+  *xfor = S->a[ind]; *yfor = S->b[ind]; *zfor = S->c[ind];
+}
+
+void shielded_pot_particle_ds(int ind, int npart, PARTICLE* part, double* pot, double alpha) {
+  std::lock_guard<std::mutex> lk(mu);
+  DirectSweep* S = direct_sweep(2, ind, npart, part, alpha);
+  if (!S) return;
+  S->served[ind] = 1;
+  *pot = S->a[ind];
+}
+
+// ---- the reference tests' fixture --------------------------------------------------------
+// RandL and boxparticles (src/tree3d.cpp:13-15, 1698-1740): the same rand() draws in the same
+// order, so the particles equal the reference's on the same C library.
+double RandL(void) { return std::rand() / (double)RAND_MAX; }
+
+void boxparticles(int npart, double dlength, double dheight, double ddepth, PARTICLE* part,
+                  double density) {
+  const double weight = density * dlength * dheight * ddepth / npart;
+  std::srand(100);
+  const double hx = dlength / 2, hy = dheight / 2, hz = ddepth / 2;
+  for (int i = 0; i < npart; i++) {
+    PARTICLE& p = part[i];
+    p.charge = -1.0;
+    p.weight = weight;
+    p.x = hx / 2 + RandL() * hx;
+    p.y = hy / 2 + RandL() * hy;
+    p.z = hz / 2 + RandL() * hz;
+    p.u = (RandL() - 0.5) * 1e6;
+    p.v = (RandL() - 0.5) * 1e6;
+    p.w = (RandL() - 0.5) * 1e6;
+    p.tot_charge = p.charge * p.weight * elec;
+  }
 }
 
 // freespace_particles_tree (src/tree3d.cpp:2268-2335)
@@ -275,7 +473,7 @@ void output_potential(int npart, PARTICLE* part, double* pot, std::string filena
   }
   const bit_status st = bit_write_potential(filename.c_str(), npart, x.data(), y.data(),
                                             z.data(), pot);
-  if (st != BIT_OK) g_err = "output_potential: cannot write " + filename;
+  if (st != BIT_OK) complain("output_potential: cannot write " + filename);
 }
 
 int loc_update(int npart, PARTICLE* part, double dt) {

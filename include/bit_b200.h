@@ -155,6 +155,31 @@ bit_status bit_eval_points(bit_tree* tree, const bit_eval_params* prm, int m,
 bit_status bit_eval_force(bit_tree* tree, double del, double acc, bit_precision prec,
                           double* fx, double* fy, double* fz);
 
+/* Fields at every particle, generalising bit_eval_force.  Host arrays, original order. */
+#define BIT_KERNEL_ORDER_MAX 8
+typedef enum {
+  /* treeforce (src/tree3d.cpp:851-971) with treetaylorforce (:456-810) and
+   * eval_grad_kernel_reg (:73-97): the field of 1/sqrt(r^2 + del), regularised by the
+   * reference's KERNEL_ORDER family (src/problem.h:13) of order kernel_order. */
+  BIT_FIELD_COULOMB = 0,
+  /* shielded_treeforce (src/tree3d.cpp:3268-3408) with shielded_treetaylorforce
+   * (:2745-2973): the reference's screened 2-D field, fx = -d/dy, fy = d/dx of
+   * q e^{-kappa r}/r summed over the sources, fz = 0; r^2 without del, the screened MAC
+   * sqradius < acc (r^2 - mac_del) (:3279-3283); no eps check at particle targets. */
+  BIT_FIELD_SCREENED = 1
+} bit_field_kind;
+typedef struct {
+  bit_field_kind kind;
+  bit_precision precision; /* MIXED only for BIT_FIELD_COULOMB with kernel_order 0 */
+  double del;              /* COULOMB: DEL of r^2 + del                                */
+  double mac_del;          /* SCREENED: the MAC offset (the reference subtracts DEL)   */
+  double kappa;            /* SCREENED: the screening parameter (alpha)               */
+  double acc;              /* MAC parameter                                            */
+  int kernel_order;        /* COULOMB: 0..BIT_KERNEL_ORDER_MAX                        */
+} bit_field_params;
+bit_status bit_eval_field(bit_tree* tree, const bit_field_params* prm, double* fx, double* fy,
+                          double* fz);
+
 /* Time stepping of the reference's particle loop, device-resident: every step rebuilds
  * the tree from the current positions and runs freespace_particles_tree
  * (src/tree3d.cpp:2268-2335: treemake, treemoments, treeforce, F = field * charge_constant
@@ -193,6 +218,23 @@ bit_status bit_direct_potential_device(bit_ctx* ctx, int n, const double* x, con
                                        const double* z, const double* q,
                                        const bit_eval_params* prm, int m, const int* targets,
                                        double* pot);
+
+/* FP64 field direct sum at m particle targets (indices into the n sources; each target
+ * skips itself by index), fx/fy/fz[i] for targets[i]: with regularised != 0,
+ * force_particle_ds_reg (src/tree3d.cpp:298-330): sum q_j G(x_j - x), G(d) = -d t,
+ * t = 1/(r rs) plus the KERNEL_ORDER terms of eval_grad_kernel_reg (:73-97), rs = |d|^2 + del;
+ * with regularised == 0, force_particle_ds_noreg (:182-213): t = 1/(rs sqrt(rs)),
+ * rs = |d|^2 (coincident particles give inf / NaN, as in the reference).  Host arrays. */
+bit_status bit_direct_field(bit_ctx* ctx, int n, const double* x, const double* y,
+                            const double* z, const double* q, int regularised, double del,
+                            int kernel_order, int m, const int* targets, double* fx, double* fy,
+                            double* fz);
+
+/* Measured CUDA-core FMA throughput of the context's device in flop/s (2 per FMA): FP32
+ * (BIT_PREC_MIXED) or FP64 (BIT_PREC_FP64), from a dense FMA-chain kernel timed with CUDA
+ * events (best of 3 launches of about 0.1 s).  The denominator of the near- and
+ * far-field rooflines; no reference counterpart. */
+bit_status bit_device_fma_peak(bit_ctx* ctx, bit_precision prec, double* flops_per_s);
 
 bit_status bit_tree_stats(const bit_tree* tree, bit_stats* st);
 
@@ -359,18 +401,24 @@ bit_status bit_bie_solve(bit_tree* tree, const bit_eval_params* prm, int nterms,
 bit_status bit_gmres_dense(bit_ctx* ctx, int n, const double* a, const double* b, double* x,
                            int* iterations);
 
-/* bit_gmres_dense without any allocation at call time, for callers that cannot allocate
- * (no reference counterpart: it is the same solve as bit_gmres_dense / solver::gmres,
- * src/solver.h:157-310, with the same kernels and results).
- * Scratch is one file-scope device array (about 4.2 MB) sized for n <= BIT_GMRES_STATIC_MAX,
- * plus file-scope host arrays; no cudaMalloc / cudaFree and no allocating library call is
- * made.  n > BIT_GMRES_STATIC_MAX returns BIT_ERR_CAPACITY.  Runs on the calling thread's
- * current device, on `stream` (a cudaStream_t; NULL = the default stream), with host
- * arrays a (row-major n x n), b, x (initial values in, solution out).  A message for any
- * error goes to err (errlen bytes, NUL-terminated; may be NULL).
- * Calls that overlap in time share the scratch and race: serialise them.  The first call
- * on a device looks up the scratch's address (cudaGetSymbolAddress) and must come before
- * any stream capture. */
+/* bit_gmres_dense without any allocation at call time, for callers that cannot allocate:
+ * code running where cudaMalloc is forbidden or unsafe (inside a caller's own memory pool
+ * or allocator hook, a real-time loop with a fixed memory plan, or a host that has
+ * reserved all device memory up front).  No reference counterpart; it gives the same
+ * results as bit_gmres_dense with the same kernels.
+ * Scratch is one file-scope device array (about 4.2 MB, held by every GPU that loads this
+ * library until the process exits) sized for n <= BIT_GMRES_STATIC_MAX, plus file-scope
+ * host arrays; no cudaMalloc / cudaFree and no allocating library call is made.
+ * n > BIT_GMRES_STATIC_MAX returns BIT_ERR_CAPACITY with a message.  Runs in the CUDA
+ * context current on the calling thread, on `stream` (a cudaStream_t; NULL = the default
+ * stream), with host arrays a (row-major n x n), b, x (initial values in, solution out);
+ * b = 0 returns x = 0.  A message for any error goes to err (errlen bytes, NUL-terminated;
+ * may be NULL).
+ * Every call looks up the scratch's address in the current context (cudaGetSymbolAddress).
+ * The first call in a context may load this library's device code (CUDA lazy loading),
+ * which creates the array: make one warm-up call per device outside any region that must
+ * not allocate, and before any stream capture.
+ * Calls that overlap in time share the scratch and race: serialise them. */
 #define BIT_GMRES_STATIC_MAX 512
 bit_status bit_gmres_dense_static(void* stream, int n, const double* a, const double* b,
                                   double* x, int* iterations, char* err, int errlen);

@@ -19,6 +19,12 @@
  *    without touching *pot.
  *  - treemake reports failure by returning -1 (the reference never returns on >maxmemb
  *    coincident particles) and a message from bit_tree3d_last_error().
+ *  - KERNEL_ORDER > 0 and the screened 2-D field are FP64 only: with
+ *    bit_tree3d_precision = 1 those calls report an error.
+ *
+ * A program written against the reference compiles unchanged with include/tree3d_compat
+ * first on its include path: its tree3d.h and constants.h there include this header,
+ * and the program's own problem.h sets DEL and KERNEL_ORDER at start-up.
  */
 #ifndef TREE3D_B200_H
 #define TREE3D_B200_H
@@ -64,8 +70,17 @@ struct TREE {
 /* run-time problem constants (the reference's src/problem.h:11-13) */
 extern double bit_tree3d_del;
 extern double bit_tree3d_mac_del;   /* screened MAC offset; the reference uses DEL */
+extern int bit_tree3d_kernel_order; /* KERNEL_ORDER (0 = the one-parameter kernel)   */
 extern int bit_tree3d_precision;    /* 0 = FP64 (default), 1 = mixed FP32 */
 const char* bit_tree3d_last_error();
+
+/* src/tree3d.cpp:13-15 and 1698-1740: the reference tests' fixture, npart particles
+ * uniform in the middle half of a dlength x dheight x ddepth box from srand(100) / rand()
+ * (the same draws in the same order, so the same particles on the same C library),
+ * charge -1, weight density * volume / npart, tot_charge = charge * weight * elec. */
+double RandL(void);
+void boxparticles(int npart, double dlength, double dheight, double ddepth, PARTICLE* part,
+                  double density);
 
 int treemake(int num, int nterms, int maxmemb, PARTICLE* part, TREE* tree);
 void treeempty(int numtree, TREE* tree);
@@ -80,6 +95,25 @@ double treeforce(int ind, int p, int nterms, double x, double y, double z, doubl
                  double* xfor, double* yfor, double* zfor, TREE* tree, PARTICLE* part);
 void freespace_particles_tree(int npart, PARTICLE* part, int nterms, double acc, TREE* tree,
                               int numtree, int maxmemb);
+/* src/tree3d.cpp:3268-3408 and 2368-2436: the screened 2-D field (FP64) and its driver;
+ * served like treeforce. */
+double shielded_treeforce(int ind, int p, int nterms, double x, double y, double z,
+                          double alpha, double acc, double* xfor, double* yfor, double* zfor,
+                          TREE* tree, PARTICLE* part);
+void shielded_freespace_particles_tree(int npart, PARTICLE* part, double alpha, int nterms,
+                                       double acc, TREE* tree, int numtree, int maxmemb);
+
+/* Direct sums (src/tree3d.cpp:298-330, 182-213, 1966-2016), assigning the field or
+ * potential of particle ind from all others.  On the GPU: the first call evaluates every
+ * particle of part[] and later calls are served from that result until a target is asked
+ * for a second time or its own position or charge differs from the snapshot; then the
+ * sums are evaluated afresh from the current part[].  A caller that changes the particles
+ * between two complete sweeps over the targets therefore sees the new values. */
+void force_particle_ds_reg(int ind, int npart, PARTICLE* part, double* xfor, double* yfor,
+                           double* zfor);
+void force_particle_ds_noreg(int ind, int npart, PARTICLE* part, double* xfor, double* yfor,
+                             double* zfor);
+void shielded_pot_particle_ds(int ind, int npart, PARTICLE* part, double* pot, double alpha);
 /* src/tree3d.cpp:4842-4850 and :4880-4888: explicit velocity and position updates */
 int vel_update(int npart, PARTICLE* part, double dt);
 int loc_update(int npart, PARTICLE* part, double dt);

@@ -12,31 +12,52 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-TAGS = {0.01: "d1e-2", 1e-4: "d1e-4", 2.5e-5: "d2.5e-5"}
-REF_SRC = os.environ.get("BIT_REFERENCE_SRC", "/root/reference/src")
+# (DEL, KERNEL_ORDER) of every library the recipe builds
+TAGS = {(0.01, 0): "d1e-2", (1e-4, 0): "d1e-4", (2.5e-5, 0): "d2.5e-5",
+        (0.01, 1): "d1e-2k1", (0.01, 2): "d1e-2k2"}
+# The reference's src/ directory, for building only (the libraries travel prebuilt).
+REF_SRC = os.environ.get("BIT_REFERENCE_SRC")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 _libs = {}
 
 
-def path(del_):
-    return os.path.join(HERE, "_ref", f"libref_{TAGS[del_]}.so")
+def path(del_, korder=0):
+    return os.path.join(HERE, "_ref", f"libref_{TAGS[(del_, korder)]}.so")
 
 
-def available(del_=0.01):
-    return del_ in TAGS and os.path.exists(path(del_))
+def available(del_=0.01, korder=0):
+    return (del_, korder) in TAGS and os.path.exists(path(del_, korder))
 
 
-def build():
-    """Build the reference libraries when the reference sources are present."""
-    if os.path.exists(os.path.join(REF_SRC, "tree3d.cpp")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={REF_SRC}"], check=True)
+def build(src=None):
+    """Build the reference libraries from the reference's src/ directory (`src`, else
+    BIT_REFERENCE_SRC); a no-op when neither names one that holds tree3d.cpp."""
+    src = src or REF_SRC
+    if src and os.path.exists(os.path.join(src, "tree3d.cpp")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={src}"], check=True)
 
 
-def lib(del_=0.01):
-    if del_ not in _libs:
-        L = C.CDLL(path(del_))
+def build_dropin(src=None):
+    """Compile the reference's own tests/treecode.cpp, treecode_mp.cpp and directsum_mp.cpp
+    unchanged against the drop-in (oracle/_ref/dropin/); needs libtree3d_b200.so built."""
+    src = src or REF_SRC
+    if src and os.path.exists(os.path.join(src, "tree3d.cpp")):
+        subprocess.run(["make", "-s", "-C", HERE, "dropin", f"REF_SRC={src}"], check=True)
+
+
+DROPIN_TESTS = ("treecode", "treecode_mp", "directsum_mp")
+
+
+def dropin_path(name):
+    return os.path.join(HERE, "_ref", "dropin", name)
+
+
+def lib(del_=0.01, korder=0):
+    key = (del_, korder)
+    if key not in _libs:
+        L = C.CDLL(path(del_, korder))
         L.ref_del.restype = C.c_double
         L.ref_boxparticles.argtypes = [C.c_int] + [C.c_double] * 4 + [_dp] * 5
         L.ref_tree_build.restype = C.c_void_p
@@ -61,11 +82,14 @@ def lib(del_=0.01):
         L.ref_gmres_dense.restype = C.c_int
         L.ref_gmres_dense.argtypes = [C.c_int, _dp, _dp, _dp]
         L.ref_output_potential.argtypes = [C.c_int] + [_dp] * 4 + [C.c_char_p]
+        L.ref_eval_screened_field.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, _ip,
+                                              _dp, _dp, _dp, _dp, _dp, _dp, C.c_int]
+        L.ref_ds_force_noreg.argtypes = [C.c_int] + [_dp] * 4 + [C.c_int, _ip] + [_dp] * 3 + [C.c_int]
         L.ref_setboundaries.restype = C.c_int
         L.ref_setboundaries.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp]
         L.ref_panelconstantsreal.argtypes = [C.c_int] * 3 + [C.c_double] * 3 + [_dp]
-        _libs[del_] = L
-    return _libs[del_]
+        _libs[key] = L
+    return _libs[key]
 
 
 def _d(a):
@@ -86,8 +110,8 @@ def boxparticles(n, dlength=1.0, dheight=1.0, ddepth=1.0, density=1.0):
 class RefTree:
     """treemake + treemoments of the reference on caller particles."""
 
-    def __init__(self, x, y, z, q, nterms, maxmemb, del_=0.01, w=None, cap=None):
-        self.L = lib(del_)
+    def __init__(self, x, y, z, q, nterms, maxmemb, del_=0.01, w=None, cap=None, korder=0):
+        self.L = lib(del_, korder)
         self.del_ = del_
         self.x, self.y, self.z, self.q = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q)]
         self.w = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
@@ -163,11 +187,29 @@ class RefTree:
         return fx, fy, fz
 
 
-def ds_force_reg(x, y, z, q, targets, del_=0.01, nthreads=0):
+    def screened_field(self, kappa, acc, targets=None, points=None, nthreads=0):
+        """shielded_treeforce: the reference's screened 2-D field."""
+        p, (tx, ty, tz) = self._targets(targets, points)
+        fx, fy, fz = np.zeros(len(p)), np.zeros(len(p)), np.zeros(len(p))
+        self.L.ref_eval_screened_field(self.h, kappa, acc, len(p), _i(p), _d(tx), _d(ty), _d(tz),
+                                       _d(fx), _d(fy), _d(fz), nthreads)
+        return fx, fy, fz
+
+
+def ds_force_noreg(x, y, z, q, targets, nthreads=0):
     x, y, z, q = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q)]
     t = np.ascontiguousarray(targets, dtype=np.int32)
     fx, fy, fz = np.zeros(len(t)), np.zeros(len(t)), np.zeros(len(t))
-    lib(del_).ref_ds_force_reg(len(x), _d(x), _d(y), _d(z), _d(q), len(t), _i(t), _d(fx),
+    lib(0.01).ref_ds_force_noreg(len(x), _d(x), _d(y), _d(z), _d(q), len(t), _i(t), _d(fx),
+                                 _d(fy), _d(fz), nthreads)
+    return fx, fy, fz
+
+
+def ds_force_reg(x, y, z, q, targets, del_=0.01, nthreads=0, korder=0):
+    x, y, z, q = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, q)]
+    t = np.ascontiguousarray(targets, dtype=np.int32)
+    fx, fy, fz = np.zeros(len(t)), np.zeros(len(t)), np.zeros(len(t))
+    lib(del_, korder).ref_ds_force_reg(len(x), _d(x), _d(y), _d(z), _d(q), len(t), _i(t), _d(fx),
                                _d(fy), _d(fz), nthreads)
     return fx, fy, fz
 
@@ -188,11 +230,12 @@ def grad_kernel(dx, dy, dz, rs, reg, del_=0.01):
 
 
 def gmres_dense(A, b, x0=None):
+    """solver::gmres on a dense matrix: (x, Arnoldi steps taken)."""
     A = np.ascontiguousarray(A, dtype=np.float64)
     b = np.ascontiguousarray(b, dtype=np.float64)
     x = np.ones(len(b)) if x0 is None else np.ascontiguousarray(x0, dtype=np.float64).copy()
-    lib(0.01).ref_gmres_dense(len(b), _d(A), _d(b), _d(x))
-    return x
+    steps = lib(0.01).ref_gmres_dense(len(b), _d(A), _d(b), _d(x))
+    return x, steps
 
 
 def setboundaries(xp, yp, zp, dl, dh, dd, del_=0.01):

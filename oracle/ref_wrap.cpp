@@ -25,7 +25,13 @@ const double DEL = BIT_REF_DEL;
 const int KERNEL_ORDER = BIT_REF_KORDER;
 
 #include "tree3d.cpp"
+// solver's work arrays are private members (src/solver.h:31-42); the GMRES test reads its
+// Hessenberg after a solve to count the Arnoldi steps, so this translation unit declares
+// the class with public members.  Every header solver.h includes (<cmath>, <iostream>) is
+// already included above, so the macro touches only the solver class itself.
+#define class struct
 #include "solver.h"
+#undef class
 
 #include <omp.h>
 #include <vector>
@@ -275,7 +281,10 @@ void ref_eval_grad_kernel(double dx, double dy, double dz, double rs, int reg,
 }
 
 // solver::gmres (src/solver.h:157-260) on a dense row-major n x n matrix.
-// x must hold the caller's initial values (only used by the stopping test).
+// x must hold the caller's initial values (only used by the stopping test).  Returns the
+// number of Arnoldi steps taken: gmres() zeroes the (n+2) x (n+1) Hessenberg first
+// (:174-177) and step j writes column j, whose subdiagonal h[j+1][j] = |v| is nonzero
+// unless v vanished exactly.
 int ref_gmres_dense(int n, const double* A, const double* b, double* x) {
   std::vector<double*> rows(n);
   std::vector<double> a(A, A + (long)n * n);
@@ -283,7 +292,47 @@ int ref_gmres_dense(int n, const double* A, const double* b, double* x) {
   std::vector<double> bb(b, b + n);
   solver s;
   s.makeFram(n + 1);
-  return s.gmres(rows.data(), bb.data(), x, n);
+  s.gmres(rows.data(), bb.data(), x, n);
+  int steps = 0;
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i <= j + 1; i++)
+      if (s.h[i][j] != 0.0) steps = j + 1;
+  return steps;
+}
+
+// shielded_treeforce (src/tree3d.cpp:3268-3408) at particle (p >= 0) or point targets.
+void ref_eval_screened_field(void* h, double kappa, double acc, int nt, const int* p,
+                             const double* tx, const double* ty, const double* tz,
+                             double* fx, double* fy, double* fz, int nthreads) {
+  RefTree* t = static_cast<RefTree*>(h);
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < nt; i++) {
+    int pi = p ? p[i] : -1;
+    double x = pi >= 0 ? t->part[pi].x : tx[i];
+    double y = pi >= 0 ? t->part[pi].y : ty[i];
+    double z = pi >= 0 ? t->part[pi].z : tz[i];
+    double a = 0.0, b = 0.0, c = 0.0;
+    shielded_treeforce(0, pi, t->nterms, x, y, z, kappa, acc, &a, &b, &c, t->tree, t->part);
+    fx[i] = a; fy[i] = b; fz[i] = c;
+  }
+}
+
+// force_particle_ds_noreg (src/tree3d.cpp:182-213) for the listed particle targets.
+void ref_ds_force_noreg(int n, const double* x, const double* y, const double* z,
+                        const double* q, int nt, const int* p, double* fx, double* fy,
+                        double* fz, int nthreads) {
+  std::vector<PARTICLE> part(n);
+  for (int i = 0; i < n; i++) {
+    part[i].x = x[i]; part[i].y = y[i]; part[i].z = z[i]; part[i].tot_charge = q[i];
+  }
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < nt; i++) {
+    double a = 0, b = 0, c = 0;
+    force_particle_ds_noreg(p[i], n, part.data(), &a, &b, &c);
+    fx[i] = a; fy[i] = b; fz[i] = c;
+  }
 }
 
 // setboundaries (src/tree3d.cpp:3764-3934): the box's boundary panels, 17 doubles each

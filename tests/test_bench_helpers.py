@@ -1,6 +1,6 @@
-"""bench.py's host-side helpers: the per-launch DRAM traffic it reports as
-roofline.traffic comes from the committed launch-list profile, the far-field flops per
-pair from the generator, and the FP32 peak from the sampled clock.  No GPU."""
+"""bench.py's host-side helpers: the far-field flops per pair come from the generator, the
+rooflines divide them by measured peaks, and the matched-accuracy parameters name valid
+expansion orders.  No GPU."""
 import importlib.util
 import os
 
@@ -14,17 +14,27 @@ def bench():
     return b
 
 
-def test_profiled_traffic_lines_parse():
-    b = bench()
-    for key in ("k_far_screened_f32", "k_near_screened_f32"):
-        v = b.profiled_traffic(key)
-        assert isinstance(v, int) and 10 ** 7 < v < 10 ** 10, (key, v)
-
-
-def test_far_flops_and_peak():
+def test_far_flops_per_pair():
     b = bench()
     f = b.far_flops_per_pair(9)
     assert f["coulomb"] == 1459 and f["screened"] == 2414
-    p = b.fp32_peak_from_clock({"sm_mhz": 1965.0})
-    assert abs(p["tflops"] - 148 * 128 * 2 * 1.965e9 / 1e12) < 1e-9
-    assert abs(p["mufu_ops"] - 148 * 16 * 1.965e9) < 1.0
+
+
+def test_roofline_entries():
+    b = bench()
+    st = {"far_pairs": 1000, "t_far": 1e-3, "near_pairs": 5000, "t_near": 2e-3}
+    r = b.roofline_far("fp64", "screened", st, 2414, 36.0)
+    assert abs(r["achieved"] - 2414 * 1000 / 1e-3 / 1e12) < 1e-12
+    assert abs(r["frac"] - r["achieved"] / 36.0) < 1e-12
+    assert r["kernel"] == "k_far<9, SCREENED, double>" and "measured" in r["peak_source"]
+    n = 1000
+    r = b.roofline_near("mixed", "coulomb", st, n, 72.0)
+    assert abs(r["achieved"] - 11 * (5000 - n) / 2e-3 / 1e12) < 1e-12
+    assert r["bound"] == "fp32+mufu"
+
+
+def test_matched_parameters():
+    b = bench()
+    for d in (b.MATCHED_C2, b.MATCHED_BIE):
+        assert 1 <= d["nterms"] <= 10 and 0 < d["acc"] < 1 and d["maxmemb"] > 0
+    assert sorted(b.MATCHED_BATCH_ACC) == [5, 7, 9]

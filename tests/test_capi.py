@@ -62,5 +62,44 @@ def test_shim_library_exports_reference_names():
         pass
     out = os.popen(f"nm -DC {path}").read()
     for name in ["treemake(", "treemoments(", "treepotential(", "shielded_treepot(",
-                 "treeforce(", "treeempty(", "freespace_particles_tree(", "solver::gmres("]:
+                 "treeforce(", "treeempty(", "freespace_particles_tree(", "solver::gmres(",
+                 "boxparticles(", "force_particle_ds_reg(", "force_particle_ds_noreg(",
+                 "shielded_pot_particle_ds(", "shielded_treeforce(",
+                 "shielded_freespace_particles_tree(", "RandL("]:
         assert name in out, name
+
+
+def _shim_symbol(path, demangled_prefix):
+    for line in os.popen(f"nm -D --defined-only {path}").read().splitlines():
+        parts = line.split()
+        if len(parts) == 3:
+            dm = os.popen(f"c++filt {parts[2]}").read().strip()
+            if dm.startswith(demangled_prefix):
+                return parts[2]
+    return None
+
+
+def test_boxparticles_matches_reference():
+    """The drop-in's boxparticles (host code, no GPU) draws the reference fixture's
+    particles bit for bit (src/tree3d.cpp:1698-1740, srand(100) and rand())."""
+    import ctypes
+    import numpy as np
+    from oracle import ref
+    if not ref.available(0.01):
+        pytest.skip("reference build not present")
+    path = os.path.join(ROOT, "bit_b200", "lib", "libtree3d_b200.so")
+    if not os.path.exists(path):
+        pytest.skip("shim not built")
+    sym = _shim_symbol(path, "boxparticles(")
+    assert sym, "boxparticles not exported"
+    L = ctypes.CDLL(path)
+    f = getattr(L, sym)
+    n = 1000
+    part = np.zeros((n, 12))  # PARTICLE: 12 doubles (charge x y z u v w xforce yforce zforce weight tot_charge)
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_void_p, ctypes.c_double]
+    f(n, 1.0, 2.0, 0.5, part.ctypes.data, 1.5)
+    x, y, z, q, w = ref.boxparticles(n, 1.0, 2.0, 0.5, 1.5)
+    for col, want in ((1, x), (2, y), (3, z), (11, q), (10, w)):
+        assert (part[:, col].view(np.int64) == want.view(np.int64)).all(), col
+    assert (part[:, 0] == -1.0).all()

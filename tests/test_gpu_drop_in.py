@@ -21,3 +21,27 @@ def test_reference_style_program(tmp_path):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "Test PASSED" in r.stdout
+
+
+def _dropin_env():
+    env = dict(os.environ)
+    env.setdefault("OMP_NUM_THREADS", "8")
+    return env
+
+
+@pytest.mark.parametrize("name", ["treecode", "treecode_mp", "directsum_mp"])
+def test_reference_test_program_unchanged(name):
+    """The reference's own tests/<name>.cpp, compiled unchanged against the drop-in
+    (include/tree3d_compat first on the include path, the reference's problem.h; built by
+    oracle/Makefile's dropin recipe), prints Test PASSED with every call served by the GPU
+    library (any failing drop-in call prints a [tree3d_b200] line on stderr)."""
+    from oracle import ref
+    exe = ref.dropin_path(name)
+    if not os.path.exists(exe):
+        pytest.skip("reference test programs were not built (no reference sources at build time)")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=600, env=_dropin_env(),
+                       cwd=os.path.dirname(exe))
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Test PASSED" in r.stdout
+    assert "[tree3d_b200]" not in r.stderr, r.stderr

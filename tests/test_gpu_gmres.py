@@ -20,6 +20,32 @@ def test_dense_gmres_matches_restatement(ctx, orc):
     assert np.linalg.norm(x_gpu - x_cpu) / np.linalg.norm(x_cpu) < 1e-6
 
 
+@pytest.mark.parametrize("n,seed", [(64, 1), (300, 4), (700, 5)])
+def test_dense_gmres_matches_reference_solver(ctx, n, seed):
+    """The device solver against the reference's own solver::gmres (src/solver.h:157-310,
+    built unmodified into oracle/_ref): the same number of Arnoldi steps and the same
+    solution to 1e-10 relative (the algorithm and its stop test are the same; only the
+    summation order of the device's dot products differs)."""
+    from oracle import ref
+    if not ref.available(0.01):
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(seed)
+    A = np.eye(n) * 3 + rng.uniform(-0.5, 0.5, (n, n)) / np.sqrt(n)
+    b = rng.uniform(-1, 1, n)
+    x_ref, it_ref = ref.gmres_dense(A, b)
+    x_gpu, it_gpu, st = ctx.gmres_dense(A, b)
+    assert st == 0
+    assert it_gpu == it_ref, (it_gpu, it_ref)
+    assert np.linalg.norm(x_gpu - x_ref) / np.linalg.norm(x_ref) < 1e-10
+
+
+def test_dense_gmres_zero_rhs(ctx):
+    """b = 0: x = 0 after no step (the reference would divide by |b| = 0)."""
+    A = np.eye(8) * 2.0
+    x, it, st = ctx.gmres_dense(A, np.zeros(8))
+    assert st == 0 and it == 0 and not x.any()
+
+
 def test_dense_gmres_breakdown(ctx):
     """A Krylov space that closes at step 1 reports breakdown (src/solver.h:220-225)."""
     n = 16

@@ -139,6 +139,22 @@ def test_dense_gmres_restatement(orc):
     np.testing.assert_allclose(A @ x, b, rtol=0, atol=1e-5 * np.abs(b).max() * 10)
 
 
+def test_dense_gmres_restatement_matches_reference(orc):
+    """The restatement of solver::gmres against the reference's own (oracle/_ref): the same
+    Arnoldi step count and solution to 1e-12."""
+    from oracle import ref
+    if not ref.available(0.01):
+        pytest.skip("reference build not present")
+    rng = np.random.default_rng(9)
+    n = 200
+    A = np.eye(n) * 3 + rng.uniform(-0.5, 0.5, (n, n)) / np.sqrt(n)
+    b = rng.uniform(-1, 1, n)
+    x_ref, it_ref = ref.gmres_dense(A, b)
+    x, it = orc.gmres_dense_ref(A, b)
+    assert it == it_ref
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-12
+
+
 def test_restarted_gmres_treecode(orc):
     """GMRES(m) with the CPU treecode matvec reaches its residual target."""
     from bit_b200 import workloads

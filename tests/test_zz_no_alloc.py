@@ -60,3 +60,54 @@ def test_static_refuses_sizes_over_the_limit():
     st, _, _, msg = static_solve(n, A, b)
     assert st == 4  # BIT_ERR_CAPACITY
     assert "512" in msg and "513" in msg
+
+
+_SECOND_CONTEXT = r"""
+import ctypes as C, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import bit_b200 as B
+L = B.lib()
+dp = C.POINTER(C.c_double)
+rng = np.random.default_rng(7)
+n = 256
+A = np.ascontiguousarray(np.eye(n) * 3 + rng.uniform(-0.5, 0.5, (n, n)) / np.sqrt(n))
+b = rng.uniform(-1, 1, n)
+def solve():
+    x = np.ones(n)
+    it = C.c_int()
+    err = C.create_string_buffer(256)
+    st = L.bit_gmres_dense_static(None, n, A.ctypes.data_as(dp), b.ctypes.data_as(dp),
+                                  x.ctypes.data_as(dp), C.byref(it), err, len(err))
+    assert st == 0, err.value
+    return x, it.value
+x1, it1 = solve()  # in the device's primary context
+cu = C.CDLL("libcuda.so.1")
+assert cu.cuInit(0) == 0
+dev, ctx = C.c_int(), C.c_void_p()
+assert cu.cuDeviceGet(C.byref(dev), 0) == 0
+assert cu.cuCtxCreate_v2(C.byref(ctx), 0, dev) == 0  # now current on this thread
+x2, it2 = solve()  # the library's code and scratch are loaded anew in this context
+assert cu.cuCtxDestroy_v2(ctx) == 0
+assert it1 == it2 and (x1 == x2).all()
+exact = np.linalg.solve(A, b)
+assert np.linalg.norm(x2 - exact) / np.linalg.norm(exact) < 1e-5
+print("second context ok")
+"""
+
+
+@pytest.mark.gpu
+def test_static_in_a_second_context_of_the_same_device():
+    """A second CUDA context on the same device (a driver-API caller, or the runtime after
+    cudaDeviceReset) holds its own copy of the scratch array at another address.  The
+    entry point looks the address up in the current context on every call, so a call made
+    in the new context gives the same result as one made in the first.  Runs in a fresh
+    process of its own."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _SECOND_CONTEXT, root], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "second context ok" in r.stdout
