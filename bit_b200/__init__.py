@@ -144,6 +144,8 @@ SIGNATURES = [
     ("bit_ctx_last_error", C.c_char_p, [_vp]),
     ("bit_ctx_synchronize", C.c_int, [_vp]),
     ("bit_ctx_set_group_size", C.c_int, [_vp, C.c_int]),
+    ("bit_ctx_set_work_queue", C.c_int, [_vp, C.c_int]),
+    ("bit_ctx_set_near_config", C.c_int, [_vp, C.c_int, C.c_int]),
     ("bit_ctx_stream", C.c_int, [_vp, C.POINTER(_vp)]),
     ("bit_ctx_memory", C.c_int, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("bit_tree_build", C.c_int, [_vp, C.c_int, _dp, _dp, _dp, C.c_int, C.POINTER(_vp)]),
@@ -316,6 +318,16 @@ class Context:
     def set_group_size(self, targets):
         """Leaf packing (0: off, else 32..1024 targets per group): a tuning knob."""
         self.check(lib().bit_ctx_set_group_size(self.h, targets), "bit_ctx_set_group_size")
+
+    def set_near_config(self, tile=0, threads_per_target=0):
+        """Near-field source tile and threads-per-target cap (0, 0: the defaults)."""
+        self.check(lib().bit_ctx_set_near_config(self.h, tile, threads_per_target),
+                   "bit_ctx_set_near_config")
+
+    def set_work_queue(self, on):
+        """Forests: one persistent kernel per field over a device work queue (True, the
+        default) or one launch per (nterms, kernel) class (False)."""
+        self.check(lib().bit_ctx_set_work_queue(self.h, int(bool(on))), "bit_ctx_set_work_queue")
 
     def synchronize(self):
         self.check(lib().bit_ctx_synchronize(self.h), "synchronize")

@@ -176,8 +176,10 @@ void eval_particles_sorted(Tree* t, const std::vector<bit_eval_params>& prm) {
   t->stats.far_entries = t->plists.nfar;
   t->stats.near_entries = t->plists.nnear;
   t->stats.batches = t->plists.ngroups;
-  t->stats.far_launches = (int)t->pplan.far_classes.size();
-  t->stats.near_launches = (int)t->pplan.near_classes.size();
+  // several classes run as one work-queue launch each when the context allows it
+  const int nfc = (int)t->pplan.far_classes.size(), nnc = (int)t->pplan.near_classes.size();
+  t->stats.far_launches = (t->ctx->work_queue && nfc > 1) ? 1 : nfc;
+  t->stats.near_launches = (t->ctx->work_queue && nnc > 1) ? 1 : nnc;
   t->stats.list_fallback = t->plists.fallback ? 1 : 0;
   t->stats.lists_shared = t->plists.shared ? 1 : 0;
 }
@@ -287,6 +289,22 @@ const char* bit_ctx_last_error(const bit_ctx* h) { return h ? h->c.last_error.c_
 bit_status bit_ctx_set_group_size(bit_ctx* h, int targets) {
   if (!h || (targets != 0 && (targets < 32 || targets > kGroupMax))) return BIT_ERR_INVALID_ARGUMENT;
   h->c.group_targets = targets;
+  return BIT_OK;
+}
+
+bit_status bit_ctx_set_near_config(bit_ctx* h, int tile, int threads_per_target) {
+  if (!h) return BIT_ERR_INVALID_ARGUMENT;
+  if (tile != 0 && (tile < 128 || tile > 2048 || (tile & (tile - 1)))) return BIT_ERR_INVALID_ARGUMENT;
+  const int s = threads_per_target;
+  if (s != 0 && (s < 1 || s > 32 || (s & (s - 1)))) return BIT_ERR_INVALID_ARGUMENT;
+  h->c.near_tile = tile;
+  h->c.near_split = s;
+  return BIT_OK;
+}
+
+bit_status bit_ctx_set_work_queue(bit_ctx* h, int on) {
+  if (!h || (on != 0 && on != 1)) return BIT_ERR_INVALID_ARGUMENT;
+  h->c.work_queue = on;
   return BIT_OK;
 }
 

@@ -178,6 +178,13 @@ struct Ctx {
   std::string last_error;
   int num_sms = 148;
   int group_targets = 0;  // leaves packed into groups of up to this many targets (0: off)
+  // Plans with several launch classes (forests): 1 runs each field as one persistent
+  // kernel over a device work queue of all groups, 0 as one launch per class.
+  int work_queue = 1;
+  DBuf<int> queue_heads;  // the work queues' counters (far, near)
+  // near-field tuning knobs (bit_ctx_set_near_config): source records per tile and the cap
+  // on threads per target (0: the defaults)
+  int near_tile = 0, near_split = 0;
   ListKey mac_hint;       // MAC of the last particle-target evaluation (acc < 0: none)
   // small device scratch for flags / counters
   DBuf<long long> scratch_ll;

@@ -9,6 +9,8 @@
 // shared-memory row; rows are summed in warp order at the end, so the result does not
 // depend on timing.  The target-centre offset is formed in FP64; the mixed path rounds it
 // once to FP32 and runs recurrence and dot product in FP32, accumulating with two-sum.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace bit {
@@ -111,8 +113,12 @@ constexpr size_t far_smem(size_t acc_bytes_per_row_target, size_t moment_bytes) 
 constexpr int NWP = 8;  // warps per CTA, potential
 constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
 
+// The far field of one target group g (the CTA's whole work for that group).  Shared
+// memory: the group's target coordinates, per warp a packed target list, an accumulator row
+// and one cluster's moments (NW * TP of them; a kernel running several orders sizes this for
+// the largest).
 template <int NT, int KER, class T>
-__global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArgs a) {
+__device__ __forceinline__ void far_group(const FarArgs& a, int g) {
   constexpr int TT = num_terms(NT);
   constexpr int TP = FarField<NT>::kPadded;
   constexpr int NW = NWP;
@@ -125,7 +131,6 @@ __global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArg
   constexpr int ROW = WarpAcc<T>::words * kGroupMax;
   T* msb = accb + NW * ROW;  // one cluster's moments per warp
 
-  const int g = a.order[blockIdx.x];
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int W = (tc + 31) >> 5;
   const long long e0 = a.off[g], e1 = e0 + a.cnt[g], m0 = a.moff[g];
@@ -173,6 +178,45 @@ __global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArg
     double s = 0.0;
     for (int q = 0; q < NW; q++) s += WarpAcc<T>::get(accb + q * ROW, i);
     a.out[t0 + i] = sign * s;
+  }
+}
+
+// One launch class: CTA b takes group order[b].
+template <int NT, int KER, class T>
+__global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArgs a) {
+  far_group<NT, KER, T>(a, a.order[blockIdx.x]);
+}
+
+// Persistent work queue over the groups of every class: each CTA takes the next item
+// (a group, in the given order) from a device counter until none is left, and runs the
+// far field of that group's system (its nterms and kernel) -- the same device code, in the
+// same order within the group, as k_far, so the results are identical.  No CTA waits for
+// another; the counter is the only shared state.
+template <class T>
+__global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1)
+    k_far_queue(FarArgs a, int count, int* head) {
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(head, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();  // every thread has read s_item before it is overwritten
+    if (item >= count) return;
+    const int g = a.order[item];
+    const SysEval* se = a.sys + a.g_sys[g];
+    const bool coul = se->kernel == BIT_KERNEL_COULOMB;
+    switch (se->nterms) {
+#define FQ(N)                                                           \
+  case N:                                                               \
+    if (coul) far_group<N, BIT_KERNEL_COULOMB, T>(a, g);                \
+    else far_group<N, BIT_KERNEL_SCREENED, T>(a, g);                    \
+    break;
+      FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10)
+#undef FQ
+      default:
+        break;
+    }
+    __syncthreads();  // the group's last reads of shared memory precede the next group's writes
   }
 }
 
@@ -300,12 +344,53 @@ FarArgs far_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const d
 }  // namespace
 
 // One launch per (nterms, kernel) class, each over its groups (P.far_ord + begin).
+template <class T>
+void launch_far_queue(Ctx* c, const FarArgs& a, int count, int max_nterms, int* head,
+                      cudaStream_t s) {
+  int tp = 0;
+  switch (max_nterms) {
+#define TPN(N) case N: tp = FarField<N>::kPadded; break;
+    TPN(1) TPN(2) TPN(3) TPN(4) TPN(5) TPN(6) TPN(7) TPN(8) TPN(9) TPN(10)
+#undef TPN
+    default: fail(BIT_ERR_STATE, "moments not computed");
+  }
+  const size_t bytes = far_smem<NWP>(WarpAcc<T>::words * sizeof(T), tp * sizeof(T));
+  set_smem(k_far_queue<T>, bytes);
+  int per_sm = 0;
+  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_far_queue<T>, 32 * NWP, bytes));
+  const int grid = std::max(1, std::min(count, c->num_sms * std::max(per_sm, 1)));
+  count_launch(), k_far_queue<T><<<grid, 32 * NWP, bytes, s>>>(a, count, head);
+}
+
+// The work-queue form is used for plans of several classes when the context allows it;
+// the queue takes every group in decreasing-work order (L->order).
+bool use_queue(const Ctx* c, const std::vector<LaunchClass>& classes) {
+  return c->work_queue && classes.size() > 1;
+}
+
+int* queue_head(Ctx* c, int which, cudaStream_t s) {
+  c->queue_heads.ensure(c, 2);
+  BIT_CUDA(cudaMemsetAsync(c->queue_heads.p + which, 0, sizeof(int), s));
+  return c->queue_heads.p + which;
+}
+
 void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const double* ty,
               const double* tz, double* out) {
   FarArgs a = far_args(t, L, P, tx, ty, tz);
   a.out = out;
   cudaStream_t s = t->ctx->stream;
   const bool f32 = P.f32;
+  if (use_queue(t->ctx, P.far_classes)) {
+    int nt_max = 0, count = 0;
+    for (const LaunchClass& k : P.far_classes) nt_max = std::max(nt_max, k.nterms);
+    for (const LaunchClass& k : P.far_classes) count += k.count;
+    a.order = L->order.p;
+    int* head = queue_head(t->ctx, 0, s);
+    if (f32) launch_far_queue<float>(t->ctx, a, count, nt_max, head, s);
+    else launch_far_queue<double>(t->ctx, a, count, nt_max, head, s);
+    BIT_CHECK_LAUNCH();
+    return;
+  }
   for (const LaunchClass& k : P.far_classes) {
     a.order = P.far_ord + k.begin;
     const int ng = k.count;

@@ -2,14 +2,15 @@
 //
 // bit_bie_solve: restarted GMRES(m) for (diag*I + K) s = f where K is the treecode with
 // charges w*s (no reference counterpart: the reference's solver::gmres takes a dense
-// matrix, src/solver.h:157-260); every matvec after the first of each precision replays a
-// CUDA graph.  Vectors live in tree order on the device; each matvec
+// matrix, src/solver.h:157-260).  Vectors live in tree order on the device; each matvec
 // rewrites the charges, recomputes the moments (FP64) and runs the far and near kernels
-// over the interaction lists built once for the tree.  Arnoldi is classical Gram-Schmidt
-// applied twice (FP64 dot products and updates on the device); the (m+1) x m Hessenberg
-// and its Givens rotations are FP64 on the host.  Mixed precision: FP32 matvecs inside an
-// FP64 iterative refinement whose residual f - A s is always recomputed with the FP64
-// treecode.
+// over the interaction lists built once for the tree.  A whole GMRES iteration runs on the
+// device -- the matvec, classical Gram-Schmidt applied twice (FP64), the normalisation and
+// the FP64 Givens rotation of the new Hessenberg column -- and every iteration after the
+// first of each precision replays it as one CUDA graph; the host reads back the residual
+// estimate once per iteration and solves the small triangular system once per cycle.
+// Mixed precision: FP32 matvecs inside an FP64 iterative refinement whose residual
+// f - A s is always recomputed with the FP64 treecode (those matvecs replay a graph too).
 //
 // bit_gmres_dense: solver::gmres itself (src/solver.h:157-310) for a dense matrix:
 // full GMRES from zero, modified Gram-Schmidt, least squares by Gram-Schmidt QR of the
@@ -109,6 +110,110 @@ __global__ void k_combine(int n, int k, const double* V, const double* y, double
   double a = x[i];
   for (int j = 0; j < k; j++) a += y[j] * V[(long long)j * n + i];
   x[i] = a;
+}
+
+// ---- one GMRES(m) iteration on the device ------------------------------------------------
+// Every kernel below reads the iteration's column k from device memory (*dk), and
+// k_givens advances it, so the same launch sequence -- and one CUDA graph of it -- serves
+// every iteration of a cycle.  The arithmetic is the host loop's: classical Gram-Schmidt
+// applied twice, normalisation, the previous Givens rotations applied to the new column, a
+// new rotation, and the rotated right-hand side g whose last entry is the residual norm.
+
+// x = V[k]
+__global__ void k_basis_in(int n, const double* V, const int* dk, double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = V[(long long)(*dk) * n + i];
+}
+// V[k + 1] = y
+__global__ void k_basis_out(int n, const double* y, double* V, const int* dk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) V[(long long)(*dk + 1) * n + i] = y[i];
+}
+// partial[j * nblk + b] = block b's share of V[j] . V[k + 1], j <= k
+__global__ void k_dots_k(int n, const double* V, const int* dk, double* partial) {
+  const int k = *dk + 1;
+  const double* w = V + (long long)k * n;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  for (int j = 0; j < k; j++) {
+    double a = 0.0;
+    const double* v = V + (long long)j * n;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) a += v[i] * w[i];
+    a = block_sum(a);
+    if (threadIdx.x == 0) partial[j * gridDim.x + blockIdx.x] = a;
+  }
+}
+// htmp[j] = V[j] . V[k + 1] (this pass), hcol[j] += htmp[j]
+__global__ void k_dots_k_finish(int nblk, const double* partial, const int* dk, double* htmp,
+                                double* hcol) {
+  const int j = blockIdx.x;
+  if (j > *dk) return;
+  double a = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) a += partial[j * nblk + b];
+  a = block_sum(a);
+  if (threadIdx.x == 0) {
+    htmp[j] = a;
+    hcol[j] += a;
+  }
+}
+// V[k + 1] -= sum_{j <= k} htmp[j] V[j]
+__global__ void k_orth_k(int n, const double* V, const int* dk, const double* htmp, double* Vw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = *dk;
+  double* w = Vw + (long long)(k + 1) * n;
+  double a = w[i];
+  for (int j = 0; j <= k; j++) a -= htmp[j] * V[(long long)j * n + i];
+  w[i] = a;
+}
+// partial[b] = block b's share of |V[k + 1]|^2
+__global__ void k_sqnorm_k(int n, const double* V, const int* dk, double* partial) {
+  const double* w = V + (long long)(*dk + 1) * n;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  double a = 0.0;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) a += w[i] * w[i];
+  a = block_sum(a);
+  if (threadIdx.x == 0) partial[blockIdx.x] = a;
+}
+// scal[0] = |V[k + 1]|
+__global__ void k_norm_finish(int nblk, const double* partial, double* scal) {
+  double a = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) a += partial[b];
+  a = block_sum(a);
+  if (threadIdx.x == 0) scal[0] = sqrt(a);
+}
+// V[k + 1] /= |V[k + 1]| (left as it is when the norm is 0)
+__global__ void k_scale_k(int n, double* V, const int* dk, const double* scal) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double hn = scal[0];
+  if (i >= n || !(hn > 0)) return;
+  double* w = V + (long long)(*dk + 1) * n;
+  w[i] = (1.0 / hn) * w[i];
+}
+// One thread: the rotations of column k (H ld m), scal[1] = |g[k + 1]|, the column
+// cleared for the next iteration, k advanced.
+__global__ void k_givens(int m, int* dk, double* H, double* cs, double* sn, double* g,
+                         double* hcol, double* scal) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int k = *dk;
+  hcol[k + 1] = scal[0];
+  for (int j = 0; j < k; j++) {
+    const double a = hcol[j], b = hcol[j + 1];
+    hcol[j] = cs[j] * a + sn[j] * b;
+    hcol[j + 1] = -sn[j] * a + cs[j] * b;
+  }
+  const double den = hypot(hcol[k], hcol[k + 1]);
+  cs[k] = den > 0 ? hcol[k] / den : 1.0;
+  sn[k] = den > 0 ? hcol[k + 1] / den : 0.0;
+  hcol[k] = den;
+  hcol[k + 1] = 0.0;
+  for (int j = 0; j <= k; j++) H[(long long)j * m + k] = hcol[j];
+  g[k + 1] = -sn[k] * g[k];
+  g[k] = cs[k] * g[k];
+  scal[1] = fabs(g[k + 1]);
+  for (int j = 0; j <= k + 1; j++) hcol[j] = 0.0;
+  *dk = k + 1;
 }
 
 struct Krylov {
@@ -242,73 +347,166 @@ struct BieOp {
 // Restarted GMRES(m) on A x = b from x (device, tree order) with matvecs in `prec`; stops
 // when the recurrence residual reaches tol*||b|| or after maxit iterations.  Returns the
 // iterations used.
-int gmres_m(BieOp& A, Krylov& K, const double* b, double* x, int m, double tol, int maxit,
-            bit_precision prec, double bnorm, bool x_is_zero) {
+// Device state of GMRES(m) for one solve: the Krylov basis and the Arnoldi / Givens
+// arrays, on fixed buffers so that one CUDA graph per precision holds a whole iteration
+// (the matvec of BieOp on its fixed input / output, the two Gram-Schmidt passes, the
+// normalisation and the rotation) and is replayed by every iteration of every cycle.  It
+// is captured on a precision's second iteration, after the first (eager) one has made
+// every allocation and plan; capture failures fall back to eager launches.
+struct GmresState {
+  Ctx* c;
+  int n, m, nblk;
+  DBuf<double> V, w, H, cs, sn, g, hcol, htmp, scal, partial;
+  DBuf<int> dk;
+  double* hpin = nullptr;  // pinned: scal[0..1] read back each iteration
+  cudaGraphExec_t iexec[2] = {nullptr, nullptr};
+  long long ilaunches[2] = {0, 0};
+  int eager[2] = {0, 0};
+  bool graphs = true;
+  GmresState(Ctx* ctx, int n_, int m_) : c(ctx), n(n_), m(m_) {
+    nblk = std::min(2 * c->num_sms, std::max(1, n / 2048));
+    V.ensure(c, (size_t)(m + 1) * n);
+    w.ensure(c, n);
+    H.ensure(c, (size_t)(m + 1) * m);
+    cs.ensure(c, m); sn.ensure(c, m); g.ensure(c, m + 1);
+    hcol.ensure(c, m + 2); htmp.ensure(c, m + 2); scal.ensure(c, 4);
+    partial.ensure(c, (size_t)nblk * (m + 2));
+    dk.ensure(c, 1);
+    BIT_CUDA(cudaMallocHost(&hpin, 4 * sizeof(double)));
+  }
+  ~GmresState() {
+    for (auto& g_ : iexec)
+      if (g_) cudaGraphExecDestroy(g_);
+    if (hpin) cudaFreeHost(hpin);
+  }
+
+  // One iteration on column *dk (eager launches).
+  void step_eager(BieOp& A, bit_precision prec) {
+    cudaStream_t s = c->stream;
+    A.gin.ensure(c, n);
+    A.gout.ensure(c, n);
+    count_launch(), k_basis_in<<<grid_for(n, 256), 256, 0, s>>>(n, V.p, dk.p, A.gin.p);
+    A.apply_eager(A.gin.p, A.gout.p, prec);
+    count_launch(), k_basis_out<<<grid_for(n, 256), 256, 0, s>>>(n, A.gout.p, V.p, dk.p);
+    for (int pass = 0; pass < 2; pass++) {
+      count_launch(), k_dots_k<<<nblk, RB, 0, s>>>(n, V.p, dk.p, partial.p);
+      count_launch(), k_dots_k_finish<<<m + 1, RB, 0, s>>>(nblk, partial.p, dk.p, htmp.p, hcol.p);
+      count_launch(), k_orth_k<<<grid_for(n, 256), 256, 0, s>>>(n, V.p, dk.p, htmp.p, V.p);
+    }
+    count_launch(), k_sqnorm_k<<<nblk, RB, 0, s>>>(n, V.p, dk.p, partial.p);
+    count_launch(), k_norm_finish<<<1, RB, 0, s>>>(nblk, partial.p, scal.p);
+    count_launch(), k_scale_k<<<grid_for(n, 256), 256, 0, s>>>(n, V.p, dk.p, scal.p);
+    count_launch(), k_givens<<<1, 32, 0, s>>>(m, dk.p, H.p, cs.p, sn.p, g.p, hcol.p, scal.p);
+    BIT_CHECK_LAUNCH();
+  }
+
+  bool capture(BieOp& A, int pi, bit_precision prec) {
+    cudaStream_t s = c->stream;
+    cudaGraph_t gr = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    const long long l0 = launch_counter().load();
+    bool ok = true;
+    try {
+      step_eager(A, prec);
+    } catch (const Error&) {
+      ok = false;
+    }
+    const long long kernels = launch_counter().load() - l0;
+    launch_counter().fetch_sub(kernels);  // counted while capturing, but nothing ran
+    const cudaError_t e = cudaStreamEndCapture(s, &gr);
+    if (!ok || e != cudaSuccess || !gr) {
+      cudaGetLastError();
+      if (gr) cudaGraphDestroy(gr);
+      return false;
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&iexec[pi], gr, 0);
+    cudaGraphDestroy(gr);
+    if (ie != cudaSuccess) {
+      cudaGetLastError();
+      iexec[pi] = nullptr;
+      return false;
+    }
+    ilaunches[pi] = kernels;
+    return true;
+  }
+
+  // One iteration (graph replay when available); returns (|v|, |g[k+1]|) read back.
+  void step(BieOp& A, bit_precision prec, double& hn, double& res) {
+    const int pi = prec == BIT_PREC_MIXED ? 1 : 0;
+    (prec == BIT_PREC_FP64 ? A.mv64 : A.mv32)++;
+    cudaStream_t s = c->stream;
+    if (graphs && !iexec[pi] && eager[pi] >= 1 && !capture(A, pi, prec)) graphs = false;
+    if (graphs && iexec[pi]) {
+      BIT_CUDA(cudaGraphLaunch(iexec[pi], s));
+      launch_counter().fetch_add(ilaunches[pi]);
+    } else {
+      eager[pi]++;
+      step_eager(A, prec);
+    }
+    BIT_CUDA(cudaMemcpyAsync(hpin, scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    hn = hpin[0];
+    res = hpin[1];
+  }
+};
+
+// Restarted GMRES(m) on A x = b from x (device, tree order) with matvecs in `prec`; stops
+// when the recurrence residual reaches tol*||b|| or after maxit iterations.  Returns the
+// iterations used.  Each iteration runs on the device (GmresState); the host reads two
+// numbers per iteration and solves the small triangular system once per cycle.
+int gmres_m(BieOp& A, Krylov& K, GmresState& G, const double* b, double* x, int m, double tol,
+            int maxit, bit_precision prec, double bnorm, bool x_is_zero) {
   Ctx* c = A.t->ctx;
   cudaStream_t s = c->stream;
   const int n = A.t->n;
-  DBuf<double> V, w;
-  V.ensure(c, (size_t)(m + 1) * n);
-  w.ensure(c, n);
-  std::vector<double> H((m + 1) * m), cs(m), sn(m), g(m + 1), y(m), hcol(m + 1);
+  double* w = G.w.p;
+  std::vector<double> H((size_t)(m + 1) * m), g(m + 1), y(m);
   int it = 0;
   while (it < maxit) {
     // r = b - A x
     if (x_is_zero) {
-      BIT_CUDA(cudaMemcpyAsync(w.p, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      BIT_CUDA(cudaMemcpyAsync(w, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
     } else {
-      A.apply(x, w.p, prec);
-      count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, b, -1.0, w.p);
+      A.apply(x, w, prec);
+      count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, b, -1.0, w);
     }
     x_is_zero = false;
-    double beta = K.norm(w.p);
+    double beta = K.norm(w);
     if (beta <= tol * bnorm || beta == 0.0) break;
-    count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0 / beta, w.p, 0.0, V.p);
+    count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0 / beta, w, 0.0, G.V.p);
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
+    BIT_CUDA(cudaMemcpyAsync(G.g.p, g.data(), (m + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemsetAsync(G.hcol.p, 0, (m + 2) * sizeof(double), s));
+    BIT_CUDA(cudaMemsetAsync(G.dk.p, 0, sizeof(int), s));
     int k = 0;
     bool done = false;
     for (; k < m && it < maxit; k++) {
       it++;
-      double* vk1 = V.p + (long long)(k + 1) * n;
-      A.apply(V.p + (long long)k * n, vk1, prec);
-      // classical Gram-Schmidt, twice
-      std::fill(hcol.begin(), hcol.end(), 0.0);
-      for (int pass = 0; pass < 2; pass++) {
-        K.dots(V.p, k + 1, vk1);
-        for (int j = 0; j <= k; j++) hcol[j] += K.hh[j];
-        count_launch(), k_orth_update<<<grid_for(n, 256), 256, 0, s>>>(n, k + 1, V.p, K.hdev.p, vk1);
-      }
-      double hn = K.norm(vk1);
-      hcol[k + 1] = hn;
-      if (hn > 0) count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0 / hn, vk1, 0.0, vk1);
-      for (int j = 0; j < k; j++) {
-        double a = hcol[j], bb = hcol[j + 1];
-        hcol[j] = cs[j] * a + sn[j] * bb;
-        hcol[j + 1] = -sn[j] * a + cs[j] * bb;
-      }
-      double den = std::hypot(hcol[k], hcol[k + 1]);
-      cs[k] = den > 0 ? hcol[k] / den : 1.0;
-      sn[k] = den > 0 ? hcol[k + 1] / den : 0.0;
-      hcol[k] = den;
-      hcol[k + 1] = 0.0;
-      for (int j = 0; j <= k; j++) H[j * m + k] = hcol[j];
-      g[k + 1] = -sn[k] * g[k];
-      g[k] = cs[k] * g[k];
-      if (std::fabs(g[k + 1]) <= tol * bnorm || hn == 0.0) {
+      double hn = 0.0, res = 0.0;
+      G.step(A, prec, hn, res);
+      if (res <= tol * bnorm || hn == 0.0) {
         k++;
         done = true;
         break;
       }
     }
+    // y = R^-1 g on the host (k x k upper triangle of the rotated Hessenberg)
+    BIT_CUDA(cudaMemcpyAsync(H.data(), G.H.p, (size_t)k * m * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(g.data(), G.g.p, k * sizeof(double), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
     for (int i = k - 1; i >= 0; i--) {
       double a = g[i];
-      for (int j = i + 1; j < k; j++) a -= H[i * m + j] * y[j];
-      y[i] = a / H[i * m + i];
+      for (int j = i + 1; j < k; j++) a -= H[(size_t)i * m + j] * y[j];
+      y[i] = a / H[(size_t)i * m + i];
     }
     BIT_CUDA(cudaMemcpyAsync(K.hdev.p, y.data(), k * sizeof(double), cudaMemcpyHostToDevice, s));
-    count_launch(), k_combine<<<grid_for(n, 256), 256, 0, s>>>(n, k, V.p, K.hdev.p, x);
+    count_launch(), k_combine<<<grid_for(n, 256), 256, 0, s>>>(n, k, G.V.p, K.hdev.p, x);
     BIT_CHECK_LAUNCH();
+    BIT_CUDA(cudaStreamSynchronize(s));  // y (pageable host memory) has been read
     if (done) break;
   }
   BIT_CUDA(cudaStreamSynchronize(s));
@@ -432,13 +630,14 @@ extern "C" bit_status bit_bie_solve(bit_tree* th, const bit_eval_params* prm, in
       tree_set_charges(t, tmp.p, nullptr);
     }
     Krylov K(c, n, opts->restart + 1);
+    GmresState G(c, n, opts->restart);
     const double bnorm = K.norm(b.p);
     int iters = 0, refine = 0;
     double relres = 0.0;
     if (bnorm == 0.0) {
       relres = 0.0;
     } else if (opts->precision == BIT_PREC_FP64) {
-      iters = gmres_m(A, K, b.p, x.p, opts->restart, opts->tol, opts->maxit, BIT_PREC_FP64,
+      iters = gmres_m(A, K, G, b.p, x.p, opts->restart, opts->tol, opts->maxit, BIT_PREC_FP64,
                       bnorm, true);
       A.apply(x.p, r.p, BIT_PREC_FP64);
       count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, b.p, -1.0, r.p);
@@ -452,7 +651,7 @@ extern "C" bit_status bit_bie_solve(bit_tree* th, const bit_eval_params* prm, in
         // inner: A32 d = r to itol relative to ||r||
         const double rn = K.norm(r.p);
         BIT_CUDA(cudaMemsetAsync(d.p, 0, n * sizeof(double), s));
-        iters += gmres_m(A, K, r.p, d.p, opts->restart, itol, opts->maxit - iters,
+        iters += gmres_m(A, K, G, r.p, d.p, opts->restart, itol, opts->maxit - iters,
                          BIT_PREC_MIXED, rn, true);
         count_launch(), k_axpby<<<grid_for(n, 256), 256, 0, s>>>(n, 1.0, d.p, 1.0, x.p);
         refine++;

@@ -15,6 +15,7 @@
 // rsqrt / ex2, and per-target compensated (two-sum) accumulation; pairs too close for FP32
 // coordinates are summed in FP64 (below).  The self pair is skipped by splitting each
 // lane's index range around it.
+#include <algorithm>
 #include <climits>
 
 #include "common.cuh"
@@ -48,6 +49,8 @@ struct NearArgs {
   int2* crec;   // up to kCloseRec (near entry, first source of the tile) per target
   int2* clist;  // (target, group) of every target with a record
   int* cn;      // entries of clist
+  int tile;     // sources per tile (Prec<>::TILE_MIN..TILE_MAX)
+  int split;    // threads per target: 0 the precision's rule, else at most this many
 };
 
 constexpr int kCloseRec = 2;  // record slots per target; beyond them k_close scans them all
@@ -62,6 +65,29 @@ __device__ __forceinline__ float ex2_approx(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+// 2^x for x <= 0 on the FMA pipe instead of the MUFU: x = n + f with n = round(x) (adding
+// and subtracting 1.5 * 2^23 rounds to the nearest integer, Cody and Waite's reduction)
+// and f in [-1/2, 1/2]; 2^f by the degree-5 polynomial of least maximum relative error on
+// that interval (Remez exchange, coefficients from remez_exp2.py, rounded to float32);
+// 2^n added into the exponent field.  Relative error at most 2.2e-7 for x >= -125 (about
+// that of ex2.approx); x below -125 is taken as -125 (2^-125 ~ 2.4e-38, i.e. 0 here).
+// The screened near field evaluates some of its exponentials this way so that its
+// rsqrt / exp2 work is shared between the MUFU and FMA pipes.
+__device__ __forceinline__ float exp2_fma(float x) {
+  x = fmaxf(x, -125.f);
+  const float big = 12582912.f;  // 1.5 * 2^23
+  const float t = x + big;
+  const float n = t - big;
+  const float f = x - n;
+  float p = fmaf(f, 0x1.5c08e6p-10f, 0x1.3d0c52p-7f);
+  p = fmaf(f, p, 0x1.c6b6e4p-5f);
+  p = fmaf(f, p, 0x1.ebf918p-3f);
+  p = fmaf(f, p, 0x1.62e428p-1f);
+  p = fmaf(f, p, 0x1.000002p+0f);
+  const int e = __float_as_int(t) - __float_as_int(big);  // round(x)
+  return __int_as_float(__float_as_int(p) + (int)((unsigned)e << 23));
+}
+
 // Knuth two-sum: s + e accumulates b with the rounding error of each step kept in e.
 __device__ __forceinline__ void two_sum(float& s, float& e, float b) {
   float t = s + b;
@@ -72,29 +98,33 @@ __device__ __forceinline__ void two_sum(float& s, float& e, float b) {
 
 template <bool F32>
 struct Prec;
+// Source tile (records per TMA copy): the default, and the range a context may choose
+// (bit_ctx_set_near_config); shared memory holds two tiles.
 template <>
 struct Prec<true> {
   using S = float4;
   using T = float;
-  static constexpr int TILE = 1024;
+  static constexpr int TILE = 1024, TILE_MIN = 256, TILE_MAX = 2048;
 };
 template <>
 struct Prec<false> {
   using S = double4;
   using T = double;
-  static constexpr int TILE = 512;
+  static constexpr int TILE = 512, TILE_MIN = 128, TILE_MAX = 1024;
 };
 
-// One pair's contribution in FP64 (the reference's arithmetic).
+// One pair's contribution in FP64: the reference's q / sqrt(r^2) and q e^{-kappa r} / r
+// (src/tree3d.cpp:4765-4769, 3609-3618), with 1/r from one FP64 rsqrt (within an ulp of
+// 1/sqrt) in place of a square root and a division.
 template <int KER, bool EPS>
 __device__ __forceinline__ double pair(double x, double y, double z, double4 s, double del,
                                        double kappa) {
   const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
   const double r2 = dx * dx + dy * dy + dz * dz + del;
   if (EPS && !(r2 > kEpsNear)) return 0.0;
-  if (KER == BIT_KERNEL_COULOMB) return s.w / sqrt(r2);
-  const double r = sqrt(r2);
-  return s.w * exp(-kappa * r) / r;
+  const double ri = rsqrt(r2);
+  if (KER == BIT_KERNEL_COULOMB) return s.w * ri;
+  return s.w * exp(-kappa * (r2 * ri)) * ri;
 }
 // Field of eval_grad_kernel_reg (src/tree3d.cpp:73-97), KERNEL_ORDER = 0:
 // q * (-(x_j - x) / (r * r^2)).
@@ -168,8 +198,9 @@ __device__ __forceinline__ float r2_32(float xt, float yt, float zt, float4 s, f
   return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
 }
 
-// p += q * G(r); CHK: pairs with r^2 < thr are left out and flagged.
-template <int KER, bool CHK>
+// p += q * G(r); CHK: pairs with r^2 < thr are left out and flagged.  FMAEXP: the
+// screened exponential on the FMA pipe (exp2_fma) instead of the MUFU.
+template <int KER, bool CHK, bool FMAEXP = false>
 __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, float del,
                                         float kl2, float thr, float& p, bool& close) {
   float r2 = r2_32(xt, yt, zt, s, del);
@@ -182,15 +213,31 @@ __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, 
   }
   const float ri = rsqrt_approx(r2);
   if (KER == BIT_KERNEL_COULOMB) p = fmaf(q, ri, p);
+  else if (FMAEXP) p = fmaf(q * ri, exp2_fma(r2 * ri * kl2), p);
   else p = fmaf(q * ri, ex2_approx(r2 * ri * kl2), p);
 }
 
-// This lane's pairs j = jb, jb + tpt, ... < je, four independent accumulators.
+// This lane's pairs j = jb, jb + tpt, ... < je, four independent accumulators.  A screened
+// pair costs 2 MUFU operations (rsqrt, exp2; 16 per clock per SM) against about 10 FMA-pipe
+// operations (128 per clock): in runs of 8 pairs, 3 take their exp2 on the FMA pipe
+// (about 9 more FMA-pipe operations each), which balances the two pipes.
 template <int KER, bool CHK>
 __device__ __forceinline__ void sweep_pot(const float4* fs, int j, int je, int tpt, float xt,
                                           float yt, float zt, float del, float kl2, float thr,
                                           float& p0, float& p1, bool& close) {
   float p2 = 0.f, p3 = 0.f;
+  if (KER != BIT_KERNEL_COULOMB) {
+    for (; j + 7 * tpt < je; j += 8 * tpt) {
+      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
+      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + tpt], del, kl2, thr, p1, close);
+      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + 2 * tpt], del, kl2, thr, p2, close);
+      acc_pot<KER, CHK, true>(xt, yt, zt, fs[j + 3 * tpt], del, kl2, thr, p3, close);
+      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + 4 * tpt], del, kl2, thr, p0, close);
+      acc_pot<KER, CHK, true>(xt, yt, zt, fs[j + 5 * tpt], del, kl2, thr, p1, close);
+      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + 6 * tpt], del, kl2, thr, p2, close);
+      acc_pot<KER, CHK, true>(xt, yt, zt, fs[j + 7 * tpt], del, kl2, thr, p3, close);
+    }
+  }
   for (; j + 3 * tpt < je; j += 4 * tpt) {
     acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
     acc_pot<KER, CHK>(xt, yt, zt, fs[j + tpt], del, kl2, thr, p1, close);
@@ -247,16 +294,18 @@ __device__ __forceinline__ void close_force(float xt, float yt, float zt, double
 // shortens each thread's run).  FP32 pairs are cheap enough that the per-unit overhead
 // weighs more: split only until half the threads are busy (measured: the utilisation rule
 // gains 1.5% on 2M clustered screened targets but loses 14% on 82k-node BIE matvecs).
+// cap > 0 (a tuned setting): the utilisation rule over 1..cap threads.
 template <bool CHEAP>
-__device__ __forceinline__ int split_for(int cnt) {
-  if (CHEAP) {
+__device__ __forceinline__ int split_for(int cnt, int cap) {
+  if (CHEAP && cap == 0) {
     int tpt = 1;
     while (tpt < 32 && cnt * tpt * 2 <= NT) tpt <<= 1;
     return tpt;
   }
+  const int maxtp = cap > 0 ? cap : 32;
   int best = 1;
   float bu = 0.f;
-  for (int tp = 1; tp <= 32; tp <<= 1) {
+  for (int tp = 1; tp <= maxtp; tp <<= 1) {
     const int units = cnt * tp;
     const int rounds = (units + NT - 1) / NT;
     const float util = (float)units / (float)(rounds * NT);
@@ -268,45 +317,45 @@ __device__ __forceinline__ int split_for(int cnt) {
   return best;
 }
 
-// Shared-memory layout of one CTA.
+// Shared-memory layout of one CTA: two source tiles of `tile` records, then the
+// accumulators, the self terms, the packed target list and the mbarriers (target
+// coordinates are read through L1).
 template <bool F32, bool FORCE>
 struct Smem {
   using S = typename Prec<F32>::S;
-  static constexpr int TILE = Prec<F32>::TILE;
   static constexpr int NACC = FORCE ? 3 : 1;
-  static constexpr size_t tiles = 2 * TILE * sizeof(S);
-  static constexpr size_t coords = 0;  // target coordinates are read through L1
   // mixed: float hi + lo per target; FP64: one double; force: three doubles
   static constexpr size_t acc = (FORCE ? 3 : 1) * kGroupMax * sizeof(double);
   static constexpr size_t self = kGroupMax * sizeof(double);
   static constexpr size_t list = kGroupMax * sizeof(int);
   static constexpr size_t bars = 64;
-  static constexpr size_t total = tiles + coords + acc + self + list + bars;
+  __host__ __device__ static size_t tiles(int tile) { return 2 * (size_t)tile * sizeof(S); }
+  __host__ __device__ static size_t total(int tile) { return tiles(tile) + acc + self + list + bars; }
 };
 
-// The whole near field of one group.  FORCE: the three field components instead of the
-// potential (Coulomb only).
+// The whole near field of group g, by the whole CTA.  FORCE: the three field components
+// instead of the potential.  Returns false (in every thread) if a bounded wait gave up:
+// the error flag is set, and the CTA has waited, bounded again, for its copies in flight.
 template <int KER, bool EPS, bool F32, bool FORCE>
-__global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a) {
+__device__ __forceinline__ bool near_group(const NearArgs& a, int g) {
   using P = Prec<F32>;
   using S = typename P::S;
   using T = typename P::T;
   using L = Smem<F32, FORCE>;
-  constexpr int TILE = P::TILE;
+  const int TILE = a.tile;
   extern __shared__ __align__(128) unsigned char sm[];
   S* tiles = reinterpret_cast<S*>(sm);
   const double* cx = a.tx + 0;  // group targets, indexed t0 + i below
   const double* cy = a.ty + 0;
   const double* cz = a.tz + 0;
-  double* accd = reinterpret_cast<double*>(sm + L::tiles + L::coords);
+  unsigned char* rest = sm + L::tiles(TILE);
+  double* accd = reinterpret_cast<double*>(rest);
   float* acch = reinterpret_cast<float*>(accd);  // mixed: hi [0,1024), lo [1024,2048)
-  double* selfv = reinterpret_cast<double*>(sm + L::tiles + L::coords + L::acc);
-  int* tl = reinterpret_cast<int*>(sm + L::tiles + L::coords + L::acc + L::self);
-  uint64_t* bar =
-      reinterpret_cast<uint64_t*>(sm + L::tiles + L::coords + L::acc + L::self + L::list);
+  double* selfv = reinterpret_cast<double*>(rest + L::acc);
+  int* tl = reinterpret_cast<int*>(rest + L::acc + L::self);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(rest + L::acc + L::self + L::list);
   __shared__ int s_cnt;
 
-  const int g = a.order[blockIdx.x];
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const SysEval* se = a.sys + a.g_sys[g];
   const double sdel = se->near_del, skappa = se->kappa;
@@ -382,11 +431,12 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
           mbar_wait(&bar[buf], (k >> 1) & 1);
           if (ne < e1) mbar_wait(&bar[buf ^ 1], ((k + 1) >> 1) & 1);
         }
-        return;
+        __syncthreads();
+        return false;
       }
       if (toff == 0) {
         cnt = s_cnt;
-        tpt = split_for<F32 && !FORCE>(cnt);
+        tpt = split_for<F32 && !FORCE>(cnt, a.split);
       }
       const S* ts = tiles + buf * TILE;
       const double4 c = a.nodec[node];
@@ -540,13 +590,63 @@ __global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a
       a.out[t0 + i] += se->near_sign * accd[i] + selfv[i];
     }
   }
+  return true;
+}
+
+// One launch class: CTA b takes group order[b].
+template <int KER, bool EPS, bool F32, bool FORCE>
+__global__ void __launch_bounds__(NT, (F32 && !FORCE) ? 4 : 0) k_near(NearArgs a) {
+  near_group<KER, EPS, F32, FORCE>(a, a.order[blockIdx.x]);
+}
+
+// Persistent work queue over the groups of every class of a potential evaluation: each CTA
+// takes the next item (a group, in the given order) from a device counter until none is
+// left and runs near_group for that group's kernel and eps rule -- the same device code as
+// k_near, so the results are identical.  A CTA whose bounded wait gave up stops taking
+// items (the host reports the error flag).
+template <bool F32>
+__global__ void __launch_bounds__(NT, F32 ? 4 : 0) k_near_queue(NearArgs a, int count, int* head) {
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(head, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();  // every thread has read s_item before it is overwritten
+    if (item >= count) return;
+    const int g = a.order[item];
+    const SysEval* se = a.sys + a.g_sys[g];
+    bool ok;
+    if (se->kernel == BIT_KERNEL_COULOMB) {
+      ok = se->eps_check ? near_group<BIT_KERNEL_COULOMB, true, F32, false>(a, g)
+                         : near_group<BIT_KERNEL_COULOMB, false, F32, false>(a, g);
+    } else {
+      ok = se->eps_check ? near_group<BIT_KERNEL_SCREENED, true, F32, false>(a, g)
+                         : near_group<BIT_KERNEL_SCREENED, false, F32, false>(a, g);
+    }
+    if (!ok) return;
+    __syncthreads();  // the group's last reads of shared memory precede the next group's writes
+  }
 }
 
 template <int KER, bool EPS, bool F32, bool FORCE>
 void launch(const NearArgs& a, int ngroups, cudaStream_t s) {
-  constexpr size_t bytes = Smem<F32, FORCE>::total;
-  ensure_smem_attr(reinterpret_cast<const void*>(k_near<KER, EPS, F32, FORCE>), (int)bytes);
+  const size_t bytes = Smem<F32, FORCE>::total(a.tile);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_near<KER, EPS, F32, FORCE>),
+                   (int)Smem<F32, FORCE>::total(Prec<F32>::TILE_MAX));
   count_launch(), k_near<KER, EPS, F32, FORCE><<<ngroups, NT, bytes, s>>>(a);
+}
+
+template <bool F32>
+void launch_queue(Ctx* c, const NearArgs& a, int count, cudaStream_t s) {
+  const size_t bytes = Smem<F32, false>::total(a.tile);
+  ensure_smem_attr(reinterpret_cast<const void*>(k_near_queue<F32>),
+                   (int)Smem<F32, false>::total(Prec<F32>::TILE_MAX));
+  int per_sm = 0;
+  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_near_queue<F32>, NT, bytes));
+  const int grid = std::max(1, std::min(count, c->num_sms * std::max(per_sm, 1)));
+  c->queue_heads.ensure(c, 2);
+  BIT_CUDA(cudaMemsetAsync(c->queue_heads.p + 1, 0, sizeof(int), s));
+  count_launch(), k_near_queue<F32><<<grid, NT, bytes, s>>>(a, count, c->queue_heads.p + 1);
 }
 
 // FP64 sum of the close pairs that the mixed near kernel left out (FP32 r^2 < thr, the
@@ -578,7 +678,7 @@ __device__ double close_sum(const NearArgs& a, const SysEval* se, int t, int g, 
     for (int k = 0; k < nrec; k++) {
       const int2 r = a.crec[(long long)t * kCloseRec + k];
       const int node = a.node[r.x];
-      tile(node, r.y, min(r.y + Prec<true>::TILE, a.nummemb[node]));
+      tile(node, r.y, min(r.y + a.tile, a.nummemb[node]));
     }
   } else {
     const int i = t - a.g_tstart[g], W = (a.g_tcount[g] + 31) >> 5;
@@ -633,6 +733,12 @@ NearArgs base_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const
   a.sys = P.sys.p;
   a.g_sys = L->g_sys.p;
   a.err = t->ctx->dev_err();
+  // the context's tile, clamped to the precision's range (0: the default)
+  const int want = t->ctx->near_tile;
+  const int lo = P.f32 ? Prec<true>::TILE_MIN : Prec<false>::TILE_MIN;
+  const int hi = P.f32 ? Prec<true>::TILE_MAX : Prec<false>::TILE_MAX;
+  a.tile = want == 0 ? (P.f32 ? Prec<true>::TILE : Prec<false>::TILE) : std::min(hi, std::max(lo, want));
+  a.split = t->ctx->near_split;
   return a;
 }
 
@@ -671,7 +777,17 @@ void eval_near(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const dou
     a.clist = c->close_list.p;
     a.cn = c->close_n.p;
   }
+  // several classes (a forest): one persistent launch over a work queue of all groups
+  if (c->work_queue && P.near_classes.size() > 1) {
+    int count = 0;
+    for (const LaunchClass& k : P.near_classes) count += k.count;
+    a.order = L->order.p;
+    if (f32) launch_queue<true>(c, a, count, s);
+    else launch_queue<false>(c, a, count, s);
+    BIT_CHECK_LAUNCH();
+  }
   for (const LaunchClass& k : P.near_classes) {
+    if (c->work_queue && P.near_classes.size() > 1) break;
     a.order = P.near_ord + k.begin;
     const int ng = k.count;
     const bool scr = k.kernel != BIT_KERNEL_COULOMB;

@@ -3,9 +3,14 @@
 // Callers submit evaluate requests (potential at every particle of a system) and solve
 // requests (the treecode GMRES) of any size at any time.  The server keeps a FIFO of
 // pending requests and `slots` worker threads, each owning a context (its own CUDA stream
-// and device memory).  A request starts as soon as a slot is free and its estimated device
-// memory fits in what the running requests leave of the HBM budget; the head of the queue
-// is never overtaken, so no request starves.  Requests in different slots run on
+// and device memory).  A request starts as soon as a slot is free and its reservation fits
+// in the HBM budget next to everything else the server's contexts hold: the reservations
+// of the running requests and the bytes the idle slots keep (live buffers and cached
+// blocks).  A running request's context may allocate at most its reservation (the larger
+// of its estimate and what its slot already holds), so the device memory of all slots
+// together never exceeds the budget: a request whose estimate proves too small fails with
+// BIT_ERR_BUDGET instead of overrunning it.  The head of the queue is never overtaken, so
+// no request starves.  Requests in different slots run on
 // different streams, so their kernels overlap on the device; a request's tree, moments,
 // interaction lists and Krylov basis stay resident in its slot until it finishes.  Every
 // request records when it was submitted, started and finished (seconds on the server's
@@ -36,6 +41,7 @@ struct Request {
   double diag = 0.0;
   bit_gmres_opts g{};
   size_t est = 0;
+  size_t reservation = 0;  // bytes its slot's context may hold while it runs
   std::vector<double> out;
   bit_request_info info{};
   bool done = false;
@@ -63,6 +69,12 @@ struct bit_server {
   int running = 0, max_running = 0;
   long long next_id = 1, submitted = 0, completed = 0;
   std::vector<bit_ctx*> ctx;
+  // device bytes each idle slot's context holds (live + cached), the cached part, and the
+  // sum over idle slots; squeeze: idle slots are asked to free their cached blocks
+  std::vector<size_t> held, cached;
+  std::vector<char> busy;  // the slot runs a request (its held / cached are not current)
+  size_t idle_held = 0;
+  bool squeeze = false;
   std::deque<std::shared_ptr<bit::Request>> queue;
   std::map<long long, std::shared_ptr<bit::Request>> reqs;
   std::mutex mu;
@@ -96,35 +108,78 @@ struct bit_server {
     r.info.status = st;
   }
 
+  // The head request fits when this slot takes it: everything else held, plus the larger of
+  // its estimate and what this slot already holds (its cached blocks are reused).
+  bool fits(int slot) const {
+    return reserved + idle_held - held[slot] + std::max(queue.front()->est, held[slot]) <= budget;
+  }
+  // It would fit if the idle slots gave back their cached blocks.
+  bool fits_after_squeeze() const {
+    size_t live = 0;
+    for (size_t i = 0; i < held.size(); i++)
+      if (!busy[i]) live += held[i] - cached[i];
+    return reserved + live + queue.front()->est <= budget;
+  }
+
   void worker(int slot) {
     for (;;) {
       std::shared_ptr<bit::Request> r;
       {
         std::unique_lock<std::mutex> lock(mu);
-        // the head of the queue starts when it fits in what the running requests leave
+        // the head of the queue starts when it fits next to everything else held; if it
+        // would fit only after the idle slots free their cached blocks, they free them
         cv_work.wait(lock, [&] {
-          return (stopping && queue.empty()) ||
-                 (!queue.empty() && reserved + queue.front()->est <= budget);
+          if (stopping && queue.empty()) return true;
+          if (queue.empty()) return false;
+          if (fits(slot)) return true;
+          if (!squeeze && fits_after_squeeze()) {
+            squeeze = true;
+            cv_work.notify_all();
+          }
+          return squeeze && cached[slot] > 0;
         });
         if (queue.empty()) return;
+        if (!fits(slot)) {
+          // give this idle slot's cached blocks back, then look again
+          lock.unlock();
+          ctx_trim(&ctx[slot]->c, 0);
+          const size_t h = ctx[slot]->c.in_use + ctx[slot]->c.cached;
+          lock.lock();
+          idle_held = idle_held - held[slot] + h;
+          held[slot] = h;
+          cached[slot] = ctx[slot]->c.cached;
+          cv_work.notify_all();
+          continue;
+        }
+        squeeze = false;
+        busy[slot] = 1;
         r = queue.front();
         queue.pop_front();
-        reserved += r->est;
+        r->reservation = std::max(r->est, held[slot]);
+        r->info.bytes_reserved = r->reservation;
+        idle_held -= held[slot];
+        reserved += r->reservation;
         running++;
-        max_reserved = std::max(max_reserved, reserved);
+        max_reserved = std::max(max_reserved, reserved + idle_held);
         max_running = std::max(max_running, running);
         r->info.t_start = now();
         r->info.slot = slot;
       }
       ctx[slot]->c.peak = ctx[slot]->c.in_use;
+      ctx[slot]->c.budget = r->reservation;  // the context may not allocate beyond it
       run(slot, *r);
       // give back cached blocks above this slot's share of the budget
       ctx_trim(&ctx[slot]->c, budget / nslots);
+      const size_t h = ctx[slot]->c.in_use + ctx[slot]->c.cached;
       {
         std::lock_guard<std::mutex> lock(mu);
         r->info.t_done = now();
         r->done = true;
-        reserved -= r->est;
+        reserved -= r->reservation;
+        held[slot] = h;
+        cached[slot] = ctx[slot]->c.cached;
+        busy[slot] = 0;
+        idle_held += h;
         running--;
         completed++;
       }
@@ -169,6 +224,11 @@ bit_status bit_server_create(bit_server** out, const bit_server_opts* o) {
       return st;
     }
     s->ctx.push_back(c);
+    const size_t h = c->c.in_use + c->c.cached;
+    s->held.push_back(h);
+    s->cached.push_back(c->c.cached);
+    s->busy.push_back(0);
+    s->idle_held += h;
   }
   for (int i = 0; i < slots; i++) s->workers.emplace_back(&bit_server::worker, s, i);
   *out = s;
@@ -277,7 +337,7 @@ bit_status bit_server_stats(bit_server* s, bit_server_info* st) {
   st->running = s->running;
   st->max_running = s->max_running;
   st->budget = s->budget;
-  st->reserved = s->reserved;
+  st->reserved = s->reserved + s->idle_held;
   st->max_reserved = s->max_reserved;
   st->slots = s->nslots;
   st->now = s->now();

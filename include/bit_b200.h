@@ -108,6 +108,16 @@ bit_status bit_ctx_synchronize(bit_ctx* ctx);
  * to that many targets (one traversal, shared source tiles).  Results do not depend on it
  * beyond FP32 summation order. */
 bit_status bit_ctx_set_group_size(bit_ctx* ctx, int targets);
+/* Evaluations whose systems fall into several (nterms, kernel) classes (forests): 1
+ * (default) runs the far field and the near field each as ONE persistent kernel whose CTAs
+ * take (system, target group) items from a device work queue in decreasing-work order;
+ * 0 launches once per class.  Results are identical either way. */
+bit_status bit_ctx_set_work_queue(bit_ctx* ctx, int on);
+/* Near-field tuning knobs (bit_b200.autotune): `tile` source records per TMA tile (a power
+ * of two, 128..2048; clamped to 256..2048 for the mixed path and 128..1024 for FP64; 0: the
+ * default, 1024 mixed / 512 FP64) and the cap on threads that share one target's sources
+ * (a power of two, 1..32; 0: the default rule).  Results change only in FP rounding order. */
+bit_status bit_ctx_set_near_config(bit_ctx* ctx, int tile, int threads_per_target);
 bit_status bit_ctx_stream(const bit_ctx* ctx, void** stream);
 /* Bytes currently allocated by the context and its trees. */
 bit_status bit_ctx_memory(const bit_ctx* ctx, size_t* in_use, size_t* peak);

@@ -397,3 +397,31 @@ def test_lists_not_shared_when_the_macs_decide_differently(ps):
     finally:
         a.close()
         b.close()
+
+
+@pytest.mark.parametrize("tile,split", [(128, 0), (256, 4), (1024, 32), (2048, 1), (512, 8)])
+def test_near_config_keeps_results(orc, tile, split):
+    """The autotuner's near-field knobs (source tile, threads-per-target cap) change only
+    the rounding order: FP64 stays within 1e-12 of the oracle, mixed within 1e-6 of FP64."""
+    import bit_b200 as B
+    from bit_b200 import workloads
+    x, y, z, q = workloads.clustered_blobs(30000, seed=17)
+    T = orc.Tree(x, y, z, 300)
+    T.compute_moments(q, 7)
+    c = B.Context()
+    try:
+        c.set_near_config(tile, split)
+        t = c.treemake(x, y, z, 300)
+        t.treemoments(q, 7)
+        for kern, kw in [(B.COULOMB, dict(del_=1e-4)), (B.SCREENED, dict(kappa=2.0))]:
+            p64 = t.evaluate(B.params(kern, B.CONSISTENT, B.FP64, acc=0.5, **kw))
+            p32 = t.evaluate(B.params(kern, B.CONSISTENT, B.MIXED, acc=0.5, **kw))
+            ref = T.evaluate(orc.params(kern, orc.MODE_CONSISTENT, acc=0.5, **kw))
+            assert rel(p64, ref) < TOL64
+            assert np.linalg.norm(p32 - p64) / np.linalg.norm(p64) < TOL_MIXED
+        t.treeempty()
+        for bad in [(100, 0), (4096, 0), (512, 3), (512, 64)]:
+            with pytest.raises(B.BitError):
+                c.set_near_config(*bad)
+    finally:
+        c.close()

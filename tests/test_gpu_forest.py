@@ -93,7 +93,8 @@ def test_forest_potentials_match_oracle_and_alone(ctx, orc, prec_name, tol):
     prm = [system_params(B, s, prec) for s in range(len(SIZES))]
     got = F.evaluate(prm)
     st = F.stats()
-    assert st["far_launches"] >= 2 and st["near_launches"] >= 2
+    # several (nterms, kernel) classes, each field run as one work-queue launch
+    assert st["far_launches"] == 1 and st["near_launches"] == 1
     for s in range(len(SIZES)):
         mine = F.system(s, got)
         T = orc.Tree(xs[s], ys[s], zs[s], MAXMEMB[s])
@@ -105,6 +106,31 @@ def test_forest_potentials_match_oracle_and_alone(ctx, orc, prec_name, tol):
         alone.treemoments(qs[s], NTERMS[s])
         np.testing.assert_array_equal(mine, alone.evaluate(prm[s]))
         alone.treeempty()
+
+
+@pytest.mark.parametrize("prec_name", ["FP64", "MIXED"])
+def test_work_queue_equals_class_launches(prec_name):
+    """The persistent work-queue kernels (one launch per field over all groups) give the
+    results of one launch per (nterms, kernel) class bit for bit."""
+    import bit_b200 as B
+    prec = getattr(B, prec_name)
+    xs, ys, zs, qs = make_systems(SIZES, 5)
+    c = B.Context()
+    try:
+        F = c.forest(np.concatenate(xs), np.concatenate(ys), np.concatenate(zs), SIZES, MAXMEMB)
+        F.set_charges(np.concatenate(qs))
+        F.moments(NTERMS)
+        prm = [system_params(B, s, prec) for s in range(len(SIZES))]
+        c.set_work_queue(True)
+        q = F.evaluate(prm)
+        assert F.stats()["far_launches"] == 1
+        c.set_work_queue(False)
+        k = F.evaluate(prm)
+        st = F.stats()
+        assert st["far_launches"] >= 2 and st["near_launches"] >= 2
+        np.testing.assert_array_equal(q, k)
+    finally:
+        c.close()
 
 
 def test_forest_one_parameter_set_for_all(ctx):

@@ -127,3 +127,24 @@ def test_submission_from_several_threads():
     srv.close()
     assert sorted(results) == list(range(len(evals)))
     assert all(st == 0 for _, _, st in results.values())
+
+
+def test_memory_held_stays_within_the_budget():
+    """Admission counts what every slot's context really holds (running reservations and
+    idle slots' live and cached blocks), and a running request's context may not allocate
+    beyond its reservation: every request's peak is at most its reservation, the total
+    accounted never exceeds the budget, and no request fails."""
+    import bit_b200 as B
+    evals = eval_requests(B, 12, seed=7)
+    budget = 3 * max(est_eval(len(r[0])) for r in evals)
+    srv = B.Server(slots=4, hbm_budget=budget)
+    ids = [srv.submit_eval(*r) for r in evals]
+    sol = solve_request(B, 4, seed=3)
+    ids.append(srv.submit_solve(*sol))
+    infos = [srv.wait(i) for i in ids]
+    stats = srv.stats()
+    srv.close()
+    for _, info, st in infos:
+        assert st == 0
+        assert info["peak_bytes"] <= info["bytes_reserved"], info
+    assert stats["max_reserved"] <= budget
