@@ -133,14 +133,35 @@ def run_bit(args):
     ctx = B.Context(local, stream=stream.cuda_stream)
     # measured CUDA-core FMA peaks of this device: the roofline denominators
     peaks = {"fp64": ctx.fma_peak(B.FP64) / 1e12, "fp32": ctx.fma_peak(B.MIXED) / 1e12}
+    # the autotuner's near-field (tile, threads-per-target cap) per (precision, kernel) of
+    # this class (p = 8, N0 = 1000, clustered), measured on a 200k-particle sample system
+    near_cfg, tuned = {}, {}
+    if args.tune:
+        from bit_b200 import autotune
+        for prec, pname in ((B.FP64, "fp64"), (B.MIXED, "mixed")):
+            default = (1024 if prec == B.MIXED else 512, 0)
+            for kern, kname, kw in ((B.SCREENED, "screened", dict(kappa=KAPPA)),
+                                    (B.COULOMB, "coulomb", dict(del_=DEL))):
+                best, times = autotune.tune_near(ctx, NTERMS, kern, 200_000, ACC, MAXMEMB,
+                                                 precision=prec, dist="clustered", **kw)
+                near_cfg[(prec, kern)] = best
+                tuned[f"{pname}_{kname}"] = {
+                    "tile": best[0], "threads_per_target": best[1],
+                    "near_speedup_vs_default": times[default] / times[best] if default in times else None}
+        ctx.set_near_config(0, 0)
+
+    def near(prec, kern):
+        ctx.set_near_config(*near_cfg.get((prec, kern), (0, 0)))
 
     def step(prec, keep=False, nterms=NTERMS, maxmemb=MAXMEMB, acc=ACC):
         t = ctx.treemake_device(n, X[0].data_ptr(), X[1].data_ptr(), X[2].data_ptr(), maxmemb)
         t.set_charges_device(X[3].data_ptr())
         t.moments(nterms)
+        near(prec, B.SCREENED)
         t.evaluate_device(B.params(B.SCREENED, B.CONSISTENT, prec, kappa=KAPPA, acc=acc),
                           out_s.data_ptr())
         st_s = t.stats() if keep else None
+        near(prec, B.COULOMB)
         t.evaluate_device(B.params(B.COULOMB, B.CONSISTENT, prec, del_=DEL, acc=acc),
                           out_c.data_ptr())
         st_c = t.stats() if keep else None
@@ -190,7 +211,9 @@ def run_bit(args):
     def e2e_step(prec):
         t = ctx.treemake(x, y, z, MAXMEMB)
         t.treemoments(q, NTERMS)
+        near(prec, B.SCREENED)
         a = t.evaluate(B.params(B.SCREENED, B.CONSISTENT, prec, kappa=KAPPA, acc=ACC), out=host_s)
+        near(prec, B.COULOMB)
         b = t.evaluate(B.params(B.COULOMB, B.CONSISTENT, prec, del_=DEL, acc=ACC), out=host_c)
         t.treeempty()
         return a, b
@@ -244,6 +267,10 @@ def run_bit(args):
                   "e2e_speedup_vs_fp64": e2e64_ms / e2e32_ms,
                   "gpu_launches_per_step": launches[B.MIXED]},
         "fma_peaks_tflops": peaks,
+        "autotune": {"near_config": tuned,
+                     "note": "near-field source tile and threads-per-target cap chosen per "
+                             "(precision, kernel) on a 200k clustered system with N0=1000, "
+                             "p=8, theta=0.7; applied to every step"} if tuned else None,
     }
     # per-phase device times and interaction counts (screened + Coulomb)
     phases = {}
@@ -815,6 +842,8 @@ def main():
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--no-matched", dest="matched", action="store_false",
                     help="skip the accuracy-matched (1e-6 vs direct sum) runs")
+    ap.add_argument("--no-tune", dest="tune", action="store_false",
+                    help="default near-field tile and threads per target instead of tuned ones")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
