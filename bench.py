@@ -46,9 +46,9 @@ FLOPS_NEAR = {"screened": 14, "coulomb": 11}     # per near pair (rsqrt, exp cou
 # Accuracy-matched parameters: (p, theta, N0) at which the plain FP64 treecode reaches 1e-6
 # relative L2 against the FP64 direct sum on these workloads (measured; the run reports
 # the errors it reaches)
-MATCHED_C2 = dict(nterms=10, acc=0.15, maxmemb=1000)
-MATCHED_BIE = dict(nterms=10, acc=0.15, maxmemb=500)
-MATCHED_BATCH_ACC = {5: 0.05, 7: 0.1, 9: 0.15}   # theta by nterms (p = 4, 6, 8)
+MATCHED_C2 = dict(nterms=9, acc=0.15, maxmemb=1000)
+MATCHED_BIE = dict(nterms=9, acc=0.15, maxmemb=500)
+MATCHED_BATCH_ACC = {5: 0.015, 7: 0.05, 9: 0.1}   # theta by nterms (p = 4, 6, 8)
 # DRAM bytes (read + write) per launch of the full-size kernels, from single-kernel ncu
 # captures of the 200k clustered case scaled by the pairs each launch processes; None
 # where no capture of the current kernel exists.
@@ -126,15 +126,20 @@ def run_bit(args):
     n = args.n
     x, y, z, q = workload(n, seed=replicas.system_seed(rank))
     dev = torch.device("cuda", local)
+    # One stream for the library's context and every CUDA event that times it: the events
+    # must be recorded on the stream the kernels run on (torch's default stream would not
+    # order against the context's work).
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     X = torch.tensor(np.stack([x, y, z, q]), dtype=torch.float64, device=dev)
     out_s = torch.empty(n, dtype=torch.float64, device=dev)
     out_c = torch.empty(n, dtype=torch.float64, device=dev)
-    stream = torch.cuda.current_stream(dev)
     ctx = B.Context(local, stream=stream.cuda_stream)
     # measured CUDA-core FMA peaks of this device: the roofline denominators
     peaks = {"fp64": ctx.fma_peak(B.FP64) / 1e12, "fp32": ctx.fma_peak(B.MIXED) / 1e12}
     # the autotuner's near-field (tile, threads-per-target cap) per (precision, kernel) of
-    # this class (p = 8, N0 = 1000, clustered), measured on a 200k-particle sample system
+    # this class (p = 8, N0 = 1000, clustered), measured on a seeded system of the step's
+    # size (a 200k sample chose settings that were slower at 2M)
     near_cfg, tuned = {}, {}
     if args.tune:
         from bit_b200 import autotune
@@ -142,7 +147,7 @@ def run_bit(args):
             default = (1024 if prec == B.MIXED else 512, 0)
             for kern, kname, kw in ((B.SCREENED, "screened", dict(kappa=KAPPA)),
                                     (B.COULOMB, "coulomb", dict(del_=DEL))):
-                best, times = autotune.tune_near(ctx, NTERMS, kern, 200_000, ACC, MAXMEMB,
+                best, times = autotune.tune_near(ctx, NTERMS, kern, n, ACC, MAXMEMB,
                                                  precision=prec, dist="clustered", **kw)
                 near_cfg[(prec, kern)] = best
                 tuned[f"{pname}_{kname}"] = {
@@ -269,7 +274,7 @@ def run_bit(args):
         "fma_peaks_tflops": peaks,
         "autotune": {"near_config": tuned,
                      "note": "near-field source tile and threads-per-target cap chosen per "
-                             "(precision, kernel) on a 200k clustered system with N0=1000, "
+                             "(precision, kernel) on a seeded clustered system of the step's size, N0=1000, "
                              "p=8, theta=0.7; applied to every step"} if tuned else None,
     }
     # per-phase device times and interaction counts (screened + Coulomb)

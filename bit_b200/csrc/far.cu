@@ -154,7 +154,9 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
     T* M = msb + w * TP;
     const T* mn = mom + a.mom_off[node];
     for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
-    // FP32: moments normalised by h^|v|, h = 2^e; the scaled recurrences take h
+    // Both precisions run the scaled form of the reference's recurrence (fewer operations
+    // than the literal one, the same function).  FP32 moments are normalised by h^|v|,
+    // h = 2^e; FP64 moments are the plain ones, i.e. h = 1.
     const T h = sizeof(T) == 4 ? (T)ldexpf(1.f, mom32_scale_exp(c.w)) : T(1);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
@@ -162,13 +164,8 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
       const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
       const T r2 = dx * dx + dy * dy + dz * dz + tadd;
       T v;
-      if constexpr (sizeof(T) == 4) {
-        if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb_s<T>(dx, dy, dz, r2, h, M);
-        else v = FarField<NT>::template screened_s<T>(dx, dy, dz, r2, tk, h, M);
-      } else {
-        if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb<T>(dx, dy, dz, r2, M);
-        else v = FarField<NT>::template screened<T>(dx, dy, dz, r2, tk, M);
-      }
+      if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb_s<T>(dx, dy, dz, r2, h, M);
+      else v = FarField<NT>::template screened_s<T>(dx, dy, dz, r2, tk, h, M);
       WarpAcc<T>::add(row, i, v);
     }
     __syncwarp();

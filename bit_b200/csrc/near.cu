@@ -65,29 +65,6 @@ __device__ __forceinline__ float ex2_approx(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-// 2^x for x <= 0 on the FMA pipe instead of the MUFU: x = n + f with n = round(x) (adding
-// and subtracting 1.5 * 2^23 rounds to the nearest integer, Cody and Waite's reduction)
-// and f in [-1/2, 1/2]; 2^f by the degree-5 polynomial of least maximum relative error on
-// that interval (Remez exchange, coefficients from remez_exp2.py, rounded to float32);
-// 2^n added into the exponent field.  Relative error at most 2.2e-7 for x >= -125 (about
-// that of ex2.approx); x below -125 is taken as -125 (2^-125 ~ 2.4e-38, i.e. 0 here).
-// The screened near field evaluates some of its exponentials this way so that its
-// rsqrt / exp2 work is shared between the MUFU and FMA pipes.
-__device__ __forceinline__ float exp2_fma(float x) {
-  x = fmaxf(x, -125.f);
-  const float big = 12582912.f;  // 1.5 * 2^23
-  const float t = x + big;
-  const float n = t - big;
-  const float f = x - n;
-  float p = fmaf(f, 0x1.5c08e6p-10f, 0x1.3d0c52p-7f);
-  p = fmaf(f, p, 0x1.c6b6e4p-5f);
-  p = fmaf(f, p, 0x1.ebf918p-3f);
-  p = fmaf(f, p, 0x1.62e428p-1f);
-  p = fmaf(f, p, 0x1.000002p+0f);
-  const int e = __float_as_int(t) - __float_as_int(big);  // round(x)
-  return __int_as_float(__float_as_int(p) + (int)((unsigned)e << 23));
-}
-
 // Knuth two-sum: s + e accumulates b with the rounding error of each step kept in e.
 __device__ __forceinline__ void two_sum(float& s, float& e, float b) {
   float t = s + b;
@@ -198,9 +175,8 @@ __device__ __forceinline__ float r2_32(float xt, float yt, float zt, float4 s, f
   return fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, del)));
 }
 
-// p += q * G(r); CHK: pairs with r^2 < thr are left out and flagged.  FMAEXP: the
-// screened exponential on the FMA pipe (exp2_fma) instead of the MUFU.
-template <int KER, bool CHK, bool FMAEXP = false>
+// p += q * G(r); CHK: pairs with r^2 < thr are left out and flagged.
+template <int KER, bool CHK>
 __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, float del,
                                         float kl2, float thr, float& p, bool& close) {
   float r2 = r2_32(xt, yt, zt, s, del);
@@ -213,31 +189,37 @@ __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, 
   }
   const float ri = rsqrt_approx(r2);
   if (KER == BIT_KERNEL_COULOMB) p = fmaf(q, ri, p);
-  else if (FMAEXP) p = fmaf(q * ri, exp2_fma(r2 * ri * kl2), p);
   else p = fmaf(q * ri, ex2_approx(r2 * ri * kl2), p);
 }
 
-// This lane's pairs j = jb, jb + tpt, ... < je, four independent accumulators.  A screened
-// pair costs 2 MUFU operations (rsqrt, exp2; 16 per clock per SM) against about 10 FMA-pipe
-// operations (128 per clock): in runs of 8 pairs, 3 take their exp2 on the FMA pipe
-// (about 9 more FMA-pipe operations each), which balances the two pipes.
+// FP64: this lane's pairs j, j + tpt, ... < je (the target's own source excluded by the
+// caller's split of the range), four independent accumulators so that consecutive pairs
+// do not wait on one another's additions.
+template <int KER, bool EPS>
+__device__ __forceinline__ void sweep_pot64(const double4* ds, int j, int je, int tpt, double x,
+                                            double y, double z, double del, double kappa,
+                                            double& p0, double& p1) {
+  double p2 = 0.0, p3 = 0.0;
+  for (; j + 3 * tpt < je; j += 4 * tpt) {
+    p0 += pair<KER, EPS>(x, y, z, ds[j], del, kappa);
+    p1 += pair<KER, EPS>(x, y, z, ds[j + tpt], del, kappa);
+    p2 += pair<KER, EPS>(x, y, z, ds[j + 2 * tpt], del, kappa);
+    p3 += pair<KER, EPS>(x, y, z, ds[j + 3 * tpt], del, kappa);
+  }
+  for (; j < je; j += tpt) p0 += pair<KER, EPS>(x, y, z, ds[j], del, kappa);
+  p0 += p2;
+  p1 += p3;
+}
+
+// This lane's pairs j = jb, jb + tpt, ... < je, four independent accumulators.  Both
+// exponentials and reciprocal square roots stay on the MUFU: moving 1, 2 or 3 of every 8
+// screened exponentials to the FMA pipe (a Cody-Waite / minimax exp2) measured 3-12%
+// slower at 2M, since this loop is bound by latency and issue, not by MUFU throughput.
 template <int KER, bool CHK>
 __device__ __forceinline__ void sweep_pot(const float4* fs, int j, int je, int tpt, float xt,
                                           float yt, float zt, float del, float kl2, float thr,
                                           float& p0, float& p1, bool& close) {
   float p2 = 0.f, p3 = 0.f;
-  if (KER != BIT_KERNEL_COULOMB) {
-    for (; j + 7 * tpt < je; j += 8 * tpt) {
-      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
-      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + tpt], del, kl2, thr, p1, close);
-      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + 2 * tpt], del, kl2, thr, p2, close);
-      acc_pot<KER, CHK, true>(xt, yt, zt, fs[j + 3 * tpt], del, kl2, thr, p3, close);
-      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + 4 * tpt], del, kl2, thr, p0, close);
-      acc_pot<KER, CHK, true>(xt, yt, zt, fs[j + 5 * tpt], del, kl2, thr, p1, close);
-      acc_pot<KER, CHK, false>(xt, yt, zt, fs[j + 6 * tpt], del, kl2, thr, p2, close);
-      acc_pot<KER, CHK, true>(xt, yt, zt, fs[j + 7 * tpt], del, kl2, thr, p3, close);
-    }
-  }
   for (; j + 3 * tpt < je; j += 4 * tpt) {
     acc_pot<KER, CHK>(xt, yt, zt, fs[j], del, kl2, thr, p0, close);
     acc_pot<KER, CHK>(xt, yt, zt, fs[j + tpt], del, kl2, thr, p1, close);
@@ -487,11 +469,11 @@ __device__ __forceinline__ bool near_group(const NearArgs& a, int g) {
           } else {
             if (valid) {
               const double4* ds = reinterpret_cast<const double4*>(ts);
-              double p = 0.0;
+              double p0 = 0.0, p1 = 0.0;
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
-              for (int j = slice; j < ns; j += tpt)
-                if (j != selfj) p += pair<KER, EPS>(x, y, z, ds[j], sdel, skappa);
-              part = p;
+              sweep_pot64<KER, EPS>(ds, slice, je, tpt, x, y, z, sdel, skappa, p0, p1);
+              if (self_in) sweep_pot64<KER, EPS>(ds, selfj + tpt, ns, tpt, x, y, z, sdel, skappa, p0, p1);
+              part = p0 + p1;
             }
           }
           if (valid && se->self_term && self_in) {
