@@ -162,6 +162,10 @@ struct Lists {
   int last_ngroups = 0;                     // groups and totals of the last build (sizing)
   unsigned long long last_totals[4] = {0, 0, 0, 0};
   bool fallback = false;                    // the last build used count, scan and fill
+  DBuf<unsigned> gstage;                    // per resident CTA: staging of one group's entries
+  DBuf<int> head;                           // the single-pass build's work counter
+  long long last_stage[2] = {0, 0};         // largest group of the last build: far, near
+                                            // staging words (entries x (mask words + 1))
   // The lists also serve alt_key when alt_valid: the build checked that MAC at every
   // (target, node) it visited and no decision differed, so that MAC's own traversal
   // would have visited the same nodes and emitted the same entries.

@@ -11,12 +11,16 @@
 // Restricted to one target, the entries are exactly its reference traversal, in order.
 // In a forest the walk starts at the root of the group's system, with that system's MAC.
 //
-// Single pass: each CTA stages its entries in shared memory, then reserves room in the
+// Single pass: a persistent kernel whose CTAs take groups from a device counter; each CTA
+// stages a group's entries in its own region of global memory, then reserves room in the
 // global lists with one atomic per list and copies them out (a group's entries stay
 // contiguous and in order; groups land in completion order, addressed by begin/count).
-// The lists are written in place, into arrays sized from an estimate.  A group whose
-// entries do not fit its staging area, or whose reservation runs past the arrays, makes
-// the whole build fall back to a count pass, a prefix sum and a fill pass.
+// The lists are written in place, into arrays sized from an estimate, and the staging
+// regions are sized from the largest group of the previous build (a first build uses an
+// allowance; no region is larger than the tree's worst case, every node a far entry and
+// every leaf a near one).  A group that overflows its staging region, or a reservation
+// that runs past the arrays, makes the whole build fall back to a count pass, a prefix
+// sum and a fill pass; so does a context whose memory budget has no room for the staging.
 //
 // Optionally the walk also evaluates a second MAC (another kernel's parameters, e.g. the
 // Coulomb test's (r^2 + del) - del next to the screened r^2 - mac_del) at every (target,
@@ -35,10 +39,8 @@ namespace {
 
 constexpr int LT = 1024;          // threads of the list builder (one per target of a group)
 constexpr int LSTK = 256;         // traversal stack entries per group
-constexpr int STAGE_FAR = 20480;  // staging words (node + mask words per entry), far list
-constexpr int STAGE_NEAR = 6144;  // staging words, near list
 constexpr size_t STACK_BYTES = 32 * LSTK * sizeof(int);  // per-warp node stacks
-constexpr size_t STAGE_BYTES = STACK_BYTES + (STAGE_FAR + STAGE_NEAR) * sizeof(unsigned);
+constexpr long long STAGE_FIRST[2] = {768 * 33, 192 * 33};  // first build: far, near words
 
 enum { MODE_COUNT = 0, MODE_FILL = 1, MODE_STAGE = 2 };
 
@@ -62,6 +64,13 @@ struct ListArgs {
   unsigned long long cap[4];   // MODE_STAGE: room in the four output arrays
   int has_alt;                 // also evaluate a second MAC and compare its decisions
   double alt_acc, alt_add, alt_sub;
+  // MODE_STAGE (k_lists_queue): each resident CTA's own staging region in global memory,
+  // stage_far + stage_near words (far nodes | far masks, near nodes | near masks), and the
+  // work counter over the ngroups groups
+  unsigned* gstage;
+  long long stage_far, stage_near;
+  int* head;
+  int ngroups;
 };
 
 // The alternative MAC's decision for squared distance s and node sqradius w.
@@ -69,17 +78,20 @@ __device__ __forceinline__ bool alt_ok(const ListArgs& a, double s, double w) {
   return w < dmul(a.alt_acc, dsub(dadd(s, a.alt_add), a.alt_sub));
 }
 
+// The walk of group g by the whole CTA.  MODE_COUNT counts the group's entries, MODE_FILL
+// writes them at the offsets a scan gave, MODE_STAGE writes them into the CTA's staging
+// region and then copies them into room reserved with one atomic per list.
 template <int MODE>
-__global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
+__device__ __forceinline__ void walk_group(const ListArgs& a, int g) {
   __shared__ unsigned s_mask[LSTK][32];  // each warp's mask word of every stack entry
   __shared__ unsigned s_am[2][32], s_rm[2][32];  // accept / reject words, by parity
   __shared__ unsigned long long s_base[4];
   extern __shared__ unsigned dyn[];
-  // dynamic shared memory: each warp's own copy of the node stack, then (MODE_STAGE) the
-  // staging area of the lists
+  // dynamic shared memory: each warp's own copy of the node stack
   int (*s_node)[LSTK] = reinterpret_cast<int (*)[LSTK]>(dyn);
-  unsigned* stage = dyn + 32 * LSTK;
-  const int g = blockIdx.x;
+  unsigned* stage = MODE == MODE_STAGE
+                        ? a.gstage + (size_t)blockIdx.x * (size_t)(a.stage_far + a.stage_near)
+                        : nullptr;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int t0 = a.g_tstart[g], tc = a.g_tcount[g];
   const int W = (tc + 31) >> 5;
@@ -87,11 +99,12 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   const int root = a.g_sys[g];
   const double macc = a.sys[root].acc, madd = a.sys[root].mac_add, msub = a.sys[root].mac_sub;
   // staging layout: far nodes | far masks, near nodes | near masks
-  const int fcap = STAGE_FAR / (W + 1), ncap = STAGE_NEAR / (W + 1);
+  const long long fcap = MODE == MODE_STAGE ? a.stage_far / (W + 1) : 0;
+  const long long ncap = MODE == MODE_STAGE ? a.stage_near / (W + 1) : 0;
   int* sf_node = reinterpret_cast<int*>(stage);
   unsigned* sf_mask = stage + fcap;
-  int* sn_node = reinterpret_cast<int*>(stage + STAGE_FAR);
-  unsigned* sn_mask = stage + STAGE_FAR + ncap;
+  int* sn_node = reinterpret_cast<int*>(stage + a.stage_far);
+  unsigned* sn_mask = stage + a.stage_far + ncap;
   double x = 0, y = 0, z = 0;
   if (i < tc) { x = a.tx[t0 + i]; y = a.ty[t0 + i]; z = a.tz[t0 + i]; }
   if (lane == 0) {
@@ -207,6 +220,28 @@ __global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
   for (int k = threadIdx.x; k < nn * W; k += LT) a.near_mask[s_base[3] + k] = sn_mask[k];
 }
 
+// Count / fill passes: CTA b walks group b.
+template <int MODE>
+__global__ void __launch_bounds__(LT) k_lists(ListArgs a) {
+  walk_group<MODE>(a, blockIdx.x);
+}
+
+// The single-pass build: a persistent kernel whose CTAs take groups from a device counter
+// and stage each group's entries in their own global-memory region, so that a group is
+// walked once.  No CTA waits for another; the counter is the only shared state.
+__global__ void __launch_bounds__(LT) k_lists_queue(ListArgs a) {
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(a.head, 1);
+    __syncthreads();
+    const int g = s_item;
+    __syncthreads();  // every thread has read s_item before it is overwritten
+    if (g >= a.ngroups) return;
+    walk_group<MODE_STAGE>(a, g);
+    __syncthreads();  // the group's copy-out reads precede the next group's staging writes
+  }
+}
+
 // Exclusive scan of int counts times a per-group factor (one block); the total goes to
 // *total.  tcount == nullptr: factor 1, else (tcount+31)/32 mask words per entry.
 __global__ void k_scan_cnt(const int* in, const int* tcount, long long* out, int n,
@@ -245,8 +280,8 @@ __global__ void k_scan_cnt(const int* in, const int* tcount, long long* out, int
 }
 
 void set_stage_attr() {
-  ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_STAGE>), (int)STAGE_BYTES);
-  // static + dynamic shared memory of the count / fill passes is above the 48 KB default
+  // static + dynamic shared memory is above the 48 KB default
+  ensure_smem_attr(reinterpret_cast<const void*>(k_lists_queue), (int)STACK_BYTES);
   ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_COUNT>), (int)STACK_BYTES);
   ensure_smem_attr(reinterpret_cast<const void*>(k_lists<MODE_FILL>), (int)STACK_BYTES);
 }
@@ -388,16 +423,43 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   a.far_node = L->far_node.p; a.far_mask = L->far_mask.p;
   a.near_node = L->near_node.p; a.near_mask = L->near_mask.p;
   set_stage_attr();
-  count_launch(), k_lists<MODE_STAGE><<<ng, LT, STAGE_BYTES, s>>>(a);
-  BIT_CHECK_LAUNCH();
-  unsigned long long h[8];
+  // staging: one region per resident CTA.  A group's entries number at most the tree's
+  // nodes (far) and leaves (near), each with at most 32 mask words.
+  int maxw = 1;
+  for (int g = 0; g < ng; g++) maxw = std::max(maxw, (tc[g] + 31) / 32);
+  int per_sm = 0;
+  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lists_queue, LT, STACK_BYTES));
+  const int slots = std::max(1, std::min(ng, c->num_sms * std::max(per_sm, 1)));
+  const long long worst[2] = {(maxw + 1LL) * std::max(t->numtree, 1),
+                              (maxw + 1LL) * std::max(t->nleaves, 1)};
+  long long want[2];
+  for (int k = 0; k < 2; k++)
+    want[k] = std::min(worst[k], L->last_stage[k] > 0 ? L->last_stage[k] + L->last_stage[k] / 4 + 64
+                                                      : STAGE_FIRST[k]);
+  a.stage_far = want[0];
+  a.stage_near = want[1];
+  const size_t stage_words = (size_t)slots * (size_t)(want[0] + want[1]);
+  const bool staged = L->gstage.n >= stage_words ||
+                      !c->budget || c->in_use + stage_words * sizeof(unsigned) <= c->budget;
+  unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   std::vector<int> hf(ng), hn(ng);
-  BIT_CUDA(cudaMemcpyAsync(h, cnt.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hf.data(), L->far_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaMemcpyAsync(hn.data(), L->near_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
-  BIT_CUDA(cudaStreamSynchronize(s));
-  int err = (int)(h[6] & 0xffffffffu);
-  if (err & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded (tree deeper than supported)");
+  int err = 2;  // no single pass: straight to count, scan and fill
+  if (staged) {
+    L->gstage.ensure(c, stage_words);
+    L->head.ensure(c, 1);
+    BIT_CUDA(cudaMemsetAsync(L->head.p, 0, sizeof(int), s));
+    a.gstage = L->gstage.p;
+    a.head = L->head.p;
+    a.ngroups = ng;
+    count_launch(), k_lists_queue<<<slots, LT, STACK_BYTES, s>>>(a);
+    BIT_CHECK_LAUNCH();
+    BIT_CUDA(cudaMemcpyAsync(h, cnt.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(hf.data(), L->far_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaMemcpyAsync(hn.data(), L->near_cnt.p, ng * sizeof(int), cudaMemcpyDeviceToHost, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
+    err = (int)(h[6] & 0xffffffffu);
+    if (err & 1) fail(BIT_ERR_CAPACITY, "traversal stack capacity exceeded (tree deeper than supported)");
+  }
   L->fallback = (err & 2) != 0;
   if (err & 2) {
     // some group's lists exceed the staging area or the arrays: count, scan, fill
@@ -424,6 +486,12 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   }
   L->last_ngroups = ng;
   for (int k = 0; k < 4; k++) L->last_totals[k] = h[k];
+  L->last_stage[0] = L->last_stage[1] = 0;
+  for (int g = 0; g < ng; g++) {
+    const long long w1 = (tc[g] + 31) / 32 + 1;
+    L->last_stage[0] = std::max(L->last_stage[0], w1 * hf[g]);
+    L->last_stage[1] = std::max(L->last_stage[1], w1 * hn[g]);
+  }
   L->nfar = (long long)h[0];
   L->nnear = (long long)h[2];
   L->far_pairs = (long long)h[4];

@@ -185,9 +185,9 @@ def test_whole_pipeline_host_buffers(ctx, orc):
 
 
 def test_acc_zero_is_the_direct_sum_through_the_fallback_lists(ctx, orc):
-    """acc = 0 accepts no cluster: every leaf is a near entry of every group, more than a
-    group's staging area holds, so the lists come from the count / scan / fill passes, and
-    the potential is the FP64 direct sum."""
+    """acc = 0 accepts no cluster: every leaf is a near entry of every group, far more than
+    the first build's estimated arrays hold, so the lists come from the count / scan / fill
+    passes, and the potential is the FP64 direct sum."""
     import bit_b200 as B
     from bit_b200 import workloads
     x, y, z, q = workloads.uniform_cube(20000, seed=7)
