@@ -168,6 +168,8 @@ SIGNATURES = [
                                          C.c_int, C.POINTER(EvalParams), _dp]),
     ("bit_tree_stats", C.c_int, [_vp, C.POINTER(Stats)]),
     ("bit_device_fma_peak", C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
+    ("bit_device_fp64_math_error", C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double)]),
     ("bit_tree_target_lists", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _ip, _ip, C.c_int,
                                         _ip]),
     ("bit_bie_solve", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, C.c_double, _dp, _dp, _dp,
@@ -309,6 +311,14 @@ class Context:
         v = C.c_double()
         self.check(lib().bit_device_fma_peak(self.h, precision, C.byref(v)), "bit_device_fma_peak")
         return v.value
+
+    def fp64_math_error(self, n=1 << 22):
+        """Largest difference, in ulps of CUDA's result, of the FP64 near field's own exp
+        and rsqrt from CUDA's, over n seeded arguments: {"exp": e, "rsqrt": r}."""
+        e, r = C.c_double(), C.c_double()
+        self.check(lib().bit_device_fp64_math_error(self.h, n, C.byref(e), C.byref(r)),
+                   "bit_device_fp64_math_error")
+        return {"exp": e.value, "rsqrt": r.value}
 
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()

@@ -896,6 +896,16 @@ bit_status bit_device_fma_peak(bit_ctx* h, bit_precision prec, double* flops_per
   });
 }
 
+bit_status bit_device_fp64_math_error(bit_ctx* h, long long n, double* exp_ulps,
+                                      double* rsqrt_ulps) {
+  if (!h || !exp_ulps || !rsqrt_ulps || n < 1) return BIT_ERR_INVALID_ARGUMENT;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    fp64_math_error(c, n, exp_ulps, rsqrt_ulps);
+  });
+}
+
 bit_status bit_tree_stats(const bit_tree* th, bit_stats* st) {
   if (!th || !st) return BIT_ERR_INVALID_ARGUMENT;
   Tree* t = const_cast<Tree*>(&th->t);

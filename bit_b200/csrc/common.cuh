@@ -141,6 +141,17 @@ struct ListKey {
   }
 };
 
+// Sizes of a list build, kept to size the next one (by its tree, and by its context for
+// the next tree: a step that rebuilds its tree meets the same MAC on similar data).
+struct ListSizing {
+  int ngroups = 0;                          // 0: no build yet
+  double acc = -1;                          // the build's MAC parameter
+  int points = 0;
+  unsigned long long totals[4] = {0, 0, 0, 0};  // far entries, far words, near entries, near words
+  long long stage[2] = {0, 0};              // largest group: far, near staging words
+                                            // (entries x (mask words + 1))
+};
+
 struct Lists {
   ListKey key;
   bool valid = false;
@@ -159,13 +170,10 @@ struct Lists {
   DBuf<int> order;                          // groups by decreasing work
   std::vector<long long> h_work;            // estimated work of each group
   long long version = 0;                    // bumped by every build
-  int last_ngroups = 0;                     // groups and totals of the last build (sizing)
-  unsigned long long last_totals[4] = {0, 0, 0, 0};
+  ListSizing last;                          // the last build's sizes
   bool fallback = false;                    // the last build used count, scan and fill
   DBuf<unsigned> gstage;                    // per resident CTA: staging of one group's entries
   DBuf<int> head;                           // the single-pass build's work counter
-  long long last_stage[2] = {0, 0};         // largest group of the last build: far, near
-                                            // staging words (entries x (mask words + 1))
   // The lists also serve alt_key when alt_valid: the build checked that MAC at every
   // (target, node) it visited and no decision differed, so that MAC's own traversal
   // would have visited the same nodes and emitted the same entries.
@@ -190,6 +198,7 @@ struct Ctx {
   // on threads per target (0: the defaults)
   int near_tile = 0, near_split = 0;
   ListKey mac_hint;       // MAC of the last particle-target evaluation (acc < 0: none)
+  ListSizing list_hint;   // sizes of the last list build of any tree
   // small device scratch for flags / counters
   DBuf<long long> scratch_ll;
   long long* h_pinned = nullptr;  // pinned host staging for small read-backs (64 entries)
@@ -303,6 +312,7 @@ void direct_potential(Ctx* c, int n, const double* x, const double* y, const dou
 void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* fy, double* fz);
 // Measured FMA throughput of the context's device, flop/s (2 per FMA), FP32 or FP64.
 double fma_peak(Ctx* c, bool f32);
+void fp64_math_error(Ctx* c, long long n, double* exp_ulps, double* rsqrt_ulps);
 // FP64 field direct sum at m particle targets tg (device pointers); out = fx | fy | fz.
 void direct_field(Ctx* c, int n, const double* x, const double* y, const double* z,
                   const double* q, int regularised, double del, int korder, int m,

@@ -16,11 +16,12 @@
 // global lists with one atomic per list and copies them out (a group's entries stay
 // contiguous and in order; groups land in completion order, addressed by begin/count).
 // The lists are written in place, into arrays sized from an estimate, and the staging
-// regions are sized from the largest group of the previous build (a first build uses an
-// allowance; no region is larger than the tree's worst case, every node a far entry and
-// every leaf a near one).  A group that overflows its staging region, or a reservation
-// that runs past the arrays, makes the whole build fall back to a count pass, a prefix
-// sum and a fill pass; so does a context whose memory budget has no room for the staging.
+// regions are sized from the largest group of the previous build (of this tree, else the
+// context's last build under the same MAC; a first build uses an allowance; no region is
+// larger than the tree's worst case, every node a far entry and every leaf a near one).
+// A group that overflows its staging region, or a reservation that runs past the arrays,
+// makes the whole build fall back to a count pass, a prefix sum and a fill pass; so does
+// a context whose memory budget has no room for the staging.
 //
 // Optionally the walk also evaluates a second MAC (another kernel's parameters, e.g. the
 // Coulomb test's (r^2 + del) - del next to the screened r^2 - mac_del) at every (target,
@@ -405,10 +406,15 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
   // its staging area or the arrays makes the build fall back to count, scan and fill.
   long long words = 0;
   for (int g = 0; g < ng; g++) words += (tc[g] + 31) / 32;
+  // sizes of this tree's last build, else of the context's last build under the same MAC
+  const ListSizing* hint = L->last.ngroups > 0 ? &L->last : nullptr;
+  if (!hint && c->list_hint.ngroups > 0 && c->list_hint.acc == key.acc &&
+      c->list_hint.points == key.points)
+    hint = &c->list_hint;
   unsigned long long cap[4];
-  if (L->last_ngroups > 0) {
-    const double f = 1.25 * (double)ng / L->last_ngroups;
-    for (int k = 0; k < 4; k++) cap[k] = (unsigned long long)(f * L->last_totals[k]) + 1024;
+  if (hint) {
+    const double f = 1.25 * (double)ng / hint->ngroups;
+    for (int k = 0; k < 4; k++) cap[k] = (unsigned long long)(f * hint->totals[k]) + 1024;
   } else {
     cap[0] = 192ull * ng + 1024;
     cap[1] = 192ull * words + 1024;
@@ -434,8 +440,9 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
                               (maxw + 1LL) * std::max(t->nleaves, 1)};
   long long want[2];
   for (int k = 0; k < 2; k++)
-    want[k] = std::min(worst[k], L->last_stage[k] > 0 ? L->last_stage[k] + L->last_stage[k] / 4 + 64
-                                                      : STAGE_FIRST[k]);
+    want[k] = std::min(worst[k], hint && hint->stage[k] > 0
+                                     ? hint->stage[k] + hint->stage[k] / 4 + 64
+                                     : STAGE_FIRST[k]);
   a.stage_far = want[0];
   a.stage_near = want[1];
   const size_t stage_words = (size_t)slots * (size_t)(want[0] + want[1]);
@@ -484,14 +491,18 @@ void build_lists(Tree* t, Lists* L, const ListKey& key, int ntargets, const doub
     count_launch(), k_lists<MODE_FILL><<<ng, LT, STACK_BYTES, s>>>(a);
     BIT_CHECK_LAUNCH();
   }
-  L->last_ngroups = ng;
-  for (int k = 0; k < 4; k++) L->last_totals[k] = h[k];
-  L->last_stage[0] = L->last_stage[1] = 0;
+  ListSizing& z = L->last;
+  z.ngroups = ng;
+  z.acc = key.acc;
+  z.points = key.points;
+  for (int k = 0; k < 4; k++) z.totals[k] = h[k];
+  z.stage[0] = z.stage[1] = 0;
   for (int g = 0; g < ng; g++) {
     const long long w1 = (tc[g] + 31) / 32 + 1;
-    L->last_stage[0] = std::max(L->last_stage[0], w1 * hf[g]);
-    L->last_stage[1] = std::max(L->last_stage[1], w1 * hn[g]);
+    z.stage[0] = std::max(z.stage[0], w1 * hf[g]);
+    z.stage[1] = std::max(z.stage[1], w1 * hn[g]);
   }
+  c->list_hint = z;
   L->nfar = (long long)h[0];
   L->nnear = (long long)h[2];
   L->far_pairs = (long long)h[4];

@@ -19,6 +19,7 @@
 #include <climits>
 
 #include "common.cuh"
+#include "fp64math.cuh"
 #include "tma.cuh"
 
 namespace bit {
@@ -91,17 +92,20 @@ struct Prec<false> {
 };
 
 // One pair's contribution in FP64: the reference's q / sqrt(r^2) and q e^{-kappa r} / r
-// (src/tree3d.cpp:4765-4769, 3609-3618), with 1/r from one FP64 rsqrt (within an ulp of
-// 1/sqrt) in place of a square root and a division.
+// (src/tree3d.cpp:4765-4769, 3609-3618), with 1/r from one refined rsqrt (within an ulp
+// of 1/sqrt) in place of a square root and a division, and a branch-free exp (within an
+// ulp), so that the unrolled pairs of a sweep interleave: at 2M clustered, p = 8,
+// theta = 0.7, the screened FP64 near field takes 21.1 ms against 26.2 ms with CUDA's
+// exp and rsqrt, the Coulomb one 15.9 against 16.5 ms.
 template <int KER, bool EPS>
 __device__ __forceinline__ double pair(double x, double y, double z, double4 s, double del,
                                        double kappa) {
   const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
   const double r2 = dx * dx + dy * dy + dz * dz + del;
   if (EPS && !(r2 > kEpsNear)) return 0.0;
-  const double ri = rsqrt(r2);
+  const double ri = rsqrt_nr(r2);
   if (KER == BIT_KERNEL_COULOMB) return s.w * ri;
-  return s.w * exp(-kappa * (r2 * ri)) * ri;
+  return s.w * exp_tang(-kappa * (r2 * ri)) * ri;
 }
 // Field of eval_grad_kernel_reg (src/tree3d.cpp:73-97), KERNEL_ORDER = 0:
 // q * (-(x_j - x) / (r * r^2)).
