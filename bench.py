@@ -43,6 +43,10 @@ ACC = 0.7           # theta
 KAPPA = 1.0
 DEL = 0.005 ** 2    # delta^2
 FLOPS_NEAR = {"screened": 14, "coulomb": 11}     # per near pair (rsqrt, exp counted as 1)
+# FP64 pipe operations the FP64 near kernel issues per pair (its own rsqrt and exp spelled
+# out: 3 differences, 3 for r^2 + del, 4 for the Newton step, 11 for exp, the products):
+# the instruction-level ceiling of that kernel is peak / 2 / ops pairs per second
+FP64_OPS_NEAR = {"screened": 26, "coulomb": 13}
 # Accuracy-matched parameters: (p, theta, N0) at which the plain FP64 treecode reaches 1e-6
 # relative L2 against the FP64 direct sum on these workloads (measured; the run reports
 # the errors it reaches)
@@ -351,14 +355,21 @@ def roofline_near(prec, kname, st, n, peak_tflops):
     ach = fl * pairs / st["t_near"] / 1e12
     t = "F64" if prec == "fp64" else "F32"
     key = f"k_near<{kname.upper()}, {t}>"
-    return {"bound": "fp64" if prec == "fp64" else "fp32+mufu", "kernel": key, "precision": prec,
-            "achieved": ach, "peak": peak_tflops, "unit": "TFLOP/s", "frac": ach / peak_tflops,
-            "peak_source": f"measured {'FP64 DFMA' if prec == 'fp64' else 'FP32 FFMA'} throughput of "
-                           "this device (bit_device_fma_peak)",
-            "traffic": TRAFFIC.get(key), "traffic_unit": "bytes per launch (dram read+write)",
-            "traffic_source": TRAFFIC_SOURCE if TRAFFIC.get(key) else None,
-            "seconds": st["t_near"],
-            "algorithmic": f"{fl} flops x {pairs} near pairs per launch"}
+    out = {"bound": "fp64" if prec == "fp64" else "fp32+mufu", "kernel": key, "precision": prec,
+           "achieved": ach, "peak": peak_tflops, "unit": "TFLOP/s", "frac": ach / peak_tflops,
+           "peak_source": f"measured {'FP64 DFMA' if prec == 'fp64' else 'FP32 FFMA'} throughput of "
+                          "this device (bit_device_fma_peak)",
+           "traffic": TRAFFIC.get(key), "traffic_unit": "bytes per launch (dram read+write)",
+           "traffic_source": TRAFFIC_SOURCE if TRAFFIC.get(key) else None,
+           "seconds": st["t_near"],
+           "algorithmic": f"{fl} flops x {pairs} near pairs per launch"}
+    if prec == "fp64":
+        ops = FP64_OPS_NEAR[kname]
+        ceiling = fl / (2.0 * ops)
+        out["fp64_ops_per_pair"] = ops
+        out["frac_ceiling"] = ceiling
+        out["frac_of_ceiling"] = out["frac"] / ceiling
+    return out
 
 
 def run_matched_c2(step, timed, ctx, x, y, z, q, out_s, out_c, args):

@@ -91,21 +91,39 @@ struct Prec<false> {
   static constexpr int TILE = 512, TILE_MIN = 128, TILE_MAX = 1024;
 };
 
-// One pair's contribution in FP64: the reference's q / sqrt(r^2) and q e^{-kappa r} / r
-// (src/tree3d.cpp:4765-4769, 3609-3618), with 1/r from one refined rsqrt (within an ulp
-// of 1/sqrt) in place of a square root and a division, and a branch-free exp (within an
-// ulp), so that the unrolled pairs of a sweep interleave: at 2M clustered, p = 8,
-// theta = 0.7, the screened FP64 near field takes 21.1 ms against 26.2 ms with CUDA's
-// exp and rsqrt, the Coulomb one 15.9 against 16.5 ms.
+// One pair's contribution in FP64, added to acc: the reference's q / sqrt(r^2) and
+// q e^{-kappa r} / r (src/tree3d.cpp:4765-4769, 3609-3618).  1/r comes from a refined
+// reciprocal square root (rsqrt_nr, within an ulp of 1/sqrt) in place of a square root
+// and a division, the exponential from a branch-free exp (exp_tang, within an ulp), so
+// that the unrolled pairs of a sweep interleave; r^2 + del is one FMA chain, and the
+// Coulomb pair folds q and the accumulation into the Newton step's last FMA.  At 2M
+// clustered, p = 8, theta = 0.7, the screened FP64 near field takes 21.2 ms against 26.2
+// ms with CUDA's exp and rsqrt and the plain forms, the Coulomb one 10.8 against 12.1 ms
+// (the same tuned tiles); the results move by about 2e-16 (relative L2).  EPS: a pair with
+// r^2 <= 1e-14 adds nothing.
 template <int KER, bool EPS>
-__device__ __forceinline__ double pair(double x, double y, double z, double4 s, double del,
-                                       double kappa) {
+__device__ __forceinline__ void pair_acc(double x, double y, double z, double4 s, double del,
+                                         double kappa, double& acc) {
   const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
-  const double r2 = dx * dx + dy * dy + dz * dz + del;
-  if (EPS && !(r2 > kEpsNear)) return 0.0;
-  const double ri = rsqrt_nr(r2);
-  if (KER == BIT_KERNEL_COULOMB) return s.w * ri;
-  return s.w * exp_tang(-kappa * (r2 * ri)) * ri;
+  const double r2 = fma(dx, dx, fma(dy, dy, fma(dz, dz, del)));
+  double q = s.w, rr = r2;
+  if (EPS) {
+    const bool skip = !(r2 > kEpsNear);
+    q = skip ? 0.0 : q;
+    rr = skip ? 1.0 : rr;
+  }
+  double y0;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y0) : "d"(rr));
+  // one third-order Newton step, as rsqrt_nr: y0 (1 + e c), e = 1 - rr y0^2, c = 1/2 + 3e/8
+  const double e = fma(-rr * y0, y0, 1.0);
+  const double ec = e * fma(e, 0.375, 0.5);
+  if (KER == BIT_KERNEL_COULOMB) {
+    const double qy = q * y0;
+    acc = fma(qy, ec, acc + qy);
+  } else {
+    const double ri = fma(y0, ec, y0);
+    acc = fma(q * exp_tang(-kappa * (rr * ri)), ri, acc);
+  }
 }
 // Field of eval_grad_kernel_reg (src/tree3d.cpp:73-97), KERNEL_ORDER = 0:
 // q * (-(x_j - x) / (r * r^2)).
@@ -197,20 +215,24 @@ __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, 
 }
 
 // FP64: this lane's pairs j, j + tpt, ... < je (the target's own source excluded by the
-// caller's split of the range), four independent accumulators so that consecutive pairs
-// do not wait on one another's additions.
+// caller's split of the range), eight pairs per iteration into four independent
+// accumulators so that consecutive pairs do not wait on one another's additions.
 template <int KER, bool EPS>
 __device__ __forceinline__ void sweep_pot64(const double4* ds, int j, int je, int tpt, double x,
                                             double y, double z, double del, double kappa,
                                             double& p0, double& p1) {
   double p2 = 0.0, p3 = 0.0;
-  for (; j + 3 * tpt < je; j += 4 * tpt) {
-    p0 += pair<KER, EPS>(x, y, z, ds[j], del, kappa);
-    p1 += pair<KER, EPS>(x, y, z, ds[j + tpt], del, kappa);
-    p2 += pair<KER, EPS>(x, y, z, ds[j + 2 * tpt], del, kappa);
-    p3 += pair<KER, EPS>(x, y, z, ds[j + 3 * tpt], del, kappa);
+  for (; j + 7 * tpt < je; j += 8 * tpt) {
+    pair_acc<KER, EPS>(x, y, z, ds[j], del, kappa, p0);
+    pair_acc<KER, EPS>(x, y, z, ds[j + tpt], del, kappa, p1);
+    pair_acc<KER, EPS>(x, y, z, ds[j + 2 * tpt], del, kappa, p2);
+    pair_acc<KER, EPS>(x, y, z, ds[j + 3 * tpt], del, kappa, p3);
+    pair_acc<KER, EPS>(x, y, z, ds[j + 4 * tpt], del, kappa, p0);
+    pair_acc<KER, EPS>(x, y, z, ds[j + 5 * tpt], del, kappa, p1);
+    pair_acc<KER, EPS>(x, y, z, ds[j + 6 * tpt], del, kappa, p2);
+    pair_acc<KER, EPS>(x, y, z, ds[j + 7 * tpt], del, kappa, p3);
   }
-  for (; j < je; j += tpt) p0 += pair<KER, EPS>(x, y, z, ds[j], del, kappa);
+  for (; j < je; j += tpt) pair_acc<KER, EPS>(x, y, z, ds[j], del, kappa, p0);
   p0 += p2;
   p1 += p3;
 }
@@ -657,7 +679,7 @@ __device__ double close_sum(const NearArgs& a, const SysEval* se, int t, int g, 
     const int s0 = a.start[node];
     for (int j = s0 + j0 + lane; j < s0 + j1; j += 32)
       if (j != self && r2_32(xt, yt, zt, fs[j], del) < thr)
-        acc += pair<KER, EPS>(x, y, z, a.src64[j], sdel, skappa);
+        pair_acc<KER, EPS>(x, y, z, a.src64[j], sdel, skappa, acc);
   };
   const int nrec = a.ccnt[t];
   if (nrec <= kCloseRec) {
