@@ -53,11 +53,21 @@ FP64_OPS_NEAR = {"screened": 26, "coulomb": 13}
 MATCHED_C2 = dict(nterms=9, acc=0.15, maxmemb=1000)
 MATCHED_BIE = dict(nterms=9, acc=0.15, maxmemb=500)
 MATCHED_BATCH_ACC = {5: 0.015, 7: 0.05, 9: 0.1}   # theta by nterms (p = 4, 6, 8)
-# DRAM bytes (read + write) per launch of the full-size kernels, from single-kernel ncu
-# captures of the 200k clustered case scaled by the pairs each launch processes; None
-# where no capture of the current kernel exists.
-TRAFFIC = {}
-TRAFFIC_SOURCE = None
+# DRAM bytes (read + write) per launch of the full-size kernels (clustered N = 2M, p = 8,
+# theta = 0.7, N0 = 1000, the near field at its default tile), from an ncu launch list of
+# one step taking dram__bytes_read.sum and dram__bytes_write.sum in one pass per launch.
+# Captures of the 200k case give 13.5 MB (FP64 near) and 7.8 MB (FP64 far) per launch,
+# i.e. 135 and 78 MB scaled by N; the full-size launches read more (sources re-read by
+# groups of several waves once the 126 MB L2 no longer holds them).
+TRAFFIC = {
+    "k_near<SCREENED, F64>": 206.03e6, "k_near<COULOMB, F64>": 225.93e6,
+    "k_far<9, SCREENED, double>": 101.88e6, "k_far<9, COULOMB, double>": 101.41e6,
+    "k_near<SCREENED, F32>": 131.50e6, "k_near<COULOMB, F32>": 113.31e6,
+    "k_far<9, SCREENED, float>": 97.85e6, "k_far<9, COULOMB, float>": 97.43e6,
+}
+TRAFFIC_SOURCE = ("ncu launch list of the full-size step (gpu__time_duration.sum, "
+                  "dram__bytes_read.sum, dram__bytes_write.sum; one pass per launch), "
+                  "kernels of this build, near field at its default tile")
 METRIC = "treecode evals/s (clustered N=2M, p=8, theta=0.7, N0=1000, screened+Coulomb)"
 
 

@@ -110,7 +110,12 @@ constexpr size_t far_smem(size_t acc_bytes_per_row_target, size_t moment_bytes) 
          NW * kGroupMax * acc_bytes_per_row_target + NW * moment_bytes;
 }
 
-constexpr int NWP = 8;  // warps per CTA, potential
+// Warps per CTA of the potential kernels.  FP32: 8 warps, two CTAs per SM at 128 registers.
+// FP64 (254 registers): 4 warps, so that two CTAs share an SM and one keeps the FP64 pipe
+// busy while the other waits at its group's closing barrier; one 8-warp CTA per SM was 5%
+// slower at 2M (screened 18.1 against 17.2 ms, Coulomb 11.5 against 11.0 ms).
+template <class T>
+constexpr int nwp() { return sizeof(T) == 4 ? 8 : 4; }
 constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
 
 // The far field of one target group g (the CTA's whole work for that group).  Shared
@@ -121,7 +126,7 @@ template <int NT, int KER, class T>
 __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
   constexpr int TT = num_terms(NT);
   constexpr int TP = FarField<NT>::kPadded;
-  constexpr int NW = NWP;
+  constexpr int NW = nwp<T>();
   extern __shared__ __align__(16) unsigned char sm[];
   double* cx = reinterpret_cast<double*>(sm);
   double* cy = cx + kGroupMax;
@@ -180,7 +185,7 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
 
 // One launch class: CTA b takes group order[b].
 template <int NT, int KER, class T>
-__global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArgs a) {
+__global__ void __launch_bounds__(32 * nwp<T>(), 2) k_far(FarArgs a) {
   far_group<NT, KER, T>(a, a.order[blockIdx.x]);
 }
 
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1) k_far(FarArg
 // same order within the group, as k_far, so the results are identical.  No CTA waits for
 // another; the counter is the only shared state.
 template <class T>
-__global__ void __launch_bounds__(32 * NWP, sizeof(T) == 4 ? 2 : 1)
+__global__ void __launch_bounds__(32 * nwp<T>(), 2)
     k_far_queue(FarArgs a, int count, int* head) {
   __shared__ int s_item;
   for (;;) {
@@ -307,9 +312,10 @@ void set_smem(K kernel, size_t bytes) {
 
 template <int NT, int KER, class T>
 void launch_far(const FarArgs& a, int ng, cudaStream_t s) {
-  const size_t bytes = far_smem<NWP>(WarpAcc<T>::words * sizeof(T), FarField<NT>::kPadded * sizeof(T));
+  const size_t bytes =
+      far_smem<nwp<T>()>(WarpAcc<T>::words * sizeof(T), FarField<NT>::kPadded * sizeof(T));
   set_smem(k_far<NT, KER, T>, bytes);
-  count_launch(), k_far<NT, KER, T><<<ng, 32 * NWP, bytes, s>>>(a);
+  count_launch(), k_far<NT, KER, T><<<ng, 32 * nwp<T>(), bytes, s>>>(a);
 }
 
 template <int NT, int FK, class T>
@@ -351,12 +357,12 @@ void launch_far_queue(Ctx* c, const FarArgs& a, int count, int max_nterms, int* 
 #undef TPN
     default: fail(BIT_ERR_STATE, "moments not computed");
   }
-  const size_t bytes = far_smem<NWP>(WarpAcc<T>::words * sizeof(T), tp * sizeof(T));
+  const size_t bytes = far_smem<nwp<T>()>(WarpAcc<T>::words * sizeof(T), tp * sizeof(T));
   set_smem(k_far_queue<T>, bytes);
   int per_sm = 0;
-  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_far_queue<T>, 32 * NWP, bytes));
+  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_far_queue<T>, 32 * nwp<T>(), bytes));
   const int grid = std::max(1, std::min(count, c->num_sms * std::max(per_sm, 1)));
-  count_launch(), k_far_queue<T><<<grid, 32 * NWP, bytes, s>>>(a, count, head);
+  count_launch(), k_far_queue<T><<<grid, 32 * nwp<T>(), bytes, s>>>(a, count, head);
 }
 
 // The work-queue form is used for plans of several classes when the context allows it;
