@@ -110,23 +110,24 @@ constexpr size_t far_smem(size_t acc_bytes_per_row_target, size_t moment_bytes) 
          NW * kGroupMax * acc_bytes_per_row_target + NW * moment_bytes;
 }
 
-// Warps per CTA of the potential kernels.  FP32: 8 warps, two CTAs per SM at 128 registers.
-// FP64 (254 registers): 4 warps, so that two CTAs share an SM and one keeps the FP64 pipe
-// busy while the other waits at its group's closing barrier; one 8-warp CTA per SM was 5%
-// slower at 2M (screened 18.1 against 17.2 ms, Coulomb 11.5 against 11.0 ms).
+// Warps per CTA of the potential kernels (NW).  FP32: 8 warps, two CTAs per SM at 128
+// registers.  FP64 (254 registers): with many groups, 4 warps, so that two CTAs share an SM
+// and one keeps the FP64 pipe busy while the other waits at its group's closing barrier;
+// with few, 8 warps, so that each group is spread over more warps (eval_far).  Measured on
+// clustered systems, p = 8 (screened, ms, 4 / 8 warps): 378 groups 1.41 / 1.07, 835 groups
+// 3.17 / 3.23, 3,091 groups (2M) 17.25 / 18.12.
 template <class T>
-constexpr int nwp() { return sizeof(T) == 4 ? 8 : 4; }
+constexpr int min_blocks(int nw) { return sizeof(T) == 8 && nw == 8 ? 1 : 2; }
 constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
 
 // The far field of one target group g (the CTA's whole work for that group).  Shared
 // memory: the group's target coordinates, per warp a packed target list, an accumulator row
 // and one cluster's moments (NW * TP of them; a kernel running several orders sizes this for
 // the largest).
-template <int NT, int KER, class T>
+template <int NT, int KER, class T, int NW>
 __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
   constexpr int TT = num_terms(NT);
   constexpr int TP = FarField<NT>::kPadded;
-  constexpr int NW = nwp<T>();
   extern __shared__ __align__(16) unsigned char sm[];
   double* cx = reinterpret_cast<double*>(sm);
   double* cy = cx + kGroupMax;
@@ -184,9 +185,9 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
 }
 
 // One launch class: CTA b takes group order[b].
-template <int NT, int KER, class T>
-__global__ void __launch_bounds__(32 * nwp<T>(), 2) k_far(FarArgs a) {
-  far_group<NT, KER, T>(a, a.order[blockIdx.x]);
+template <int NT, int KER, class T, int NW>
+__global__ void __launch_bounds__(32 * NW, min_blocks<T>(NW)) k_far(FarArgs a) {
+  far_group<NT, KER, T, NW>(a, a.order[blockIdx.x]);
 }
 
 // Persistent work queue over the groups of every class: each CTA takes the next item
@@ -194,8 +195,8 @@ __global__ void __launch_bounds__(32 * nwp<T>(), 2) k_far(FarArgs a) {
 // far field of that group's system (its nterms and kernel) -- the same device code, in the
 // same order within the group, as k_far, so the results are identical.  No CTA waits for
 // another; the counter is the only shared state.
-template <class T>
-__global__ void __launch_bounds__(32 * nwp<T>(), 2)
+template <class T, int NW>
+__global__ void __launch_bounds__(32 * NW, min_blocks<T>(NW))
     k_far_queue(FarArgs a, int count, int* head) {
   __shared__ int s_item;
   for (;;) {
@@ -210,8 +211,8 @@ __global__ void __launch_bounds__(32 * nwp<T>(), 2)
     switch (se->nterms) {
 #define FQ(N)                                                           \
   case N:                                                               \
-    if (coul) far_group<N, BIT_KERNEL_COULOMB, T>(a, g);                \
-    else far_group<N, BIT_KERNEL_SCREENED, T>(a, g);                    \
+    if (coul) far_group<N, BIT_KERNEL_COULOMB, T, NW>(a, g);            \
+    else far_group<N, BIT_KERNEL_SCREENED, T, NW>(a, g);                \
     break;
       FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10)
 #undef FQ
@@ -310,12 +311,12 @@ void set_smem(K kernel, size_t bytes) {
   ensure_smem_attr(reinterpret_cast<const void*>(kernel), (int)bytes);
 }
 
-template <int NT, int KER, class T>
+template <int NT, int KER, class T, int NW>
 void launch_far(const FarArgs& a, int ng, cudaStream_t s) {
   const size_t bytes =
-      far_smem<nwp<T>()>(WarpAcc<T>::words * sizeof(T), FarField<NT>::kPadded * sizeof(T));
-  set_smem(k_far<NT, KER, T>, bytes);
-  count_launch(), k_far<NT, KER, T><<<ng, 32 * nwp<T>(), bytes, s>>>(a);
+      far_smem<NW>(WarpAcc<T>::words * sizeof(T), FarField<NT>::kPadded * sizeof(T));
+  set_smem(k_far<NT, KER, T, NW>, bytes);
+  count_launch(), k_far<NT, KER, T, NW><<<ng, 32 * NW, bytes, s>>>(a);
 }
 
 template <int NT, int FK, class T>
@@ -347,7 +348,7 @@ FarArgs far_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const d
 }  // namespace
 
 // One launch per (nterms, kernel) class, each over its groups (P.far_ord + begin).
-template <class T>
+template <class T, int NW>
 void launch_far_queue(Ctx* c, const FarArgs& a, int count, int max_nterms, int* head,
                       cudaStream_t s) {
   int tp = 0;
@@ -357,12 +358,12 @@ void launch_far_queue(Ctx* c, const FarArgs& a, int count, int max_nterms, int* 
 #undef TPN
     default: fail(BIT_ERR_STATE, "moments not computed");
   }
-  const size_t bytes = far_smem<nwp<T>()>(WarpAcc<T>::words * sizeof(T), tp * sizeof(T));
-  set_smem(k_far_queue<T>, bytes);
+  const size_t bytes = far_smem<NW>(WarpAcc<T>::words * sizeof(T), tp * sizeof(T));
+  set_smem(k_far_queue<T, NW>, bytes);
   int per_sm = 0;
-  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_far_queue<T>, 32 * nwp<T>(), bytes));
+  BIT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_far_queue<T, NW>, 32 * NW, bytes));
   const int grid = std::max(1, std::min(count, c->num_sms * std::max(per_sm, 1)));
-  count_launch(), k_far_queue<T><<<grid, 32 * nwp<T>(), bytes, s>>>(a, count, head);
+  count_launch(), k_far_queue<T, NW><<<grid, 32 * NW, bytes, s>>>(a, count, head);
 }
 
 // The work-queue form is used for plans of several classes when the context allows it;
@@ -383,14 +384,19 @@ void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const doub
   a.out = out;
   cudaStream_t s = t->ctx->stream;
   const bool f32 = P.f32;
+  // FP64: 4-warp CTAs when the evaluation has at least 4 groups per SM.  The choice
+  // follows the whole list (not a launch class), so the queue and the class launches of
+  // one evaluation sum in the same order.
+  const bool narrow = !f32 && L->ngroups >= 4 * t->ctx->num_sms;
   if (use_queue(t->ctx, P.far_classes)) {
     int nt_max = 0, count = 0;
     for (const LaunchClass& k : P.far_classes) nt_max = std::max(nt_max, k.nterms);
     for (const LaunchClass& k : P.far_classes) count += k.count;
     a.order = L->order.p;
     int* head = queue_head(t->ctx, 0, s);
-    if (f32) launch_far_queue<float>(t->ctx, a, count, nt_max, head, s);
-    else launch_far_queue<double>(t->ctx, a, count, nt_max, head, s);
+    if (f32) launch_far_queue<float, 8>(t->ctx, a, count, nt_max, head, s);
+    else if (narrow) launch_far_queue<double, 4>(t->ctx, a, count, nt_max, head, s);
+    else launch_far_queue<double, 8>(t->ctx, a, count, nt_max, head, s);
     BIT_CHECK_LAUNCH();
     return;
   }
@@ -402,11 +408,14 @@ void eval_far(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const doub
 #define CASE(N)                                                                   \
   case N:                                                                         \
     if (f32) {                                                                    \
-      if (coul) launch_far<N, BIT_KERNEL_COULOMB, float>(a, ng, s);               \
-      else launch_far<N, BIT_KERNEL_SCREENED, float>(a, ng, s);                   \
+      if (coul) launch_far<N, BIT_KERNEL_COULOMB, float, 8>(a, ng, s);            \
+      else launch_far<N, BIT_KERNEL_SCREENED, float, 8>(a, ng, s);                \
+    } else if (narrow) {                                                          \
+      if (coul) launch_far<N, BIT_KERNEL_COULOMB, double, 4>(a, ng, s);           \
+      else launch_far<N, BIT_KERNEL_SCREENED, double, 4>(a, ng, s);               \
     } else {                                                                      \
-      if (coul) launch_far<N, BIT_KERNEL_COULOMB, double>(a, ng, s);              \
-      else launch_far<N, BIT_KERNEL_SCREENED, double>(a, ng, s);                  \
+      if (coul) launch_far<N, BIT_KERNEL_COULOMB, double, 8>(a, ng, s);           \
+      else launch_far<N, BIT_KERNEL_SCREENED, double, 8>(a, ng, s);               \
     }                                                                             \
     break;
       CASE(1) CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10)
