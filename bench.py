@@ -683,6 +683,7 @@ def run_serving(ctx, args, matched=False):
     srv = B.Server(slots=1, hbm_budget=budget)
     try:
         serve(reqs, closed, B.FP64, srv, 1)
+        _, cap64 = serve(reqs, closed, B.FP64, srv, 1)
         res64, plain = serve(reqs, arrivals, B.FP64, srv, 1)
     finally:
         srv.close()
@@ -713,6 +714,8 @@ def run_serving(ctx, args, matched=False):
                         f"icosphere level 4..7, p={sp['nterms'] - 1}, theta={sp['acc']}, "
                         f"N0={sp['maxmemb']}, GMRES(50) to 1e-8), 150 GB budget",
             "offered_load": load, "mixed_closed_loop_requests_per_s": cap["requests_per_s"],
+            "fp64_closed_loop_requests_per_s": cap64["requests_per_s"],
+            "capacity_ratio": cap["requests_per_s"] / cap64["requests_per_s"],
             "mixed_continuous_batching": mixed, "fp64_one_at_a_time": plain,
             "throughput_ratio": mixed["requests_per_s"] / plain["requests_per_s"],
             "p99_ratio": plain["p99_latency_s"] / mixed["p99_latency_s"],

@@ -63,7 +63,14 @@ constexpr double kExpLlo = 0x1.abc9e3b39803fp-62;
 constexpr double kRoundShift = 0x1.8p52;  // adding it rounds a double below 2^51 to an integer
 
 // Tang's exp; the table is read through the read-only data cache (a warp's lanes gather
-// from 64 entries in eight 128-byte lines).
+// from 64 entries in eight 128-byte lines).  SMALL: the caller guarantees |t| < 8
+// (kSmallExpArg), so exp(t) cannot underflow and the result needs no check; the value is
+// the full form's.  At 2M clustered, p = 8, theta = 0.7 the screened FP64 near field takes
+// 2% less time (20.3 -> 19.9 ms) with the small form where every pair of a target's tile
+// has kappa r < 8.  (Dropping the second reduction step as well gained another 2% but
+// moved results by up to 3 ulps, so it is not done.)
+constexpr double kSmallExpArg = 8.0;
+template <bool SMALL = false>
 __device__ __forceinline__ double exp_tang(double t) {
   const double kd = fma(t, kExpInvL, kRoundShift);
   const int n = __double2loint(kd);  // rint(t / L), two's complement in the low word
@@ -80,6 +87,7 @@ __device__ __forceinline__ double exp_tang(double t) {
   const double v = s.x + fma(s.x, p, s.y);
   const int m = n >> 6;
   const double e = __hiloint2double(__double2hiint(v) + (m << 20), __double2loint(v));
+  if (SMALL) return e;
   return n < -65280 ? 0.0 : e;  // m < -1020: exp(t) < 1e-307
 }
 

@@ -1,6 +1,7 @@
 // Agreement of the near field's own FP64 exp and rsqrt (fp64math.cuh) with CUDA's exp and
 // rsqrt on the device: the largest difference, in units in the last place of CUDA's
-// result, over n seeded arguments (exp: t uniform in [-707, 0]; rsqrt: x log-uniform in
+// result, over n seeded arguments (exp: t uniform in [-707, 0] for the full form and in
+// (-8, 0] for the small-argument form, the larger of the two; rsqrt: x log-uniform in
 // [1e-12, 1e6]).  A test holds both to a bound.
 #include "common.cuh"
 #include "fp64math.cuh"
@@ -31,7 +32,9 @@ __global__ void k_math_check(long long n, unsigned long long* worst) {
        i += (long long)gridDim.x * blockDim.x) {
     const double t = -707.0 * unit(2 * i);
     const double x = exp10(-12.0 + 18.0 * unit(2 * i + 1));
+    const double ts = -kSmallExpArg * unit(2 * i + 1);
     we = fmax(we, ulp_diff(exp_tang(t), exp(t)));
+    we = fmax(we, ulp_diff(exp_tang<true>(ts), exp(ts)));
     wr = fmax(wr, ulp_diff(rsqrt_nr(x), rsqrt(x)));
   }
   // non-negative doubles order as their bit patterns

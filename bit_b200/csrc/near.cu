@@ -100,8 +100,9 @@ struct Prec<false> {
 // clustered, p = 8, theta = 0.7, the screened FP64 near field takes 21.2 ms against 26.2
 // ms with CUDA's exp and rsqrt and the plain forms, the Coulomb one 10.8 against 12.1 ms
 // (the same tuned tiles); the results move by about 2e-16 (relative L2).  EPS: a pair with
-// r^2 <= 1e-14 adds nothing.
-template <int KER, bool EPS>
+// r^2 <= 1e-14 adds nothing.  SMALL: kappa r < kSmallExpArg, the exponential's
+// small-argument form (no underflow check; the same value).
+template <int KER, bool EPS, bool SMALL = false>
 __device__ __forceinline__ void pair_acc(double x, double y, double z, double4 s, double del,
                                          double kappa, double& acc) {
   const double dx = x - s.x, dy = y - s.y, dz = z - s.z;
@@ -122,7 +123,7 @@ __device__ __forceinline__ void pair_acc(double x, double y, double z, double4 s
     acc = fma(qy, ec, acc + qy);
   } else {
     const double ri = fma(y0, ec, y0);
-    acc = fma(q * exp_tang(-kappa * (rr * ri)), ri, acc);
+    acc = fma(q * exp_tang<SMALL>(-kappa * (rr * ri)), ri, acc);
   }
 }
 // Field of eval_grad_kernel_reg (src/tree3d.cpp:73-97), KERNEL_ORDER = 0:
@@ -216,23 +217,24 @@ __device__ __forceinline__ void acc_pot(float xt, float yt, float zt, float4 s, 
 
 // FP64: this lane's pairs j, j + tpt, ... < je (the target's own source excluded by the
 // caller's split of the range), eight pairs per iteration into four independent
-// accumulators so that consecutive pairs do not wait on one another's additions.
-template <int KER, bool EPS>
+// accumulators so that consecutive pairs do not wait on one another's additions.  SMALL:
+// kappa r < kSmallExpArg for every pair (exp_tang's small-argument form).
+template <int KER, bool EPS, bool SMALL = false>
 __device__ __forceinline__ void sweep_pot64(const double4* ds, int j, int je, int tpt, double x,
                                             double y, double z, double del, double kappa,
                                             double& p0, double& p1) {
   double p2 = 0.0, p3 = 0.0;
   for (; j + 7 * tpt < je; j += 8 * tpt) {
-    pair_acc<KER, EPS>(x, y, z, ds[j], del, kappa, p0);
-    pair_acc<KER, EPS>(x, y, z, ds[j + tpt], del, kappa, p1);
-    pair_acc<KER, EPS>(x, y, z, ds[j + 2 * tpt], del, kappa, p2);
-    pair_acc<KER, EPS>(x, y, z, ds[j + 3 * tpt], del, kappa, p3);
-    pair_acc<KER, EPS>(x, y, z, ds[j + 4 * tpt], del, kappa, p0);
-    pair_acc<KER, EPS>(x, y, z, ds[j + 5 * tpt], del, kappa, p1);
-    pair_acc<KER, EPS>(x, y, z, ds[j + 6 * tpt], del, kappa, p2);
-    pair_acc<KER, EPS>(x, y, z, ds[j + 7 * tpt], del, kappa, p3);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j], del, kappa, p0);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + tpt], del, kappa, p1);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + 2 * tpt], del, kappa, p2);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + 3 * tpt], del, kappa, p3);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + 4 * tpt], del, kappa, p0);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + 5 * tpt], del, kappa, p1);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + 6 * tpt], del, kappa, p2);
+    pair_acc<KER, EPS, SMALL>(x, y, z, ds[j + 7 * tpt], del, kappa, p3);
   }
-  for (; j < je; j += tpt) pair_acc<KER, EPS>(x, y, z, ds[j], del, kappa, p0);
+  for (; j < je; j += tpt) pair_acc<KER, EPS, SMALL>(x, y, z, ds[j], del, kappa, p0);
   p0 += p2;
   p1 += p3;
 }
@@ -498,12 +500,27 @@ __device__ __forceinline__ bool near_group(const NearArgs& a, int g) {
               part = p0 + p1;
             }
           } else {
+            // screened: kappa r stays below kSmallExpArg for every pair of this warp's
+            // targets and tile if it does at r^2 = dmax^2 + del, dmax the target's distance
+            // to the leaf centre plus the leaf's half diagonal (a warp-uniform choice of
+            // the exp form)
+            bool small = false;
+            if (KER == BIT_KERNEL_SCREENED) {
+              const double ox = cx[t0 + i] - c.x, oy = cy[t0 + i] - c.y, oz = cz[t0 + i] - c.z;
+              const double dmax = sqrt(fma(ox, ox, fma(oy, oy, oz * oz))) + sqrt(c.w);
+              small = __all_sync(0xffffffffu, !valid || skappa * sqrt(fma(dmax, dmax, sdel)) < kSmallExpArg);
+            }
             if (valid) {
               const double4* ds = reinterpret_cast<const double4*>(ts);
               double p0 = 0.0, p1 = 0.0;
               const double x = cx[t0 + i], y = cy[t0 + i], z = cz[t0 + i];
-              sweep_pot64<KER, EPS>(ds, slice, je, tpt, x, y, z, sdel, skappa, p0, p1);
-              if (self_in) sweep_pot64<KER, EPS>(ds, selfj + tpt, ns, tpt, x, y, z, sdel, skappa, p0, p1);
+              if (small) {
+                sweep_pot64<KER, EPS, true>(ds, slice, je, tpt, x, y, z, sdel, skappa, p0, p1);
+                if (self_in) sweep_pot64<KER, EPS, true>(ds, selfj + tpt, ns, tpt, x, y, z, sdel, skappa, p0, p1);
+              } else {
+                sweep_pot64<KER, EPS>(ds, slice, je, tpt, x, y, z, sdel, skappa, p0, p1);
+                if (self_in) sweep_pot64<KER, EPS>(ds, selfj + tpt, ns, tpt, x, y, z, sdel, skappa, p0, p1);
+              }
               part = p0 + p1;
             }
           }

@@ -247,8 +247,9 @@ bit_status bit_direct_field(bit_ctx* ctx, int n, const double* x, const double* 
 bit_status bit_device_fma_peak(bit_ctx* ctx, bit_precision prec, double* flops_per_s);
 
 /* Largest difference, in ulps of CUDA's result, between the FP64 near field's own exp and
- * rsqrt and CUDA's exp and rsqrt over n seeded arguments (exp: [-707, 0]; rsqrt:
- * [1e-12, 1e6], log-uniform).  A diagnostic of the device math; no reference counterpart. */
+ * rsqrt and CUDA's exp and rsqrt over n seeded arguments (exp: [-707, 0], and (-8, 0] for
+ * its small-argument form, the larger of the two; rsqrt: [1e-12, 1e6], log-uniform).  A
+ * diagnostic of the device math; no reference counterpart. */
 bit_status bit_device_fp64_math_error(bit_ctx* ctx, long long n, double* exp_ulps,
                                       double* rsqrt_ulps);
 

@@ -1,5 +1,6 @@
 """The FP64 near field's own exp and rsqrt (bit_b200/csrc/fp64math.cuh) against CUDA's on the
-device, over 4M seeded arguments each: exp on [-707, 0], rsqrt on [1e-12, 1e6]."""
+device, over 4M seeded arguments each: exp on [-707, 0] (and its small-argument form on
+(-8, 0]), rsqrt on [1e-12, 1e6]."""
 import pytest
 
 
