@@ -1,5 +1,5 @@
 """The generated far-field recurrences (bit_b200/csrc/gen_farfield.py), run in FP64 on the
-CPU: the scaled forms the FP32 kernels use (coefficients times R^(|v|+1), moments
+CPU: the scaled forms the kernels use (coefficients times R^(|v|+1), moments
 normalised by h^|v|, shells folded in with (h/R)^n / R) are the same function as the
 literal form of the reference's recurrence, so the two agree to rounding for every
 nterms and both kernels.  Also pins the per-pair flop counts behind the bench's roofline.
@@ -60,6 +60,7 @@ def test_scaled_recurrences_equal_the_literal_ones(nt):
     sc_c = compile_lines(g.gen_coulomb_scaled(nt), ["dx", "dy", "dz", "rs", "h", "M"])
     lit_s = compile_lines(g.gen_screened(nt), ["dx", "dy", "dz", "dist2", "kappa", "M"])
     sc_s = compile_lines(g.gen_screened_scaled(nt), ["dx", "dy", "dz", "dist2", "kappa", "h", "M"])
+    sp_s = compile_lines(g.gen_screened_scaled_plain(nt), ["dx", "dy", "dz", "dist2", "kappa", "h", "M"])
     deg = shell_degrees(g, nt)
     rng = np.random.default_rng(nt)
     for _ in range(20):
@@ -77,6 +78,8 @@ def test_scaled_recurrences_equal_the_literal_ones(nt):
         for kappa in (0.5, 3.0):
             a, b = lit_s(*d, r2, kappa, M), sc_s(*d, r2, kappa, h, Mn)
             assert abs(a - b) <= TOL * max(abs(a), 1e-300), (nt, kappa, a, b)
+            b = sp_s(*d, r2, kappa, h, Mn)
+            assert abs(a - b) <= TOL * max(abs(a), 1e-300), (nt, kappa, a, b)
 
 
 def test_flop_counts_behind_the_roofline():
@@ -86,4 +89,4 @@ def test_flop_counts_behind_the_roofline():
     assert g.flops_per_pair(9)["coulomb"] == 1459
     assert g.flops_per_pair(9)["screened"] == 2414
     assert g.count_flops(g.gen_coulomb_scaled(9)) < 1459
-    assert g.count_flops(g.gen_screened_scaled(9)) < 2414
+    assert g.count_flops(g.gen_screened_scaled(9)) < g.count_flops(g.gen_screened_scaled_plain(9)) < 2414
