@@ -162,10 +162,12 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
     for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
     // Both precisions run the scaled form of the reference's recurrence (fewer operations
     // than the literal one, the same function).  FP32 moments are normalised by h^|v|,
-    // h = 2^e; FP64 moments are the plain ones, i.e. h = 1.  The screened FP32 kernels
-    // take the form with per-pair products hoisted (886 fma + 189 mul per pair at nterms
-    // 9 against 886 + 447; 9.77 -> 9.09 ms at 2M clustered, p = 8, theta = 0.7); the FP64
-    // ones keep the plain form, since the hoisted one spilled there and ran 1% slower.
+    // h = 2^e; FP64 moments are the plain ones, i.e. h = 1.  The FP32 kernels take the
+    // forms with per-pair products hoisted (at nterms 9, screened: 886 fma + 189 mul per
+    // pair against 886 + 447, Coulomb: 572 + 68 against 572 + 123; at 2M clustered, p = 8,
+    // theta = 0.7: screened 9.77 -> 9.09 ms, Coulomb 6.41 -> 6.07 ms); the FP64
+    // ones keep the plain forms, since the hoisted screened one spilled there and ran 1%
+    // slower.
     const T h = sizeof(T) == 4 ? (T)ldexpf(1.f, mom32_scale_exp(c.w)) : T(1);
     __syncwarp();
     for (int r = lane; r < cnt; r += 32) {
@@ -173,9 +175,12 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
       const T dx = (T)(cx[i] - c.x), dy = (T)(cy[i] - c.y), dz = (T)(cz[i] - c.z);
       const T r2 = dx * dx + dy * dy + dz * dz + tadd;
       T v;
-      if (KER == BIT_KERNEL_COULOMB) v = FarField<NT>::template coulomb_s<T>(dx, dy, dz, r2, h, M);
-      else if (sizeof(T) == 4) v = FarField<NT>::template screened_s<T>(dx, dy, dz, r2, tk, h, M);
-      else v = FarField<NT>::template screened_sp<T>(dx, dy, dz, r2, tk, h, M);
+      if (sizeof(T) == 4)
+        v = KER == BIT_KERNEL_COULOMB ? FarField<NT>::template coulomb_s<T>(dx, dy, dz, r2, h, M)
+                                      : FarField<NT>::template screened_s<T>(dx, dy, dz, r2, tk, h, M);
+      else
+        v = KER == BIT_KERNEL_COULOMB ? FarField<NT>::template coulomb_sp<T>(dx, dy, dz, r2, h, M)
+                                      : FarField<NT>::template screened_sp<T>(dx, dy, dz, r2, tk, h, M);
       WarpAcc<T>::add(row, i, v);
     }
     __syncwarp();

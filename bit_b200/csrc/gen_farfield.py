@@ -252,8 +252,10 @@ class ShellSum:
         self.L.append("  return s;")
 
 
-def coul_scaled_expr(v):
+def coul_scaled_expr(v, hs=None):
+    """hs: a Hoisted whose (2 - 1/i) u_a products replace the literal multiplies."""
     b = lambda w: "E" if w == (0, 0, 0) else name("B", w)
+    axis = lambda a, i: (f"{U(a)}, {lit(2.0 - 1.0 / i)}*" if hs is None else f"{hs.uc(a, i)}, ")
     U = lambda a: "u" + AX[a]
     U2 = lambda a: "u" + AX[a] + "2"
     nz, n1, ax = classify(v)
@@ -262,7 +264,7 @@ def coul_scaled_expr(v):
         if k == 1:
             return U(u)
         ik = 1.0 / k
-        return f"fma_t({U(u)}, {lit(2.0 - ik)}*{b(sub(v, u, 1))}, -({lit(1 - ik)}*{b(sub(v, u, 2))}))"
+        return f"fma_t({axis(u, k)}{b(sub(v, u, 1))}, -({lit(1 - ik)}*{b(sub(v, u, 2))}))"
     if nz == 1 and n1 == 2:
         u, w = ax
         return _chain(None, [(U(u), b(sub(v, u, 1))), (U2(w), b(sub(v, w, 1)))])
@@ -271,7 +273,7 @@ def coul_scaled_expr(v):
         ii = 1.0 / v[u]
         e = f"fma_t({lit(-(1 - ii))}, {b(sub(v, u, 2))}, -{b(sub(v, w, 2))})"
         e = _chain(e, [(U2(w), b(sub(v, w, 1)))])
-        return f"fma_t({U(u)}, {lit(2.0 - ii)}*{b(sub(v, u, 1))}, {e})"
+        return f"fma_t({axis(u, v[u])}{b(sub(v, u, 1))}, {e})"
     if n1 >= 1:
         f = next(a for a in range(3) if v[a] == 1)
         subs = [b(sub(v, a, 2)) for a in range(3) if a != f and v[a] >= 2]
@@ -281,24 +283,28 @@ def coul_scaled_expr(v):
     ii = 1.0 / v[0]
     e = f"fma_t({lit(-(1.0 - ii))}, {b(sub(v, 0, 2))}, -({b(sub(v, 1, 2))} + {b(sub(v, 2, 2))}))"
     e = _chain(e, [("uy2", b(sub(v, 1, 1))), ("uz2", b(sub(v, 2, 1)))])
-    return f"fma_t(ux, {lit(2.0 - ii)}*{b(sub(v, 0, 1))}, {e})"
+    return f"fma_t({axis(0, v[0])}{b(sub(v, 0, 1))}, {e})"
 
 
-def gen_coulomb_scaled(nt):
+def gen_coulomb_scaled(nt, hoisted=True):
+    """hoisted: the (2 - 1/i) u_a products formed once per pair (the FP32 kernels); else
+    the literal multiplies in place (the FP64 kernels, which hold more registers)."""
     mi = shell_index(nt)
-    L = ["  const T rinv = rsqrt_t(rs);",
-         "  const T ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;",
-         "  const T ux2 = ux + ux, uy2 = uy + uy, uz2 = uz + uz;",
-         "  const T eta = h * rinv;",
-         "  const T E = T(1);",
-         "  T q = rinv, S;"]
+    head = ["  const T rinv = rsqrt_t(rs);",
+            "  const T ux = dx * rinv, uy = dy * rinv, uz = dz * rinv;",
+            "  const T ux2 = ux + ux, uy2 = uy + uy, uz2 = uz + uz;",
+            "  const T eta = h * rinv;",
+            "  const T E = T(1);",
+            "  T q = rinv, S;"]
+    hs = Hoisted() if hoisted else None
+    L = []
     sh = ShellSum(L, mi)
     for v in shells(nt - 1):
         if v != (0, 0, 0):
-            L.append(f"  const T {name('B', v)} = {coul_scaled_expr(v)};")
+            L.append(f"  const T {name('B', v)} = {coul_scaled_expr(v, hs)};")
         sh.add(v, "E" if v == (0, 0, 0) else name("B", v))
     sh.done()
-    return L
+    return head + (hs.place(L) if hs else L)
 
 
 def scr_scaled_expr(v):
@@ -331,17 +337,9 @@ def scr_scaled_expr(v):
     return cexp, e
 
 
-class ScreenedScaled:
-    """The scaled screened recurrence with its per-pair products hoisted.
-
-    Every pattern of the recurrence is a sum of (factor, coefficient) products whose
-    factors are u_a, 2 u_a, kappa-scaled u (ku_a = rho u_a), rho, and literals 1/i,
-    2 - 1/i, 1 - 1/i.  Products of a pair factor and a literal (e.g. (1/i) ku_a, the
-    (2 - 1/i) u_a of the axis term) are formed once per pair ("hoisted"), so each term
-    of a pattern costs one fma.  A coefficient c~_w that is a single product ku_g a~_{w-g}
-    (w has a component equal to 1; g the first such axis) is never formed: its consumers
-    take ku_f ku_g (or (1/i) ku_f ku_g, (1/i) rho ku_g) times a~_{w-g} instead.  At
-    nterms 9 this takes the pair from 886 fma + 447 mul to about 1,100 operations."""
+class Hoisted:
+    """Products of per-pair factors and literals, formed once per pair and placed where
+    they are first needed."""
 
     def __init__(self):
         self.pre = {}
@@ -389,6 +387,22 @@ class ScreenedScaled:
             out.append(ln)
         return out
 
+    def uc(self, a, i):
+        return self.hoist(f"uc{AX[a]}_{i}", f"{lit(2.0 - 1.0 / i)}*u{AX[a]}")
+
+
+class ScreenedScaled(Hoisted):
+    """The scaled screened recurrence with its per-pair products hoisted.
+
+    Every pattern of the recurrence is a sum of (factor, coefficient) products whose
+    factors are u_a, 2 u_a, kappa-scaled u (ku_a = rho u_a), rho, and literals 1/i,
+    2 - 1/i, 1 - 1/i.  Products of a pair factor and a literal (e.g. (1/i) ku_a, the
+    (2 - 1/i) u_a of the axis term) are formed once per pair ("hoisted"), so each term
+    of a pattern costs one fma.  A coefficient c~_w that is a single product ku_g a~_{w-g}
+    (w has a component equal to 1; g the first such axis) is never formed: its consumers
+    take ku_f ku_g (or (1/i) ku_f ku_g, (1/i) rho ku_g) times a~_{w-g} instead.  At
+    nterms 9 this takes the pair from 886 fma + 447 mul to about 1,100 operations."""
+
     @staticmethod
     def A(w):
         return "E" if w == (0, 0, 0) else name("A", w)
@@ -414,8 +428,6 @@ class ScreenedScaled:
     def rc(self, i):
         return self.hoist(f"rc_{i}", f"{lit(1.0 / i)}*rho")
 
-    def uc(self, a, i):
-        return self.hoist(f"uc{AX[a]}_{i}", f"{lit(2.0 - 1.0 / i)}*u{AX[a]}")
 
     def cterm(self, mult, w):
         """(factor, coefficient) of `mult` * c~_w; mult is ("k", a) for ku_a,
@@ -726,6 +738,10 @@ def main(out):
         parts.append("  template <class T> static __device__ __forceinline__ T coulomb_s("
                      "T dx, T dy, T dz, T rs, T h, const T* __restrict__ M) {")
         parts += gen_coulomb_scaled(nt)
+        parts.append("  }")
+        parts.append("  template <class T> static __device__ __forceinline__ T coulomb_sp("
+                     "T dx, T dy, T dz, T rs, T h, const T* __restrict__ M) {")
+        parts += gen_coulomb_scaled(nt, hoisted=False)
         parts.append("  }")
         parts.append("  template <class T> static __device__ __forceinline__ T screened_s("
                      "T dx, T dy, T dz, T dist2, T kappa, T h, const T* __restrict__ M) {")

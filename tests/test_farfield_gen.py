@@ -58,6 +58,7 @@ def test_scaled_recurrences_equal_the_literal_ones(nt):
     g = gen()
     lit_c = compile_lines(g.gen_coulomb(nt), ["dx", "dy", "dz", "rs", "M"])
     sc_c = compile_lines(g.gen_coulomb_scaled(nt), ["dx", "dy", "dz", "rs", "h", "M"])
+    sp_c = compile_lines(g.gen_coulomb_scaled(nt, hoisted=False), ["dx", "dy", "dz", "rs", "h", "M"])
     lit_s = compile_lines(g.gen_screened(nt), ["dx", "dy", "dz", "dist2", "kappa", "M"])
     sc_s = compile_lines(g.gen_screened_scaled(nt), ["dx", "dy", "dz", "dist2", "kappa", "h", "M"])
     sp_s = compile_lines(g.gen_screened_scaled_plain(nt), ["dx", "dy", "dz", "dist2", "kappa", "h", "M"])
@@ -75,6 +76,8 @@ def test_scaled_recurrences_equal_the_literal_ones(nt):
         for reg in (0.0, 1e-4):
             a, b = lit_c(*d, r2 + reg, M), sc_c(*d, r2 + reg, h, Mn)
             assert abs(a - b) <= TOL * max(abs(a), 1e-300), (nt, a, b)
+            b = sp_c(*d, r2 + reg, h, Mn)
+            assert abs(a - b) <= TOL * max(abs(a), 1e-300), (nt, a, b)
         for kappa in (0.5, 3.0):
             a, b = lit_s(*d, r2, kappa, M), sc_s(*d, r2, kappa, h, Mn)
             assert abs(a - b) <= TOL * max(abs(a), 1e-300), (nt, kappa, a, b)
@@ -88,5 +91,5 @@ def test_flop_counts_behind_the_roofline():
     g = gen()
     assert g.flops_per_pair(9)["coulomb"] == 1459
     assert g.flops_per_pair(9)["screened"] == 2414
-    assert g.count_flops(g.gen_coulomb_scaled(9)) < 1459
+    assert g.count_flops(g.gen_coulomb_scaled(9)) < g.count_flops(g.gen_coulomb_scaled(9, False)) < 1459
     assert g.count_flops(g.gen_screened_scaled(9)) < g.count_flops(g.gen_screened_scaled_plain(9)) < 2414
