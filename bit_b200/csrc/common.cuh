@@ -257,10 +257,15 @@ struct Tree {
   DBuf<float> mom32;
   std::vector<long long> h_mom_off;  // first moment of each node (systems may differ in nterms)
   DBuf<long long> mom_off;
+  // the same moments in the far field's shell order, each node's block padded with zeros to
+  // a multiple of 4 (16-byte aligned blocks, copied whole into shared memory by TMA)
+  DBuf<double> msh64;
+  DBuf<float> msh32;
+  DBuf<long long> msh_off;
   // moment work plan: (node, first, last) member chunks and per-chunk partial sums
   long long mplan_gen = -1;
   int mplan_nch = 0;
-  long long mom_total = 0;
+  long long mom_total = 0, msh_total = 0;
   std::vector<int> mplan_cls;  // chunk range of each nterms class
   DBuf<int4> mplan_chunks;
   DBuf<int> mplan_c0, mplan_c1, mplan_T;

@@ -3,15 +3,17 @@
 // one CTA per target group.
 //
 // The CTA's warps take the group's far entries round-robin.  A warp packs the targets of
-// its entry (the set bits of the entry's mask) into a dense list and its lanes run the
-// unrolled recurrence (generated per nterms by gen_farfield.py) for one target each,
-// against the cluster's moments (warp-uniform loads).  Each warp accumulates into its own
+// its entry (the set bits of the entry's mask) into a dense list while a TMA bulk copy
+// brings the cluster's moments (a padded shell-order block, no multicast) into the warp's
+// shared-memory slot, and its lanes run the unrolled recurrence (generated per nterms by
+// gen_farfield.py) for one target each, against those moments (warp-uniform loads).  Each warp accumulates into its own
 // shared-memory row; rows are summed in warp order at the end, so the result does not
 // depend on timing.  The target-centre offset is formed in FP64; the mixed path rounds it
 // once to FP32 and runs recurrence and dot product in FP32, accumulating with two-sum.
 #include <algorithm>
 
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace bit {
 // Precision-generic math used by the generated recurrences.
@@ -57,6 +59,9 @@ struct FarArgs {
   const double4* nodec;
   const void* mom;  // float or double, T(nterms of the node's system) per node
   const long long* mom_off;  // first moment of each node
+  const void* msh;           // the same in shell order, padded blocks (potential kernels)
+  const long long* msh_off;  // first element of each node's block
+  int* err;                  // device error flags (a bounded wait that gave up: 8)
   const SysEval* sys;        // per system: far_add, kappa, far_sign
   const int* g_sys;          // per group: system
   double *out, *out_y, *out_z;
@@ -123,9 +128,12 @@ constexpr int NWF = 4;  // warps per CTA, force (three accumulators)
 // The far field of one target group g (the CTA's whole work for that group).  Shared
 // memory: the group's target coordinates, per warp a packed target list, an accumulator row
 // and one cluster's moments (NW * TP of them; a kernel running several orders sizes this for
-// the largest).
+// the largest).  bar: one mbarrier per warp, phase: this warp's count of its completed
+// copies.  Returns false (in every thread) if a warp's bounded wait for its moments gave up:
+// the error flag is set, the warp has waited (bounded again) for that copy, and the group's
+// result is not valid.
 template <int NT, int KER, class T, int NW>
-__device__ __forceinline__ void far_group(const FarArgs& a, int g) {
+__device__ __forceinline__ bool far_group(const FarArgs& a, int g, uint64_t* bar, unsigned& phase) {
   constexpr int TT = num_terms(NT);
   constexpr int TP = FarField<NT>::kPadded;
   extern __shared__ __align__(16) unsigned char sm[];
@@ -148,18 +156,37 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
   __syncthreads();
   unsigned short* tl = tlb + w * kGroupMax;
   T* row = accb + w * ROW;
-  const T* mom = reinterpret_cast<const T*>(a.mom);
+  const T* msh = reinterpret_cast<const T*>(a.msh);
   const SysEval* se = a.sys + a.g_sys[g];
   const T tadd = (T)se->far_add, tk = (T)se->kappa;
   const double sign = se->far_sign;
+  bool failed = false;
   for (long long e = e0 + w; e < e1; e += NW) {
+    const int node = a.node[e];
+    T* M = msb + w * TP;
+    // The cluster's moments, its whole padded shell-order block (TP values, 16-byte aligned
+    // in global and shared memory), by one TMA bulk copy into the warp's slot while the
+    // warp packs the entry's targets.  The previous entry's reads of the slot ended at the
+    // __syncwarp closing its loop.
+    if (lane == 0) {
+      fence_proxy_async();
+      mbar_expect_tx(&bar[w], TP * (unsigned)sizeof(T));
+      tma_load_1d(M, msh + a.msh_off[node], TP * (unsigned)sizeof(T), &bar[w]);
+    }
     const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
     const int cnt = warp_pack(wd, tl);
-    const int node = a.node[e];
     const double4 c = a.nodec[node];
-    T* M = msb + w * TP;
-    const T* mn = mom + a.mom_off[node];
-    for (int k = lane; k < TP; k += 32) M[k] = k < TT ? mn[FarField<NT>::canon(k)] : T(0);
+    const bool landed = __all_sync(0xffffffffu, mbar_wait(&bar[w], phase & 1));
+    phase++;
+    if (!landed) {
+      if (lane == 0) {
+        atomicOr(a.err, 8);
+        mbar_wait(&bar[w], (phase - 1) & 1);
+      }
+      __syncwarp();
+      failed = true;
+      break;
+    }
     // Both precisions run the scaled form of the reference's recurrence (fewer operations
     // than the literal one, the same function).  FP32 moments are normalised by h^|v|,
     // h = 2^e; FP64 moments are the plain ones, i.e. h = 1.  The FP32 kernels take the
@@ -185,18 +212,32 @@ __device__ __forceinline__ void far_group(const FarArgs& a, int g) {
     }
     __syncwarp();
   }
-  __syncthreads();
+  if (__syncthreads_or(failed)) return false;
   for (int i = tid; i < tc; i += 32 * NW) {
     double s = 0.0;
     for (int q = 0; q < NW; q++) s += WarpAcc<T>::get(accb + q * ROW, i);
     a.out[t0 + i] = sign * s;
+  }
+  return true;
+}
+
+// One mbarrier per warp for the moment copies, initialised before the kernel's first
+// __syncthreads.
+template <int NW>
+__device__ __forceinline__ void far_bars_init(uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < NW; k++) mbar_init(&bar[k], 1);
+    fence_mbar_init();
   }
 }
 
 // One launch class: CTA b takes group order[b].
 template <int NT, int KER, class T, int NW>
 __global__ void __launch_bounds__(32 * NW, min_blocks<T>(NW)) k_far(FarArgs a) {
-  far_group<NT, KER, T, NW>(a, a.order[blockIdx.x]);
+  __shared__ uint64_t bar[NW];
+  far_bars_init<NW>(bar);
+  unsigned phase = 0;
+  far_group<NT, KER, T, NW>(a, a.order[blockIdx.x], bar, phase);
 }
 
 // Persistent work queue over the groups of every class: each CTA takes the next item
@@ -208,6 +249,9 @@ template <class T, int NW>
 __global__ void __launch_bounds__(32 * NW, min_blocks<T>(NW))
     k_far_queue(FarArgs a, int count, int* head) {
   __shared__ int s_item;
+  __shared__ uint64_t bar[NW];
+  far_bars_init<NW>(bar);
+  unsigned phase = 0;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(head, 1);
     __syncthreads();
@@ -217,17 +261,19 @@ __global__ void __launch_bounds__(32 * NW, min_blocks<T>(NW))
     const int g = a.order[item];
     const SysEval* se = a.sys + a.g_sys[g];
     const bool coul = se->kernel == BIT_KERNEL_COULOMB;
+    bool ok = true;
     switch (se->nterms) {
-#define FQ(N)                                                           \
-  case N:                                                               \
-    if (coul) far_group<N, BIT_KERNEL_COULOMB, T, NW>(a, g);            \
-    else far_group<N, BIT_KERNEL_SCREENED, T, NW>(a, g);                \
+#define FQ(N)                                                                   \
+  case N:                                                                       \
+    ok = coul ? far_group<N, BIT_KERNEL_COULOMB, T, NW>(a, g, bar, phase)       \
+              : far_group<N, BIT_KERNEL_SCREENED, T, NW>(a, g, bar, phase);     \
     break;
       FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10)
 #undef FQ
       default:
         break;
     }
+    if (!ok) return;  // a bounded wait gave up (every thread saw it): take no more items
     __syncthreads();  // the group's last reads of shared memory precede the next group's writes
   }
 }
@@ -349,6 +395,9 @@ FarArgs far_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const d
   a.nodec = t->nodec.p;
   a.mom = P.f32 ? (const void*)t->mom32.p : (const void*)t->mom64.p;
   a.mom_off = t->mom_off.p;
+  a.msh = P.f32 ? (const void*)t->msh32.p : (const void*)t->msh64.p;
+  a.msh_off = t->msh_off.p;
+  a.err = t->ctx->dev_err();
   a.sys = P.sys.p;
   a.g_sys = L->g_sys.p;
   return a;

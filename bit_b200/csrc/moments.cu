@@ -122,6 +122,18 @@ __device__ int canon_degree(int t, int nt) {
   return i + j + t;
 }
 
+// Position of canonical moment index t in the far field's shell order: by degree d, then i
+// descending, then j descending (the order gen_farfield.py's recurrences produce their
+// coefficients in): the C(d + 2, 3) terms of lower degree, then (d - i)(d - i + 1) / 2 for
+// the larger i of degree d, then d - i - j.
+__device__ int canon_shell_pos(int t, int nt) {
+  int i = 0, j = 0;
+  for (; t >= (nt - i) * (nt - i + 1) / 2; i++) t -= (nt - i) * (nt - i + 1) / 2;
+  for (; t >= nt - i - j; j++) t -= nt - i - j;
+  const int d = i + j + t;
+  return d * (d + 1) * (d + 2) / 6 + (d - i) * (d - i + 1) / 2 + (d - i - j);
+}
+
 constexpr int kReduceSlices = 4;  // chunk-sum slices per term (a top node has ~n/1024 chunks)
 
 // Per node: the sum of its chunks' partials.  Slice k of term t sums chunks c0 + k,
@@ -131,8 +143,9 @@ constexpr int kReduceSlices = 4;  // chunk-sum slices per term (a top node has ~
 // exponent shift).
 __global__ void __launch_bounds__(256 * kReduceSlices)
     k_moments_reduce(const int* node_c0, const int* node_c1, const int* node_T,
-                     const long long* mom_off, const double4* nodec, const double* part,
-                     double* mom64, float* mom32) {
+                     const long long* mom_off, const long long* msh_off, const double4* nodec,
+                     const double* part, double* mom64, float* mom32, double* msh64,
+                     float* msh32) {
   constexpr int TMAX = num_terms(kNtermsMax);
   static_assert(TMAX <= 256, "one slice of 256 threads covers every term");
   __shared__ double s_part[kReduceSlices][256];
@@ -145,14 +158,23 @@ __global__ void __launch_bounds__(256 * kReduceSlices)
     s_part[slice][t] = s;
   }
   __syncthreads();
-  if (slice != 0 || t >= T) return;
+  if (slice != 0) return;
+  const long long so = msh_off[node];
+  if (t >= T) {
+    if (t < (T + 3) / 4 * 4) { msh64[so + t] = 0.0; msh32[so + t] = 0.f; }  // block padding
+    return;
+  }
   double s = s_part[0][t];
   for (int k = 1; k < kReduceSlices; k++) s += s_part[k][t];
   int nt = 1;
   while (num_terms(nt) < T) nt++;
   const long long o = mom_off[node];
+  const float s32 = (float)ldexp(s, -mom32_scale_exp(nodec[node].w) * canon_degree(t, nt));
   mom64[o + t] = s;
-  mom32[o + t] = (float)ldexp(s, -mom32_scale_exp(nodec[node].w) * canon_degree(t, nt));
+  mom32[o + t] = s32;
+  const int p = canon_shell_pos(t, nt);
+  msh64[so + p] = s;
+  msh32[so + p] = s32;
 }
 
 __global__ void k_gather_charges(int n, const int* perm, const double* q, const double* w,
@@ -220,10 +242,11 @@ void tree_moments_sys(Tree* t, const std::vector<int>& nt_sys) {
     // chunks of every node, grouped by the node's nterms (one launch per distinct nterms)
     const int nn = t->numtree;
     std::vector<int> c0(nn), c1(nn), nodeT(nn);
-    std::vector<long long> off(nn + 1, 0);
+    std::vector<long long> off(nn + 1, 0), soff(nn + 1, 0);
     for (int i = 0; i < nn; i++) {
       nodeT[i] = num_terms(nt_sys[t->h_node_sys[i]]);
       off[i + 1] = off[i] + nodeT[i];
+      soff[i + 1] = soff[i] + (nodeT[i] + 3) / 4 * 4;
     }
     std::vector<int4> ck;
     std::vector<int> cls_begin(kNtermsMax + 2, 0);
@@ -243,16 +266,19 @@ void tree_moments_sys(Tree* t, const std::vector<int>& nt_sys) {
     t->mplan_nch = (int)ck.size();
     t->h_mom_off.assign(off.begin(), off.end() - 1);
     t->mom_total = off[nn];
+    t->msh_total = soff[nn];
     t->mplan_chunks.ensure(c, ck.size());
     t->mplan_c0.ensure(c, nn);
     t->mplan_c1.ensure(c, nn);
     t->mplan_T.ensure(c, nn);
     t->mom_off.ensure(c, nn);
+    t->msh_off.ensure(c, nn);
     BIT_CUDA(cudaMemcpyAsync(t->mplan_chunks.p, ck.data(), ck.size() * sizeof(int4), cudaMemcpyHostToDevice, s));
     BIT_CUDA(cudaMemcpyAsync(t->mplan_c0.p, c0.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
     BIT_CUDA(cudaMemcpyAsync(t->mplan_c1.p, c1.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
     BIT_CUDA(cudaMemcpyAsync(t->mplan_T.p, nodeT.data(), nn * sizeof(int), cudaMemcpyHostToDevice, s));
     BIT_CUDA(cudaMemcpyAsync(t->mom_off.p, t->h_mom_off.data(), nn * sizeof(long long), cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaMemcpyAsync(t->msh_off.p, soff.data(), nn * sizeof(long long), cudaMemcpyHostToDevice, s));
     BIT_CUDA(cudaStreamSynchronize(s));
     t->mplan_gen = t->gen;
     t->h_sys_nterms = nt_sys;
@@ -260,6 +286,8 @@ void tree_moments_sys(Tree* t, const std::vector<int>& nt_sys) {
   t->mplan_part.ensure(c, (size_t)t->mplan_nch * TMAX);
   t->mom64.ensure(c, t->mom_total);
   t->mom32.ensure(c, t->mom_total);
+  t->msh64.ensure(c, t->msh_total);
+  t->msh32.ensure(c, t->msh_total);
   for (int k = 1; k <= kNtermsMax; k++) {
     const int b0 = t->mplan_cls[k], b1 = t->mplan_cls[k + 1];
     if (b1 == b0) continue;
@@ -271,9 +299,9 @@ void tree_moments_sys(Tree* t, const std::vector<int>& nt_sys) {
     }
   }
   count_launch(), k_moments_reduce<<<t->numtree, 256 * kReduceSlices, 0, s>>>(t->mplan_c0.p, t->mplan_c1.p, t->mplan_T.p,
-                                                              t->mom_off.p, t->nodec.p,
+                                                              t->mom_off.p, t->msh_off.p, t->nodec.p,
                                                               t->mplan_part.p, t->mom64.p,
-                                                              t->mom32.p);
+                                                              t->mom32.p, t->msh64.p, t->msh32.p);
   BIT_CHECK_LAUNCH();
   int mx = 0;
   for (int v : nt_sys) mx = std::max(mx, v);
