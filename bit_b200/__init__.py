@@ -170,6 +170,7 @@ SIGNATURES = [
     ("bit_device_fma_peak", C.c_int, [_vp, C.c_int, C.POINTER(C.c_double)]),
     ("bit_device_fp64_math_error", C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double),
                                              C.POINTER(C.c_double)]),
+    ("bit_device_wait_check", C.c_int, [_vp, C.c_int]),
     ("bit_tree_target_lists", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _ip, _ip, C.c_int,
                                         _ip]),
     ("bit_bie_solve", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, C.c_double, _dp, _dp, _dp,
@@ -319,6 +320,11 @@ class Context:
         self.check(lib().bit_device_fp64_math_error(self.h, n, C.byref(e), C.byref(r)),
                    "bit_device_fp64_math_error")
         return {"exp": e.value, "rsqrt": r.value}
+
+    def wait_check(self, limit=1000):
+        """Run the device-side give-up path of a bounded wait (a barrier nothing
+        completes); returns the status (BIT_ERR_CUDA when the wait gave up, as it must)."""
+        return lib().bit_device_wait_check(self.h, limit)
 
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()

@@ -906,6 +906,16 @@ bit_status bit_device_fp64_math_error(bit_ctx* h, long long n, double* exp_ulps,
   });
 }
 
+bit_status bit_device_wait_check(bit_ctx* h, int limit) {
+  if (!h || limit < 1) return BIT_ERR_INVALID_ARGUMENT;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    device_wait_check(c, limit);
+    check_dev_err(c);
+  });
+}
+
 bit_status bit_tree_stats(const bit_tree* th, bit_stats* st) {
   if (!th || !st) return BIT_ERR_INVALID_ARGUMENT;
   Tree* t = const_cast<Tree*>(&th->t);

@@ -168,6 +168,7 @@ struct Lists {
   DBuf<int> far_node, near_node;            // entry -> node
   DBuf<unsigned> far_mask, near_mask;       // (tcount+31)/32 words per entry
   DBuf<int> order;                          // groups by decreasing work
+  DBuf<int> far_cost;                       // far field scratch: targets of each far entry
   std::vector<long long> h_work;            // estimated work of each group
   long long version = 0;                    // bumped by every build
   ListSizing last;                          // the last build's sizes
@@ -318,6 +319,7 @@ void eval_near_force(Tree* t, Lists* L, const EvalPlan& P, double* fx, double* f
 // Measured FMA throughput of the context's device, flop/s (2 per FMA), FP32 or FP64.
 double fma_peak(Ctx* c, bool f32);
 void fp64_math_error(Ctx* c, long long n, double* exp_ulps, double* rsqrt_ulps);
+void device_wait_check(Ctx* c, int limit);
 // FP64 field direct sum at m particle targets tg (device pointers); out = fx | fy | fz.
 void direct_field(Ctx* c, int n, const double* x, const double* y, const double* z,
                   const double* q, int regularised, double del, int korder, int m,

@@ -62,6 +62,7 @@ struct FarArgs {
   const void* msh;           // the same in shell order, padded blocks (potential kernels)
   const long long* msh_off;  // first element of each node's block
   int* err;                  // device error flags (a bounded wait that gave up: 8)
+  int* cost;                 // scratch, one int per far entry: its number of targets
   const SysEval* sys;        // per system: far_add, kappa, far_sign
   const int* g_sys;          // per group: system
   double *out, *out_y, *out_z;
@@ -161,7 +162,36 @@ __device__ __forceinline__ bool far_group(const FarArgs& a, int g, uint64_t* bar
   const T tadd = (T)se->far_add, tk = (T)se->kappa;
   const double sign = se->far_sign;
   bool failed = false;
+  // Each warp takes a contiguous run of the group's entries holding about 1/NW of its
+  // (target, cluster) pairs: the entries whose exclusive prefix P of target counts has
+  // w C <= NW P < (w + 1) C, C the group's total.  The entries' costs vary widely, so the
+  // round-robin deal this replaces left warps idle at the group's closing barrier.  The
+  // split depends on the lists only, so results stay deterministic.
   for (long long e = e0 + w; e < e1; e += NW) {
+    const unsigned wd = lane < W ? a.mask[m0 + (e - e0) * W + lane] : 0u;
+    const int c = __reduce_add_sync(0xffffffffu, __popc(wd));
+    if (lane == 0) a.cost[e] = c;
+  }
+  __syncthreads();
+  long long tot = 0;
+  for (long long b = e0; b < e1; b += 32)
+    tot += __reduce_add_sync(0xffffffffu, b + lane < e1 ? __ldcg(a.cost + b + lane) : 0);
+  long long run = 0;
+  int eb = 0, ee = 0;
+  for (long long b = e0; b < e1; b += 32) {
+    const bool in = b + lane < e1;
+    const int c = in ? __ldcg(a.cost + b + lane) : 0;
+    int inc = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const long long P = (run + inc - c) * NW;
+    eb += __popc(__ballot_sync(0xffffffffu, in && P < w * tot));
+    ee += __popc(__ballot_sync(0xffffffffu, in && P < (w + 1) * tot));
+    run += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  for (long long e = e0 + eb; e < e0 + ee; e++) {
     const int node = a.node[e];
     T* M = msb + w * TP;
     // The cluster's moments, its whole padded shell-order block (TP values, 16-byte aligned
@@ -398,6 +428,8 @@ FarArgs far_args(Tree* t, Lists* L, const EvalPlan& P, const double* tx, const d
   a.msh = P.f32 ? (const void*)t->msh32.p : (const void*)t->msh64.p;
   a.msh_off = t->msh_off.p;
   a.err = t->ctx->dev_err();
+  L->far_cost.ensure(t->ctx, std::max(L->nfar, 1LL));
+  a.cost = L->far_cost.p;
   a.sys = P.sys.p;
   a.g_sys = L->g_sys.p;
   return a;

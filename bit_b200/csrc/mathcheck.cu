@@ -5,6 +5,7 @@
 // [1e-12, 1e6]).  A test holds both to a bound.
 #include "common.cuh"
 #include "fp64math.cuh"
+#include "tma.cuh"
 
 namespace bit {
 
@@ -42,7 +43,28 @@ __global__ void k_math_check(long long n, unsigned long long* worst) {
   atomicMax(worst + 1, (unsigned long long)__double_as_longlong(wr));
 }
 
+// The kernels' give-up path, exercised where no copy is in flight: an mbarrier that no
+// copy and no thread ever arrives at, waited on by every thread with the kernels' bounded
+// wait (at most `limit` attempts), the outcome combined for the CTA as the near field does,
+// and the error flag raised (16) when the wait gives up.
+__global__ void k_wait_check(int limit, int* err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const bool landed = mbar_wait(&bar, 0, limit);
+  if (__syncthreads_or(!landed) && threadIdx.x == 0) atomicOr(err, 16);
+}
+
 }  // namespace
+
+void device_wait_check(Ctx* c, int limit) {
+  count_launch(), k_wait_check<<<1, 128, 0, c->stream>>>(limit, c->dev_err());
+  BIT_CHECK_LAUNCH();
+  BIT_CUDA(cudaStreamSynchronize(c->stream));
+}
 
 void fp64_math_error(Ctx* c, long long n, double* exp_ulps, double* rsqrt_ulps) {
   cudaStream_t s = c->stream;

@@ -52,9 +52,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false if it never completed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (int it = 0; it < (1 << 20); it++)
+// Bounded wait for the phase with the given parity: at most `limit` try_wait attempts;
+// false if the phase never completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int limit = 1 << 20) {
+  for (int it = 0; it < limit; it++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -253,6 +253,15 @@ bit_status bit_device_fma_peak(bit_ctx* ctx, bit_precision prec, double* flops_p
 bit_status bit_device_fp64_math_error(bit_ctx* ctx, long long n, double* exp_ulps,
                                       double* rsqrt_ulps);
 
+/* The kernels' give-up path for a device-side wait, exercised on its own: one CTA waits,
+ * with the same bounded mbarrier wait the near and far fields use (at most `limit`
+ * attempts), on a barrier that nothing ever completes, combines the outcome for the CTA
+ * and raises the context's device error flag.  Returns BIT_ERR_CUDA ("a device-side wait
+ * gave up", flag 16) with the flag then cleared, so the context stays usable for later
+ * calls.  No copy is in flight, nothing faults and nothing hangs.  A diagnostic of the
+ * failure path; no reference counterpart. */
+bit_status bit_device_wait_check(bit_ctx* ctx, int limit);
+
 bit_status bit_tree_stats(const bit_tree* tree, bit_stats* st);
 
 /* Per-target interaction lists of the last evaluation, in the reference's traversal
