@@ -43,10 +43,24 @@ void ctx_trim(Ctx* c, size_t keep) {
   }
 }
 
+// Over the budget, a request is served from any larger cached block (it costs no memory),
+// and otherwise only as many cached blocks are freed, largest first, as the new block needs:
+// every cudaFree waits for the device, and freeing the whole cache for one small block
+// stalled served requests by hundreds of milliseconds.
+static void release_for(Ctx* c, size_t bytes) {
+  while (!c->cache.empty() && c->in_use + c->cached + bytes > c->budget) {
+    auto it = std::prev(c->cache.end());
+    cudaFree(it->second);
+    c->cached -= it->first;
+    c->cache.erase(it);
+  }
+}
+
 void* dev_alloc(Ctx* c, size_t bytes) {
   bytes = round_block(bytes);
   auto it = c->cache.lower_bound(bytes);
-  if (it != c->cache.end() && it->first <= 2 * bytes) {
+  const bool tight = c->budget && c->in_use + c->cached + bytes > c->budget;
+  if (it != c->cache.end() && (it->first <= 2 * bytes || tight)) {
     void* p = it->second;
     size_t sz = it->first;
     c->cache.erase(it);
@@ -56,7 +70,7 @@ void* dev_alloc(Ctx* c, size_t bytes) {
     c->allocs.push_back({p, sz});
     return p;
   }
-  if (c->budget && c->in_use + c->cached + bytes > c->budget) release_cache(c);
+  if (tight) release_for(c, bytes);
   if (c->budget && c->in_use + bytes > c->budget)
     fail(BIT_ERR_BUDGET, "allocation of " + std::to_string(bytes) + " bytes exceeds the HBM budget");
   void* p = nullptr;
