@@ -868,7 +868,7 @@ def main():
     ap.add_argument("--batched", type=int, default=2048, help="systems of the batched run (0: skip)")
     ap.add_argument("--serve-requests", type=int, default=120,
                     help="requests of the serving stream (0: skip)")
-    ap.add_argument("--serve-slots", type=int, default=4)
+    ap.add_argument("--serve-slots", type=int, default=8)
     ap.add_argument("--no-matched", dest="matched", action="store_false",
                     help="skip the accuracy-matched (1e-6 vs direct sum) runs")
     ap.add_argument("--no-tune", dest="tune", action="store_false",
