@@ -1,10 +1,11 @@
-// Host <-> device copies of caller (pageable) arrays.
+// Host <-> device copies of caller arrays.
 //
 // A pageable cudaMemcpy goes through the driver's own staging at ~20 GB/s on the B200
-// hosts, against ~53 GB/s for DMA from pinned memory.  Large copies therefore go through
-// two pinned chunks per context: the host-side copy of chunk k+1 into one chunk (split over
-// a few worker threads) overlaps the DMA of chunk k from the other.  Small copies stay
-// plain cudaMemcpyAsync.
+// hosts, against ~53 GB/s for DMA from pinned memory.  Large copies of pageable arrays
+// therefore go through two pinned chunks per context: the host-side copy of chunk k+1 into
+// one chunk (split over a few worker threads) overlaps the DMA of chunk k from the other.
+// Arrays the caller has page-locked (cudaHostAlloc, cudaHostRegister, a pinned tensor) are
+// copied by DMA directly, with no staging.  Small copies stay plain cudaMemcpyAsync.
 #include <condition_variable>
 #include <cstring>
 #include <functional>
@@ -103,12 +104,28 @@ void ensure_stage(Ctx* c) {
   }
 }
 
+// The host array is page-locked memory the device can DMA from or to.
+bool host_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
 
 void copy_h2d(Ctx* c, void* dst, const void* src, size_t bytes) {
   cudaStream_t s = c->stream;
   if (bytes < kDirectBelow) {
     BIT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    return;
+  }
+  if (host_pinned(src)) {
+    // DMA straight from the caller's array; it may be reused once the copy is done
+    BIT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+    BIT_CUDA(cudaStreamSynchronize(s));
     return;
   }
   ensure_stage(c);
@@ -127,7 +144,7 @@ void copy_h2d(Ctx* c, void* dst, const void* src, size_t bytes) {
 
 void copy_d2h(Ctx* c, void* dst, const void* src, size_t bytes) {
   cudaStream_t s = c->stream;
-  if (bytes < kDirectBelow) {
+  if (bytes < kDirectBelow || host_pinned(dst)) {
     BIT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
     BIT_CUDA(cudaStreamSynchronize(s));
     return;

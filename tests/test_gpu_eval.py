@@ -425,3 +425,34 @@ def test_near_config_keeps_results(orc, tile, split):
                 c.set_near_config(*bad)
     finally:
         c.close()
+
+
+def test_pinned_host_arrays_give_the_same_results(ctx):
+    """Page-locked caller arrays take the direct DMA path (copies of 4 MB and more), pageable
+    ones the staged path: the tree, its moments and the potentials are the same bit for bit,
+    into a pinned or a pageable result array."""
+    import torch
+    import bit_b200 as B
+    n = 600_000
+    rng = np.random.default_rng(7)
+    x, y, z, q = (rng.uniform(-1, 1, n) for _ in range(4))
+    keep = []
+
+    def pinned(a):
+        t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        keep.append(t)
+        arr = t.numpy()
+        arr[:] = a
+        return arr
+    p = B.params(B.SCREENED, B.CONSISTENT, B.FP64, kappa=1.0, acc=0.5)
+    t1 = ctx.treemake(x, y, z, 1000)
+    t1.treemoments(q, 5)
+    r1 = t1.evaluate(p)
+    t1.treeempty()
+    t2 = ctx.treemake(pinned(x), pinned(y), pinned(z), 1000)
+    t2.treemoments(pinned(q), 5)
+    out = pinned(np.zeros(n))
+    r2 = t2.evaluate(p, out=out)
+    t2.treeempty()
+    assert r2 is out
+    assert np.array_equal(r1, r2)
