@@ -624,9 +624,12 @@ __device__ __forceinline__ bool near_group(const NearArgs& a, int g) {
 }
 
 // One launch class: CTA b takes group order[b].  Potential kernels keep four CTAs per SM
-// (64 registers; the FP64 one chose 72 and three CTAs unconstrained, 4% slower at 2M).
+// (64 registers; the FP64 one chose 72 and three CTAs unconstrained, 4% slower at 2M),
+// except the mixed screened one, which runs three (85 registers): at 2M clustered, p = 8,
+// theta = 0.7, 6.43 -> 6.13 ms, while the mixed Coulomb one went 3.92 -> 4.26 ms with three.
 template <int KER, bool EPS, bool F32, bool FORCE>
-__global__ void __launch_bounds__(NT, FORCE ? 0 : 4) k_near(NearArgs a) {
+__global__ void __launch_bounds__(NT, FORCE ? 0 : ((F32 && KER == BIT_KERNEL_SCREENED) ? 3 : 4))
+    k_near(NearArgs a) {
   near_group<KER, EPS, F32, FORCE>(a, a.order[blockIdx.x]);
 }
 
