@@ -79,6 +79,12 @@ __device__ __forceinline__ bool alt_ok(const ListArgs& a, double s, double w) {
   return w < dmul(a.alt_acc, dsub(dadd(s, a.alt_add), a.alt_sub));
 }
 
+// Barrier `id` (1..15) among the first `nthreads` threads of the CTA (a multiple of 32);
+// barrier 0 is __syncthreads.
+__device__ __forceinline__ void bar_sync_n(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
 // The walk of group g by the whole CTA.  MODE_COUNT counts the group's entries, MODE_FILL
 // writes them at the offsets a scan gave, MODE_STAGE writes them into the CTA's staging
 // region and then copies them into room reserved with one atomic per list.
@@ -87,6 +93,8 @@ __device__ __forceinline__ void walk_group(const ListArgs& a, int g) {
   __shared__ unsigned s_mask[LSTK][32];  // each warp's mask word of every stack entry
   __shared__ unsigned s_am[2][32], s_rm[2][32];  // accept / reject words, by parity
   __shared__ unsigned long long s_base[4];
+  __shared__ int s_flags;  // the walk's overflow (1) / full staging (2), for every warp
+  __shared__ long long s_n[2];  // the walk's far and near entry counts, for every warp
   extern __shared__ unsigned dyn[];
   // dynamic shared memory: each warp's own copy of the node stack
   int (*s_node)[LSTK] = reinterpret_cast<int (*)[LSTK]>(dyn);
@@ -113,6 +121,12 @@ __device__ __forceinline__ void walk_group(const ListArgs& a, int g) {
     int live = tc - 32 * w;
     s_mask[0][w] = live >= 32 ? 0xffffffffu : (live > 0 ? (1u << live) - 1u : 0u);
   }
+  // warps without targets do not walk: their accept / reject words stay 0
+  if (threadIdx.x < 64) {
+    s_am[threadIdx.x >> 5][lane] = 0u;
+    s_rm[threadIdx.x >> 5][lane] = 0u;
+  }
+  if (threadIdx.x == 0) s_flags = 0;
   int sp = 1;
   long long nf = 0, nn = 0, fpairs = 0, npairs = 0;
   const long long fo = MODE == MODE_FILL ? a.far_off[g] : 0, no = MODE == MODE_FILL ? a.near_off[g] : 0;
@@ -123,9 +137,12 @@ __device__ __forceinline__ void walk_group(const ListArgs& a, int g) {
   // words.  Every warp pushes the same children onto its own stack (all threads see the
   // same children and the same CTA-wide decision), so no warp waits for another's push;
   // the words alternate between two buffers, so a fast warp never overwrites words a
-  // slow one is still reading (it cannot get two barriers ahead of it).
+  // slow one is still reading (it cannot get two barriers ahead of it).  Only the W warps
+  // that hold targets walk, on barrier 1 among their 32 W threads: they pop the same
+  // entries and take the same number of steps, while the others wait at the barrier after
+  // the walk (a group of 650 targets leaves 11 of the 32 warps idle).
   int par = 0;
-  while (sp > 0) {
+  while (w < W && sp > 0) {
     sp--;
     const int node = s_node[w][sp];
     const unsigned word = s_mask[sp][w];
@@ -141,7 +158,7 @@ __device__ __forceinline__ void walk_group(const ListArgs& a, int g) {
     const unsigned am = __ballot_sync(0xffffffffu, ok) & word;
     const unsigned rm = word & ~am;
     if (lane == 0) { s_am[par][w] = am; s_rm[par][w] = rm; }
-    __syncthreads();
+    bar_sync_n(1, 32 * W);
     const bool anyA = __ballot_sync(0xffffffffu, s_am[par][lane] != 0u) != 0u;
     const bool anyR = __ballot_sync(0xffffffffu, s_rm[par][lane] != 0u) != 0u;
     par ^= 1;
@@ -183,6 +200,17 @@ __device__ __forceinline__ void walk_group(const ListArgs& a, int g) {
     }
     __syncwarp();  // this warp's pushes, before its next pop
   }
+  // the walk's outcome and entry counts for every warp (thread 0's warp walked)
+  if (threadIdx.x == 0) {
+    if (overflow || full) s_flags = overflow ? 1 : 2;
+    s_n[0] = nf;
+    s_n[1] = nn;
+  }
+  __syncthreads();
+  overflow = s_flags == 1;
+  full = s_flags == 2;
+  nf = s_n[0];
+  nn = s_n[1];
   if (threadIdx.x == 0 && (overflow || full)) atomicOr(a.err, overflow ? 1 : 2);
   if (a.has_alt && __any_sync(0xffffffffu, differ) && lane == 0) atomicOr(a.err, 4);
   if (MODE != MODE_FILL && lane == 0 && (fpairs || npairs)) {
