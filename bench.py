@@ -341,6 +341,9 @@ def run_bit(args):
         if args.matched:
             line["accuracy_matched"]["batched"] = run_batched(ctx, args, dev, acc_by_nterms=MATCHED_BATCH_ACC)
     if args.serve_requests:
+        # the servers below get the device memory the batched runs left cached here
+        ctx.trim(0)
+        torch.cuda.empty_cache()
         line["serving"] = run_serving(ctx, args)
         if args.matched:
             line["accuracy_matched"]["serving"] = run_serving(ctx, args, matched=True)

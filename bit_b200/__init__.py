@@ -171,6 +171,7 @@ SIGNATURES = [
     ("bit_device_fp64_math_error", C.c_int, [_vp, C.c_longlong, C.POINTER(C.c_double),
                                              C.POINTER(C.c_double)]),
     ("bit_device_wait_check", C.c_int, [_vp, C.c_int]),
+    ("bit_ctx_trim", C.c_int, [_vp, C.c_size_t]),
     ("bit_tree_target_lists", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, _ip, _ip, C.c_int,
                                         _ip]),
     ("bit_bie_solve", C.c_int, [_vp, C.POINTER(EvalParams), C.c_int, C.c_double, _dp, _dp, _dp,
@@ -330,6 +331,10 @@ class Context:
         a, b = C.c_size_t(), C.c_size_t()
         lib().bit_ctx_memory(self.h, C.byref(a), C.byref(b))
         return a.value, b.value
+
+    def trim(self, keep=0):
+        """Free the context's cached device blocks until it holds at most `keep` bytes."""
+        self.check(lib().bit_ctx_trim(self.h, keep), "bit_ctx_trim")
 
     def set_group_size(self, targets):
         """Leaf packing (0: off, else 32..1024 targets per group): a tuning knob."""

@@ -340,6 +340,15 @@ bit_status bit_ctx_memory(const bit_ctx* h, size_t* in_use, size_t* peak) {
   return BIT_OK;
 }
 
+bit_status bit_ctx_trim(bit_ctx* h, size_t keep) {
+  if (!h) return BIT_ERR_INVALID_ARGUMENT;
+  Ctx* c = &h->c;
+  return guard(c, [&] {
+    BIT_CUDA(cudaSetDevice(c->device));
+    ctx_trim(c, keep);
+  });
+}
+
 static bit_status build_common(bit_ctx* h, int nsys, const int* ns, const int* mm,
                                const double* x, const double* y, const double* z,
                                bit_tree** out, bool host) {

@@ -121,6 +121,12 @@ bit_status bit_ctx_set_near_config(bit_ctx* ctx, int tile, int threads_per_targe
 bit_status bit_ctx_stream(const bit_ctx* ctx, void** stream);
 /* Bytes currently allocated by the context and its trees. */
 bit_status bit_ctx_memory(const bit_ctx* ctx, size_t* in_use, size_t* peak);
+/* Give back to the device the freed blocks the context keeps for reuse, largest first,
+ * until the bytes it holds (live + cached) are at most `keep`; live buffers are never
+ * freed.  Waits for the context's stream.  For a long-lived process that moves from one
+ * workload to another (e.g. a large batch, then serving) so that the next one finds the
+ * memory free.  No reference counterpart. */
+bit_status bit_ctx_trim(bit_ctx* ctx, size_t keep);
 
 /* treemake (src/tree3d.cpp:1345-1551): build the aspect-ratio bisection tree of the n
  * particles.  x, y, z are host arrays (original order).  The node numbering, children

@@ -456,3 +456,23 @@ def test_pinned_host_arrays_give_the_same_results(ctx):
     t2.treeempty()
     assert r2 is out
     assert np.array_equal(r1, r2)
+
+
+def test_trim_gives_back_cached_blocks_and_the_context_keeps_working(ctx):
+    """bit_ctx_trim frees the context's cached blocks (never live ones): an evaluation
+    after it gives the same potentials as before."""
+    import bit_b200 as B
+    g = load_golden("uniform3000")
+    p = B.params(B.SCREENED, B.CONSISTENT, B.FP64, kappa=1.0, acc=0.5)
+    t = ctx.treemake(g["x"], g["y"], g["z"], int(g["maxmemb"]))
+    t.treemoments(g["q"], int(g["nterms"]))
+    before = t.evaluate(p)
+    ctx.trim(0)  # the tree's live buffers stay
+    again = t.evaluate(p)
+    t.treeempty()
+    ctx.trim(0)
+    t = ctx.treemake(g["x"], g["y"], g["z"], int(g["maxmemb"]))
+    t.treemoments(g["q"], int(g["nterms"]))
+    after = t.evaluate(p)
+    t.treeempty()
+    assert np.array_equal(before, again) and np.array_equal(before, after)
