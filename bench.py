@@ -689,7 +689,9 @@ def run_serving(ctx, args, matched=False):
     srv = B.Server(slots=args.serve_slots, hbm_budget=budget)
     try:
         serve(reqs, closed, B.MIXED, srv, args.serve_slots)
-        _, cap = serve(reqs, closed, B.MIXED, srv, args.serve_slots)
+        with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+            _, cap = serve(reqs, closed, B.MIXED, srv, args.serve_slots)
+        cap_clocks = clk.summary()
         rate = load * cap["requests_per_s"]
         rng = np.random.default_rng(6)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
@@ -730,6 +732,7 @@ def run_serving(ctx, args, matched=False):
                         f"icosphere level 4..7, p={sp['nterms'] - 1}, theta={sp['acc']}, "
                         f"N0={sp['maxmemb']}, GMRES(50) to 1e-8), 150 GB budget",
             "offered_load": load, "mixed_closed_loop_requests_per_s": cap["requests_per_s"],
+            "mixed_closed_loop_clocks": cap_clocks,
             "fp64_closed_loop_requests_per_s": cap64["requests_per_s"],
             "capacity_ratio": cap["requests_per_s"] / cap64["requests_per_s"],
             "mixed_continuous_batching": mixed, "fp64_one_at_a_time": plain,
