@@ -317,6 +317,14 @@ def run_bit(args):
         ph["numtree"] = ss["numtree"]
         phases[prec] = ph
     line["phases"] = phases
+    # interactions per step: near (target, source) and far (target, cluster) pairs of both
+    # kernels, counted from the lists (the same for both precisions and for the reference)
+    inter = sum(st[k] for st in (st64_s, st64_c) for k in ("far_pairs", "near_pairs")) * world
+    line["interactions"] = {
+        "per_step": inter, "fp64_per_s": inter / (ms64 * 1e-3), "mixed_per_s": inter / (ms32 * 1e-3),
+        "e2e_fp64_per_s": inter / (e2e64_ms * 1e-3), "e2e_mixed_per_s": inter / (e2e32_ms * 1e-3),
+        "counted": "near (target, source) pairs plus far (target, cluster) pairs, screened and "
+                   "Coulomb, all ranks"}
     # rooflines: the dominant kernel of the FP64 step first, then the others
     fpp = far_flops_per_pair(NTERMS)
     roofs = []
@@ -349,6 +357,8 @@ def run_bit(args):
             line["accuracy_matched"]["serving"] = run_serving(ctx, args, matched=True)
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(x, y, z, q, n, args)
+        # the same lists, so the same interactions per eval
+        line["cpu_baseline"]["interactions_per_s"] = line["cpu_baseline"]["value"] * inter / evals
     line["gpu_launches"] = launches[B.FP64] * args.steps
     line["gpu_launches_per_step"] = launches[B.FP64]
     print(json.dumps(line), flush=True)
