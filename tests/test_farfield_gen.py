@@ -93,3 +93,29 @@ def test_flop_counts_behind_the_roofline():
     assert g.flops_per_pair(9)["screened"] == 2414
     assert g.count_flops(g.gen_coulomb_scaled(9)) < g.count_flops(g.gen_coulomb_scaled(9, False)) < 1459
     assert g.count_flops(g.gen_screened_scaled(9)) < g.count_flops(g.gen_screened_scaled_plain(9)) < 2414
+
+
+def test_shell_positions_of_the_tma_moment_blocks():
+    """The moment reduction writes each node's moments into a shell-order block by the
+    closed form of moments.cu's canon_shell_pos: degree d, then i and j descending, i.e.
+    C(d + 2, 3) + (d - i)(d - i + 1) / 2 + (d - i - j).  It must be the inverse of the
+    generator's shell order (what the far-field kernels consume), for every nterms, and
+    the blocks are padded to a multiple of 4 (16-byte TMA copies of FP32 moments)."""
+    g = gen()
+
+    def pos(t, nt):
+        i = j = 0
+        while t >= (nt - i) * (nt - i + 1) // 2:
+            t -= (nt - i) * (nt - i + 1) // 2
+            i += 1
+        while t >= nt - i - j:
+            t -= nt - i - j
+            j += 1
+        d = i + j + t
+        return d * (d + 1) * (d + 2) // 6 + (d - i) * (d - i + 1) // 2 + (d - i - j)
+
+    for nt in range(1, 11):
+        canon = g.moment_index(nt)
+        for k, v in enumerate(g.shells(nt - 1)):
+            assert pos(canon[v], nt) == k
+        assert g.padded(len(canon)) % 4 == 0 and g.padded(len(canon)) - len(canon) < 4
