@@ -60,10 +60,10 @@ MATCHED_BATCH_ACC = {5: 0.015, 7: 0.05, 9: 0.1}   # theta by nterms (p = 4, 6, 8
 # i.e. 135 and 78 MB scaled by N; the full-size launches read more (sources re-read by
 # groups of several waves once the 126 MB L2 no longer holds them).
 TRAFFIC = {
-    "k_near<SCREENED, F64>": 263.49e6, "k_near<COULOMB, F64>": 227.06e6,
-    "k_far<9, SCREENED, double>": 101.16e6, "k_far<9, COULOMB, double>": 100.93e6,
-    "k_near<SCREENED, F32>": 132.38e6, "k_near<COULOMB, F32>": 113.82e6,
-    "k_far<9, SCREENED, float>": 98.07e6, "k_far<9, COULOMB, float>": 97.25e6,
+    "k_near<SCREENED, F64>": 266.19e6, "k_near<COULOMB, F64>": 225.88e6,
+    "k_far<9, SCREENED, double>": 102.06e6, "k_far<9, COULOMB, double>": 102.54e6,
+    "k_near<SCREENED, F32>": 131.96e6, "k_near<COULOMB, F32>": 114.60e6,
+    "k_far<9, SCREENED, float>": 98.32e6, "k_far<9, COULOMB, float>": 98.96e6,
 }
 TRAFFIC_SOURCE = ("ncu launch list of the full-size step (gpu__time_duration.sum, "
                   "dram__bytes_read.sum, dram__bytes_write.sum; one pass per launch), "
